@@ -1,0 +1,942 @@
+// C ABI of libfbp_b200: context, device buffers, transfers and the pipeline
+// stages of class FBP3D / FBP2D (Source/FilteredBackProjection/FBP3D.h:16-170,
+// FBP2D.h:8-72 in the reference). Every entry point returns a status code and
+// records a message instead of the reference's `std::cout` + ASSERT(false).
+
+#include "fbp_internal.h"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+using fbp::Stack;
+
+namespace {
+
+thread_local std::string g_thread_error;
+constexpr double kPi = 3.14159265358979323846;
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+int next_pow2_reference(int m) {
+  // 1 << ceil_log2(m), ceil_log2(m) = floor_log2(2m - 1)
+  // (FastFourierTransformGPU.cpp:258-262, 269-280)
+  int l = 0;
+  for (long t = 2L * m - 1; t > 1; t >>= 1) l++;
+  return 1 << l;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define FBP_CTX(ctx)                                                                   \
+  if (!(ctx)) {                                                                        \
+    g_thread_error = "null context";                                                  \
+    return FBP_ERR_INVALID_ARGUMENT;                                                   \
+  }                                                                                    \
+  DeviceGuard device_guard_((ctx)->device)
+
+#define FBP_TRY(expr)          \
+  do {                         \
+    int rc_ = (expr);          \
+    if (rc_ != FBP_OK) return rc_; \
+  } while (0)
+
+cudaMemcpyKind kind_of(bool src_dev, bool dst_dev) {
+  if (src_dev && dst_dev) return cudaMemcpyDeviceToDevice;
+  if (src_dev) return cudaMemcpyDeviceToHost;
+  if (dst_dev) return cudaMemcpyHostToDevice;
+  return cudaMemcpyHostToHost;
+}
+
+// Device error word -> status (and reset).
+int check_device_error(fbp_context* ctx) {
+  int h = 0;
+  FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                          "error word readback"));
+  FBP_TRY(fbp::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+  if (h == fbp::kDevOk) return FBP_OK;
+  cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  switch (h) {
+    case fbp::kDevTimeout:
+      return fbp::set_error(ctx, FBP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+    case fbp::kDevFootprint:
+      return fbp::set_error(ctx, FBP_ERR_DEVICE_CHECK, "detector footprint exceeded the staged window");
+    case fbp::kDevGeometry:
+      return fbp::set_error(ctx, FBP_ERR_DEVICE_CHECK,
+                            "a voxel lies at or behind the source plane (source distance too small)");
+    default:
+      return fbp::set_error(ctx, FBP_ERR_DEVICE_CHECK, "device check failed");
+  }
+}
+
+int sync_host(fbp_context* ctx, bool host_involved) {
+  if (!host_involved) return FBP_OK;
+  FBP_TRY(fbp::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+  return check_device_error(ctx);
+}
+
+void free_stack(Stack& s) {
+  cudaFree(s.f32);
+  cudaFree(s.f16);
+  cudaFree(s.inv_scale);
+  bool sino = s.sinogram;
+  s = Stack();
+  s.sinogram = sino;
+}
+
+int alloc_stack(fbp_context* ctx, Stack& s, int u, int v, int n) {
+  if (u <= 0 || v <= 0 || n <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "stack sizes must be positive");
+  if (s.f32 && s.u == u && s.v == v && s.n == n) {
+    // same size: keep the allocation and clear it (FBP3D.cpp:30-38)
+    s.state = fbp::kRawF32;
+    s.log_pending = s.weights_pending = false;
+    return fbp::cuda_check(ctx, cudaMemsetAsync(s.f32, 0, s.bytes32(), ctx->stream), "clear stack");
+  }
+  free_stack(s);
+  s.u = u;
+  s.v = v;
+  s.n = n;
+  s.pitch = round_up(u, 4);
+  s.pitch16 = round_up(u, 8);
+  cudaError_t e = cudaMalloc(&s.f32, s.bytes32());
+  if (e != cudaSuccess) {
+    s.f32 = nullptr;
+    free_stack(s);
+    cudaGetLastError();
+    return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the detector stack failed");
+  }
+  return fbp::cuda_check(ctx, cudaMemsetAsync(s.f32, 0, s.bytes32(), ctx->stream), "clear stack");
+}
+
+fbp::RowSet rowset_of(Stack& s) {
+  fbp::RowSet rs{};
+  rs.data = s.f32;
+  rs.pitch = s.pitch;
+  rs.rows = (long long)s.rows();
+  rs.m = s.u;
+  rs.n_views = s.n;
+  rs.n_v = s.v;
+  rs.sinogram = s.sinogram;
+  rs.log_norm = s.log_pending;
+  rs.log_base = (float)s.log_base;
+  rs.weight = s.weights_pending;
+  rs.w_sdd = (float)s.w_sdd;
+  rs.w_du = (float)s.w_du;
+  rs.w_dv = (float)s.w_dv;
+  return rs;
+}
+
+// Apply any pending log / weight to the f32 rows in place.
+int flush_pending(fbp_context* ctx, Stack& s) {
+  if (!s.log_pending && !s.weights_pending) return FBP_OK;
+  FBP_TRY(fbp::launch_elementwise_pre(ctx, rowset_of(s)));
+  s.log_pending = s.weights_pending = false;
+  return FBP_OK;
+}
+
+// Bring the data back into f32 (from FP16 filtered storage) and flush.
+int materialize_f32(fbp_context* ctx, Stack& s) {
+  if (s.state == fbp::kFilteredF16) {
+    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, 0, s.rows(), s.f32, s.pitch));
+    s.state = fbp::kFilteredF32;
+  }
+  return flush_pending(ctx, s);
+}
+
+int require_stack(fbp_context* ctx, const Stack& s, const char* what) {
+  if (!s.f32) return fbp::set_error(ctx, FBP_ERR_STATE, std::string(what) + " but the buffer is not allocated");
+  return FBP_OK;
+}
+
+int ensure_volume(fbp_context* ctx, int x, int y, int z, bool clear) {
+  if (x <= 0 || y <= 0 || z <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume sizes must be positive");
+  if (!(ctx->vol && ctx->vx == x && ctx->vy == y && ctx->vz == z)) {
+    cudaFree(ctx->vol);
+    ctx->vol = nullptr;
+    ctx->vx = ctx->vy = ctx->vz = 0;
+    cudaError_t e = cudaMalloc(&ctx->vol, sizeof(float) * (size_t)x * y * z);
+    if (e != cudaSuccess) {
+      ctx->vol = nullptr;
+      cudaGetLastError();
+      return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the volume failed");
+    }
+    ctx->vx = x;
+    ctx->vy = y;
+    ctx->vz = z;
+    clear = true;
+  }
+  if (clear)
+    return fbp::cuda_check(ctx, cudaMemsetAsync(ctx->vol, 0, sizeof(float) * (size_t)x * y * z, ctx->stream),
+                           "clear volume");
+  return FBP_OK;
+}
+
+int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int n, int on_dev) {
+  if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
+  if (!(s.f32 && s.u == u && s.v == v && s.n == n)) FBP_TRY(alloc_stack(ctx, s, u, v, n));
+  s.state = fbp::kRawF32;
+  s.log_pending = s.weights_pending = false;
+  FBP_TRY(fbp::cuda_check(ctx,
+                          cudaMemcpy2DAsync(s.f32, (size_t)s.pitch * 4, src, (size_t)u * 4, (size_t)u * 4,
+                                            s.rows(), kind_of(on_dev, true), ctx->stream),
+                          "stack upload"));
+  return sync_host(ctx, !on_dev);
+}
+
+int download_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, float* dst, int on_dev) {
+  if (!dst) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null destination pointer");
+  FBP_TRY(flush_pending(ctx, s));
+  if (s.state == fbp::kFilteredF16) {
+    // convert just these rows into a scratch f32 block
+    float* tmp = static_cast<float*>(fbp::scratch(ctx, sizeof(float) * nrows * s.pitch));
+    if (!tmp) return FBP_ERR_OUT_OF_MEMORY;
+    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, row0, nrows, tmp, s.pitch));
+    FBP_TRY(fbp::cuda_check(ctx,
+                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, tmp, (size_t)s.pitch * 4, (size_t)s.u * 4, nrows,
+                                              kind_of(true, on_dev), ctx->stream),
+                            "row download"));
+  } else {
+    FBP_TRY(fbp::cuda_check(ctx,
+                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, s.f32 + row0 * s.pitch, (size_t)s.pitch * 4,
+                                              (size_t)s.u * 4, nrows, kind_of(true, on_dev), ctx->stream),
+                            "row download"));
+  }
+  return sync_host(ctx, !on_dev);
+}
+
+int upload_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, const float* src, int on_dev) {
+  if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
+  FBP_TRY(materialize_f32(ctx, s));
+  FBP_TRY(fbp::cuda_check(ctx,
+                          cudaMemcpy2DAsync(s.f32 + row0 * s.pitch, (size_t)s.pitch * 4, src, (size_t)s.u * 4,
+                                            (size_t)s.u * 4, nrows, kind_of(on_dev, true), ctx->stream),
+                          "row upload"));
+  return sync_host(ctx, !on_dev);
+}
+
+// Run weights / log (pending) + filter on a stack.
+int filter_stack(fbp_context* ctx, Stack& s, int filter_type) {
+  if (filter_type < 0 || filter_type > FBP_FILTER_RAMP_SAMPLED)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
+  if (s.state == fbp::kFilteredF16) {
+    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, 0, s.rows(), s.f32, s.pitch));
+    s.state = fbp::kFilteredF32;
+  }
+  const int n = ctx->pad_len > 0 ? ctx->pad_len : next_pow2_reference(s.u);
+  if (n < s.u || (n & (n - 1)))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length must be a power of two >= the row width");
+  FBP_TRY(fbp::ensure_filter_tables(ctx, n, filter_type));
+  fbp::RowSet rs = rowset_of(s);
+  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  int impl = ctx->filter_impl;
+  if (impl == FBP_FILTER_IMPL_AUTO)
+    impl = (mixed && fbp::toeplitz_supported(s.u)) ? FBP_FILTER_IMPL_TOEPLITZ : FBP_FILTER_IMPL_FFT;
+  if (mixed) {
+    if (!s.f16) {
+      if (fbp::cuda_check(ctx, cudaMalloc(&s.f16, s.bytes16()), "cudaMalloc(f16 stack)")) {
+        s.f16 = nullptr;
+        return FBP_ERR_OUT_OF_MEMORY;
+      }
+      if (fbp::cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
+        s.inv_scale = nullptr;
+        return FBP_ERR_OUT_OF_MEMORY;
+      }
+    }
+    float* scale = s.inv_scale + s.n;
+    FBP_TRY(fbp::launch_view_absmax(ctx, rs, scale, s.inv_scale));
+    rs.out16 = s.f16;
+    rs.pitch16 = s.pitch16;
+    rs.view_scale = scale;
+  }
+  if (impl == FBP_FILTER_IMPL_TOEPLITZ)
+    FBP_TRY(fbp::launch_filter_toeplitz(ctx, rs, n, filter_type));
+  else
+    FBP_TRY(fbp::launch_filter_fft(ctx, rs, n));
+  s.log_pending = s.weights_pending = false;
+  s.state = mixed ? fbp::kFilteredF16 : fbp::kFilteredF32;
+  return FBP_OK;
+}
+
+int record_weights(fbp_context* ctx, Stack& s, float sod, float odd, float det_w, const char* what) {
+  FBP_TRY(require_stack(ctx, s, what));
+  if (!(sod > 0.f) || !(odd >= 0.f) || !(det_w > 0.f))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "distances and detector width must be positive");
+  if (s.state == fbp::kFilteredF16) FBP_TRY(materialize_f32(ctx, s));
+  if (s.weights_pending) FBP_TRY(flush_pending(ctx, s));
+  s.weights_pending = true;
+  s.w_sdd = (double)sod + (double)odd;
+  s.w_du = (double)det_w / s.u;
+  s.w_dv = s.w_du;  // square detector pixels
+  return FBP_OK;
+}
+
+int record_log(fbp_context* ctx, Stack& s, float base, const char* what) {
+  FBP_TRY(require_stack(ctx, s, what));
+  if (!(base > 0.f)) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "base_value must be positive");
+  if (s.state == fbp::kFilteredF16) FBP_TRY(materialize_f32(ctx, s));
+  // log must run before weights; if weights are already pending (or a log
+  // is), materialise them first so that the call order is honoured
+  if (s.weights_pending || s.log_pending) FBP_TRY(flush_pending(ctx, s));
+  s.log_pending = true;
+  s.log_base = base;
+  return FBP_OK;
+}
+
+fbp::BPGeom cone_geom(const Stack& s, float sod, float odd, float det_w, float vol_w, float rot, int h, int v,
+                      float offset) {
+  fbp::BPGeom g{};
+  g.kind = FBP_GEOMETRY_CONE;
+  g.sod = sod;
+  g.sdd = (double)sod + (double)odd;
+  g.du = (double)det_w / s.u;
+  g.dv = g.du;
+  g.vox = (double)vol_w / h;
+  g.span = 2.0 * kPi * (double)rot;
+  g.offset = offset;
+  g.nu = s.u;
+  g.nv = s.v;
+  g.nviews = s.n;
+  g.nx = h;
+  g.ny = v;
+  g.nz = h;
+  return g;
+}
+
+int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
+  if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
+  if (g.kind == FBP_GEOMETRY_CONE && !(g.sod > 0.0 && g.sdd >= g.sod))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "source distance must be positive");
+  if (!(g.du > 0.0) || !(g.vox > 0.0))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
+  FBP_TRY(flush_pending(ctx, s));
+  FBP_TRY(ensure_volume(ctx, g.nx, g.ny, g.nz, false));
+  const int ylim = ctx->clip_after_bp ? g.nz : 0;  // the reference clips y-slices below z_size
+  return fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, ctx->precision == FBP_PRECISION_MIXED);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+}  // namespace
+
+namespace fbp {
+
+int set_error(fbp_context* ctx, int code, const std::string& msg) {
+  if (ctx)
+    ctx->last_error = msg;
+  else
+    g_thread_error = msg;
+  return code;
+}
+
+int cuda_check(fbp_context* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FBP_OK;
+  cudaGetLastError();
+  int code = e == cudaErrorMemoryAllocation ? FBP_ERR_OUT_OF_MEMORY : FBP_ERR_CUDA;
+  return set_error(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* scratch(fbp_context* ctx, size_t bytes) {
+  if (bytes <= ctx->scratch_bytes) return ctx->d_scratch;
+  cudaFree(ctx->d_scratch);
+  ctx->d_scratch = nullptr;
+  ctx->scratch_bytes = 0;
+  size_t b = std::max<size_t>(bytes, 1 << 20);
+  if (cudaMalloc(&ctx->d_scratch, b) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of scratch memory failed");
+    ctx->d_scratch = nullptr;
+    return nullptr;
+  }
+  ctx->scratch_bytes = b;
+  return ctx->d_scratch;
+}
+
+int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
+                       const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]) {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
+  cuuint64_t gstr[2] = {strides_bytes[0], strides_bytes[1]};
+  cuuint32_t bdim[3] = {box[0], box[1], box[2]};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(map, dtype, 3, base, gdim, gstr, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return FBP_OK;
+}
+
+}  // namespace fbp
+
+extern "C" {
+
+// ------------------------------------------------------------------ context
+int fbp_create(fbp_context** out, int device) {
+  if (!out) {
+    g_thread_error = "null output pointer";
+    return FBP_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    g_thread_error = "no CUDA device";
+    return FBP_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) {
+    g_thread_error = "device index out of range";
+    return FBP_ERR_INVALID_ARGUMENT;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major != 10) {
+    g_thread_error = std::string("libfbp_b200 is built for sm_100a (B200); device is ") + prop.name;
+    return FBP_ERR_UNSUPPORTED;
+  }
+  DeviceGuard guard(device);
+  fbp_context* ctx = new fbp_context();
+  ctx->device = device;
+  ctx->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) {
+    g_thread_error = std::string("context setup failed: ") + cudaGetErrorString(cudaGetLastError());
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    cudaFree(ctx->d_err);
+    delete ctx;
+    return FBP_ERR_CUDA;
+  }
+  ctx->own_stream = true;
+  ctx->proj.sinogram = false;
+  ctx->sino.sinogram = true;
+  *out = ctx;
+  return FBP_OK;
+}
+
+int fbp_destroy(fbp_context* ctx) {
+  if (!ctx) return FBP_OK;
+  {
+    DeviceGuard guard(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_stack(ctx->proj);
+    free_stack(ctx->sino);
+    cudaFree(ctx->vol);
+    cudaFree(ctx->d_err);
+    cudaFree(ctx->d_trig);
+    cudaFree(ctx->d_span);
+    cudaFree(ctx->ftab.twiddle);
+    cudaFree(ctx->ftab.hbr);
+    cudaFree(ctx->ftab.kernel);
+    cudaFree(ctx->d_scratch);
+    cudaFreeHost(ctx->h_pinned);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return FBP_OK;
+}
+
+const char* fbp_last_error(const fbp_context* ctx) {
+  return ctx ? ctx->last_error.c_str() : g_thread_error.c_str();
+}
+
+int fbp_set_stream(fbp_context* ctx, void* stream) {
+  FBP_CTX(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  if (stream) {
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->own_stream = false;
+  } else {
+    ctx->own_stream = true;
+    return fbp::cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream create");
+  }
+  return FBP_OK;
+}
+
+int fbp_synchronize(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  FBP_TRY(fbp::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"));
+  return check_device_error(ctx);
+}
+
+int fbp_set_precision(fbp_context* ctx, int precision) {
+  FBP_CTX(ctx);
+  if (precision != FBP_PRECISION_FP32 && precision != FBP_PRECISION_MIXED)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown precision");
+  ctx->precision = precision;
+  return FBP_OK;
+}
+
+int fbp_set_filter_impl(fbp_context* ctx, int impl) {
+  FBP_CTX(ctx);
+  if (impl < FBP_FILTER_IMPL_AUTO || impl > FBP_FILTER_IMPL_TOEPLITZ)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter implementation");
+  ctx->filter_impl = impl;
+  return FBP_OK;
+}
+
+int fbp_set_filter_padding(fbp_context* ctx, int padded_length) {
+  FBP_CTX(ctx);
+  if (padded_length < 0 || (padded_length & (padded_length - 1)))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padding must be 0 or a power of two");
+  ctx->pad_len = padded_length;
+  return FBP_OK;
+}
+
+int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable) {
+  FBP_CTX(ctx);
+  ctx->clip_after_bp = enable ? 1 : 0;
+  return FBP_OK;
+}
+
+int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes) {
+  if (!ctx || !bytes) return FBP_ERR_INVALID_ARGUMENT;
+  size_t b = 0;
+  if (ctx->vol) b += sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
+  for (const Stack* s : {&ctx->proj, &ctx->sino}) {
+    if (s->f32) b += s->bytes32();
+    if (s->f16) b += s->bytes16() + sizeof(float) * 2 * s->n;
+  }
+  b += ctx->scratch_bytes;
+  *bytes = b;
+  return FBP_OK;
+}
+
+// ------------------------------------------------------------------ buffers
+int fbp_generate_blank_volume(fbp_context* ctx, int x, int y, int z) {
+  FBP_CTX(ctx);
+  return ensure_volume(ctx, x, y, z, true);
+}
+
+int fbp_generate_blank_projections(fbp_context* ctx, int x, int y, int n) {
+  FBP_CTX(ctx);
+  return alloc_stack(ctx, ctx->proj, x, y, n);
+}
+
+int fbp_generate_blank_sinograms(fbp_context* ctx, int x, int y, int n) {
+  FBP_CTX(ctx);
+  return alloc_stack(ctx, ctx->sino, x, y, n);
+}
+
+int fbp_free_volume(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->vol);
+  ctx->vol = nullptr;
+  ctx->vx = ctx->vy = ctx->vz = 0;
+  return FBP_OK;
+}
+
+int fbp_free_projections(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  free_stack(ctx->proj);
+  return FBP_OK;
+}
+
+int fbp_free_sinograms(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  free_stack(ctx->sino);
+  return FBP_OK;
+}
+
+int fbp_get_volume_size(const fbp_context* ctx, int* x, int* y, int* z) {
+  if (!ctx || !x || !y || !z) return FBP_ERR_INVALID_ARGUMENT;
+  *x = ctx->vx;
+  *y = ctx->vy;
+  *z = ctx->vz;
+  return FBP_OK;
+}
+
+int fbp_get_projections_size(const fbp_context* ctx, int* u, int* v, int* n) {
+  if (!ctx || !u || !v || !n) return FBP_ERR_INVALID_ARGUMENT;
+  *u = ctx->proj.u;
+  *v = ctx->proj.v;
+  *n = ctx->proj.n;
+  return FBP_OK;
+}
+
+// ---------------------------------------------------------------- transfers
+int fbp_upload_projections(fbp_context* ctx, const float* src, int u, int v, int n, int on_dev) {
+  FBP_CTX(ctx);
+  return upload_stack(ctx, ctx->proj, src, u, v, n, on_dev);
+}
+
+int fbp_upload_sinograms(fbp_context* ctx, const float* src, int u, int v, int n, int on_dev) {
+  FBP_CTX(ctx);
+  return upload_stack(ctx, ctx->sino, src, u, v, n, on_dev);
+}
+
+int fbp_download_projections(fbp_context* ctx, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "download_projections"));
+  return download_rows(ctx, ctx->proj, 0, ctx->proj.rows(), dst, on_dev);
+}
+
+int fbp_download_sinograms(fbp_context* ctx, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "download_sinograms"));
+  return download_rows(ctx, ctx->sino, 0, ctx->sino.rows(), dst, on_dev);
+}
+
+int fbp_store_projection(fbp_context* ctx, const float* src, int index, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "store_projection"));
+  if (index < 0 || index >= ctx->proj.n) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "projection index out of range");
+  return upload_rows(ctx, ctx->proj, (size_t)index * ctx->proj.v, ctx->proj.v, src, on_dev);
+}
+
+int fbp_load_projection(fbp_context* ctx, int index, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "load_projection"));
+  if (index < 0 || index >= ctx->proj.n) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "projection index out of range");
+  return download_rows(ctx, ctx->proj, (size_t)index * ctx->proj.v, ctx->proj.v, dst, on_dev);
+}
+
+int fbp_store_sinogram(fbp_context* ctx, const float* src, int y, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "store_sinogram"));
+  if (y < 0 || y >= ctx->sino.v) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "sinogram index out of range");
+  return upload_rows(ctx, ctx->sino, (size_t)y * ctx->sino.n, ctx->sino.n, src, on_dev);
+}
+
+int fbp_load_sinogram(fbp_context* ctx, int y, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "load_sinogram"));
+  if (y < 0 || y >= ctx->sino.v) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "sinogram index out of range");
+  return download_rows(ctx, ctx->sino, (size_t)y * ctx->sino.n, ctx->sino.n, dst, on_dev);
+}
+
+static int volume_slice(fbp_context* ctx, int axis, int index, float* host_or_dev, int on_dev, bool load) {
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "volume is not allocated");
+  if (!host_or_dev) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
+  const int nx = ctx->vx, ny = ctx->vy, nz = ctx->vz;
+  const int lim = axis == 0 ? nx : axis == 1 ? ny : nz;
+  if (index < 0 || index >= lim) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "slice index out of range");
+  float* v = ctx->vol;
+  cudaError_t e;
+  const cudaMemcpyKind k = load ? kind_of(true, on_dev) : kind_of(on_dev, true);
+  if (axis == 2) {  // z-slice [y][x]: contiguous
+    float* p = v + (size_t)index * nx * ny;
+    e = load ? cudaMemcpyAsync(host_or_dev, p, sizeof(float) * nx * ny, k, ctx->stream)
+             : cudaMemcpyAsync(p, host_or_dev, sizeof(float) * nx * ny, k, ctx->stream);
+  } else if (axis == 1) {  // y-slice [z][x]
+    float* p = v + (size_t)index * nx;
+    e = load ? cudaMemcpy2DAsync(host_or_dev, sizeof(float) * nx, p, sizeof(float) * nx * ny, sizeof(float) * nx, nz, k,
+                                 ctx->stream)
+             : cudaMemcpy2DAsync(p, sizeof(float) * nx * ny, host_or_dev, sizeof(float) * nx, sizeof(float) * nx, nz, k,
+                                 ctx->stream);
+  } else {  // x-slice [z][y]
+    float* p = v + index;
+    e = load ? cudaMemcpy2DAsync(host_or_dev, sizeof(float), p, sizeof(float) * nx, sizeof(float), (size_t)ny * nz, k,
+                                 ctx->stream)
+             : cudaMemcpy2DAsync(p, sizeof(float) * nx, host_or_dev, sizeof(float), sizeof(float), (size_t)ny * nz, k,
+                                 ctx->stream);
+  }
+  FBP_TRY(fbp::cuda_check(ctx, e, "volume slice copy"));
+  return sync_host(ctx, !on_dev);
+}
+
+int fbp_load_volume_slice_x(fbp_context* ctx, int i, float* d, int o) { FBP_CTX(ctx); return volume_slice(ctx, 0, i, d, o, true); }
+int fbp_load_volume_slice_y(fbp_context* ctx, int i, float* d, int o) { FBP_CTX(ctx); return volume_slice(ctx, 1, i, d, o, true); }
+int fbp_load_volume_slice_z(fbp_context* ctx, int i, float* d, int o) { FBP_CTX(ctx); return volume_slice(ctx, 2, i, d, o, true); }
+int fbp_store_volume_slice_x(fbp_context* ctx, const float* s, int i, int o) { FBP_CTX(ctx); return volume_slice(ctx, 0, i, const_cast<float*>(s), o, false); }
+int fbp_store_volume_slice_y(fbp_context* ctx, const float* s, int i, int o) { FBP_CTX(ctx); return volume_slice(ctx, 1, i, const_cast<float*>(s), o, false); }
+int fbp_store_volume_slice_z(fbp_context* ctx, const float* s, int i, int o) { FBP_CTX(ctx); return volume_slice(ctx, 2, i, const_cast<float*>(s), o, false); }
+
+int fbp_read_volume(fbp_context* ctx, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "read_volume but the volume is not allocated");
+  if (!dst) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null destination pointer");
+  size_t bytes = sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
+  FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(dst, ctx->vol, bytes, kind_of(true, on_dev), ctx->stream), "volume download"));
+  return sync_host(ctx, true);
+}
+
+int fbp_write_volume_data(fbp_context* ctx, const float* src, int on_dev) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "write_volume_data but the volume is not allocated");
+  if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
+  size_t bytes = sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
+  FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(ctx->vol, src, bytes, kind_of(on_dev, true), ctx->stream), "volume upload"));
+  return sync_host(ctx, !on_dev);
+}
+
+int fbp_volume_device_ptr(fbp_context* ctx, float** ptr) {
+  FBP_CTX(ctx);
+  if (!ptr) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
+  *ptr = ctx->vol;
+  return ctx->vol ? FBP_OK : fbp::set_error(ctx, FBP_ERR_STATE, "volume is not allocated");
+}
+
+int fbp_projections_device_ptr(fbp_context* ctx, float** ptr, int* pitch) {
+  FBP_CTX(ctx);
+  if (!ptr || !pitch) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
+  FBP_TRY(require_stack(ctx, ctx->proj, "projections_device_ptr"));
+  FBP_TRY(materialize_f32(ctx, ctx->proj));
+  *ptr = ctx->proj.f32;
+  *pitch = ctx->proj.pitch;
+  return FBP_OK;
+}
+
+// ----------------------------------------------------------- pipeline stages
+int fbp_log_normalize_projections(fbp_context* ctx, float base) {
+  FBP_CTX(ctx);
+  return record_log(ctx, ctx->proj, base, "log_normalize_projections");
+}
+
+int fbp_log_normalize_sinograms(fbp_context* ctx, float base) {
+  FBP_CTX(ctx);
+  return record_log(ctx, ctx->sino, base, "log_normalize_sinograms");
+}
+
+int fbp_apply_fdk_weights_to_projections(fbp_context* ctx, float sod, float odd, float det_w) {
+  FBP_CTX(ctx);
+  return record_weights(ctx, ctx->proj, sod, odd, det_w, "apply_fdk_weights_to_projections");
+}
+
+int fbp_apply_fdk_weights_to_sinograms(fbp_context* ctx, float sod, float odd, float det_w) {
+  FBP_CTX(ctx);
+  return record_weights(ctx, ctx->sino, sod, odd, det_w, "apply_fdk_weights_to_sinograms");
+}
+
+int fbp_apply_filter_to_projections(fbp_context* ctx, int filter_type) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "apply_filter_to_projections"));
+  return filter_stack(ctx, ctx->proj, filter_type);
+}
+
+int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "apply_filter_to_sinograms"));
+  return filter_stack(ctx, ctx->sino, filter_type);
+}
+
+int fbp_clip_negatives_of_volume(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "clip_negatives_of_volume but the volume is not allocated");
+  return fbp::launch_clip(ctx, ctx->vol, ctx->vx, ctx->vy, ctx->vz, ctx->vz);
+}
+
+int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,
+                                                   float rot, int h, int v, float offset) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "project_backward_cone_fdk_from_projections"));
+  return backproject(ctx, ctx->proj, cone_geom(ctx->proj, sod, odd, det_w, vol_w, rot, h, v, offset));
+}
+
+int fbp_project_backward_cone_fdk_from_sinograms(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,
+                                                 float rot, int h, int v, float offset) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "project_backward_cone_fdk_from_sinograms"));
+  return backproject(ctx, ctx->sino, cone_geom(ctx->sino, sod, odd, det_w, vol_w, rot, h, v, offset));
+}
+
+static fbp::BPGeom parallel_geom(const Stack& s, float rot, int h, int v, float offset) {
+  // The reference passes projection_plane_width = volume_width = x size
+  // (FBP3D.cpp:481-482): the detector spans the volume width, in voxel units.
+  fbp::BPGeom g{};
+  g.kind = FBP_GEOMETRY_PARALLEL;
+  g.vox = 1.0;
+  g.du = (double)h / s.u;
+  g.dv = (double)v / s.v;
+  g.span = 2.0 * kPi * (double)rot;
+  g.offset = offset;
+  g.nu = s.u;
+  g.nv = s.v;
+  g.nviews = s.n;
+  g.nx = h;
+  g.ny = v;
+  g.nz = h;
+  return g;
+}
+
+int fbp_project_backward_parallel_from_projections(fbp_context* ctx, float rot, int h, int v, float offset) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "project_backward_parallel_from_projections"));
+  if (h <= 0 || v <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
+  return backproject(ctx, ctx->proj, parallel_geom(ctx->proj, rot, h, v, offset));
+}
+
+int fbp_project_backward_parallel_from_sinograms(fbp_context* ctx, float rot, int h, int v, float offset) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "project_backward_parallel_from_sinograms"));
+  if (h <= 0 || v <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
+  return backproject(ctx, ctx->sino, parallel_geom(ctx->sino, rot, h, v, offset));
+}
+
+int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* g, int filter_type, int h, int v) {
+  FBP_CTX(ctx);
+  if (!g) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null geometry");
+  FBP_TRY(require_stack(ctx, ctx->proj, "reconstruct_fdk"));
+  if (g->kind == FBP_GEOMETRY_CONE) {
+    FBP_TRY(record_weights(ctx, ctx->proj, g->source_distance, g->detector_distance, g->detector_width, "reconstruct_fdk"));
+    FBP_TRY(filter_stack(ctx, ctx->proj, filter_type));
+    return backproject(ctx, ctx->proj,
+                       cone_geom(ctx->proj, g->source_distance, g->detector_distance, g->detector_width, g->volume_width,
+                                 g->full_rotation_count, h, v, g->rotation_offset_radian));
+  }
+  FBP_TRY(filter_stack(ctx, ctx->proj, filter_type));
+  fbp::BPGeom pg = parallel_geom(ctx->proj, g->full_rotation_count, h, v, g->rotation_offset_radian);
+  pg.vox = (double)g->volume_width / h;
+  pg.du = (double)g->detector_width / ctx->proj.u;
+  pg.dv = pg.du;
+  return backproject(ctx, ctx->proj, pg);
+}
+
+// ----------------------------------------------------------------------- 2D
+static int stage_2d(fbp_context* ctx, const float* sino, int bins, int views, Stack& st, size_t offset_bytes) {
+  st = Stack();
+  st.u = bins;
+  st.v = 1;
+  st.n = views;
+  st.pitch = round_up(bins, 4);
+  st.state = fbp::kFilteredF32;
+  char* base = static_cast<char*>(fbp::scratch(ctx, offset_bytes + st.bytes32()));
+  if (!base) return FBP_ERR_OUT_OF_MEMORY;
+  st.f32 = reinterpret_cast<float*>(base + offset_bytes);
+  return fbp::cuda_check(ctx,
+                         cudaMemcpy2DAsync(st.f32, (size_t)st.pitch * 4, sino, (size_t)bins * 4, (size_t)bins * 4,
+                                           views, cudaMemcpyDeviceToDevice, ctx->stream),
+                         "2D sinogram staging");
+}
+
+int fbp2d_filter_sinogram(fbp_context* ctx, float* sino, int bins, int views, int filter_type, float fan_sdd,
+                          float det_w) {
+  FBP_CTX(ctx);
+  if (!sino || bins <= 0 || views <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad sinogram");
+  if (filter_type < 0 || filter_type > FBP_FILTER_RAMP_SAMPLED)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
+  const int n = ctx->pad_len > 0 ? ctx->pad_len : next_pow2_reference(bins);
+  if (n < bins) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length smaller than the row");
+  FBP_TRY(fbp::ensure_filter_tables(ctx, n, filter_type));
+  fbp::RowSet rs{};
+  rs.data = sino;
+  rs.pitch = bins;
+  rs.rows = views;
+  rs.m = bins;
+  rs.n_views = views;
+  rs.n_v = 1;
+  rs.sinogram = false;
+  if (fan_sdd > 0.f) {
+    if (!(det_w > 0.f)) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector width must be positive");
+    rs.weight = true;
+    rs.w_sdd = fan_sdd;
+    rs.w_du = det_w / bins;
+    rs.w_dv = 0.f;
+  }
+  return fbp::launch_filter_fft(ctx, rs, n);
+}
+
+int fbp2d_project_backward(fbp_context* ctx, const float* sino, int bins, int views, const fbp_geometry* geom,
+                           float* image, int nx, int nz) {
+  FBP_CTX(ctx);
+  if (!sino || !image || !geom || bins <= 0 || views <= 0 || nx <= 0 || nz <= 0)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad 2D backprojection arguments");
+  if (!(geom->detector_width > 0.f) || !(geom->volume_width > 0.f))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
+  fbp::BPGeom g{};
+  g.kind = geom->kind == FBP_GEOMETRY_CONE ? FBP_GEOMETRY_CONE : FBP_GEOMETRY_PARALLEL;
+  g.sod = geom->source_distance;
+  g.sdd = (double)geom->source_distance + geom->detector_distance;
+  if (g.kind == FBP_GEOMETRY_CONE && !(g.sod > 0.0))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "source distance must be positive");
+  g.du = (double)geom->detector_width / bins;
+  g.dv = 1.0;
+  g.vox = (double)geom->volume_width / nx;
+  g.span = 2.0 * kPi * (double)geom->full_rotation_count;
+  g.offset = geom->rotation_offset_radian;
+  g.nu = bins;
+  g.nv = 1;
+  g.nviews = views;
+  g.nx = nx;
+  g.ny = 1;
+  g.nz = nz;
+  Stack st;
+  FBP_TRY(stage_2d(ctx, sino, bins, views, st, 0));
+  return fbp::launch_backproject(ctx, g, st, image, 0, false);
+}
+
+int fbp2d_parallelize_fan_beam_sinogram(fbp_context* ctx, const float* fan, int bins, int views,
+                                        const fbp_geometry* geom, float* par, int out_bins, float out_w) {
+  FBP_CTX(ctx);
+  if (!fan || !par || !geom || bins <= 0 || views <= 0 || out_bins <= 0 || !(out_w > 0.f))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad rebinning arguments");
+  fbp::BPGeom g{};
+  g.sod = geom->source_distance;
+  g.sdd = (double)geom->source_distance + geom->detector_distance;
+  g.du = (double)geom->detector_width / bins;
+  g.span = 2.0 * kPi * (double)geom->full_rotation_count;
+  g.offset = geom->rotation_offset_radian;
+  return fbp::launch_rebin_fan(ctx, fan, bins, views, g, par, out_bins, (double)out_w / out_bins);
+}
+
+// ------------------------------------------------------------------ FFT rows
+int fbp_fft_rows(fbp_context* ctx, float* rows, int n, int count, int inverse) {
+  FBP_CTX(ctx);
+  if (!rows) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null rows");
+  return fbp::launch_fft_rows(ctx, reinterpret_cast<float2*>(rows), n, count, inverse);
+}
+
+int fbp_fft_shift_rows(fbp_context* ctx, float* rows, int n, int count, int shift) {
+  FBP_CTX(ctx);
+  if (!rows) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null rows");
+  return fbp::launch_fft_shift_rows(ctx, reinterpret_cast<float2*>(rows), n, count, shift);
+}
+
+// ------------------------------------------------------------------ phantoms
+int fbp_project_ellipsoids_to_projections(fbp_context* ctx, const double* ell, int count, const fbp_geometry* geom) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->proj, "project_ellipsoids_to_projections"));
+  if (!geom || (count > 0 && !ell)) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null argument");
+  if (count < 0 || count > 64) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "ellipsoid count must be in [0, 64]");
+  Stack& s = ctx->proj;
+  fbp::BPGeom g{};
+  g.kind = geom->kind;
+  g.sod = geom->source_distance;
+  g.sdd = (double)geom->source_distance + geom->detector_distance;
+  g.du = (double)geom->detector_width / s.u;
+  g.dv = g.du;
+  g.span = 2.0 * kPi * (double)geom->full_rotation_count;
+  g.offset = geom->rotation_offset_radian;
+  g.nu = s.u;
+  g.nv = s.v;
+  g.nviews = s.n;
+  double* d = static_cast<double*>(fbp::scratch(ctx, sizeof(double) * 16 * std::max(count, 1)));
+  if (!d) return FBP_ERR_OUT_OF_MEMORY;
+  if (count > 0)
+    FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(d, ell, sizeof(double) * 16 * count, cudaMemcpyHostToDevice, ctx->stream),
+                            "ellipsoid upload"));
+  s.state = fbp::kRawF32;
+  s.log_pending = s.weights_pending = false;
+  FBP_TRY(fbp::launch_project_ellipsoids(ctx, d, count, g, s.f32, s.pitch));
+  // the host array is only borrowed for the call
+  return fbp::cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+}
+
+}  // extern "C"

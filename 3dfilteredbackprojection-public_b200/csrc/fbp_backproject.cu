@@ -1,0 +1,652 @@
+// Voxel-driven, distance-weighted backprojection with bilinear detector
+// interpolation, for flat-panel cone beam (FDK) and parallel beam, in 3D and
+// 2D (a 2D image is a volume with one y-slice and a one-row detector).
+//
+// Replaces the reference's per-view dispatch loop
+// FBP3D::project_backward_cone_fdk_from_projections (Source/FilteredBackProjection/
+// FBP3D.cpp:524-559, one full read-modify-write of the volume per view) and the
+// 3D / 2D parallel variants (FBP3D.cpp:460-522, FBP2D.cpp:96-122). The GLSL
+// bodies are not in the reference; the arithmetic is the textbook FDK one.
+//
+// Design (one launch for all views):
+//   * A CTA owns a TX x TZ tile of voxel columns and NY voxels along the
+//     rotation axis (y); each thread owns one column segment of NY voxels and
+//     keeps its NY sums in registers across every view, so the volume is
+//     written exactly once.
+//   * Views are processed in chunks. For every (tile, view) one lane of warp 0
+//     computes, in FP64, the tile's detector footprint and the tile-local
+//     projective coefficients (the tile's rows of the projection matrix,
+//     re-based on the tile corner and on the staged window so that the FP32
+//     detector coordinates the threads form stay small and accurate). The
+//     footprint window (box_u x box_v detector samples) is copied into shared
+//     memory by TMA (cp.async.bulk.tensor, no multicast), double-buffered
+//     through mbarriers; samples outside the detector arrive as zeros from the
+//     TMA out-of-bounds fill.
+//   * Per view a thread forms 1/D, its detector column u (constant along the
+//     column), the distance weight and the v step once, then walks its NY
+//     voxels with one FMA per voxel for v: four shared-memory taps and three
+//     lerps per update.
+//   * Every mbarrier wait is bounded; on expiry the CTA records an error and
+//     leaves, and every CTA checks the error word before starting.
+
+#include "fbp_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+namespace fbp {
+namespace {
+
+constexpr int kMaxChunk = 8;            // views per pipeline stage (upper bound)
+constexpr uint32_t kWaitLimit = 1u << 24;  // mbarrier polls before giving up
+
+struct ViewCoef {
+  float Dx, Dz, D0;  // D = L / SOD (cone) or 1 (parallel), affine in (x', z')
+  float Nx, Nz, N0;  // u_local * D
+  float Vx, Vz, V0;  // v_local * D at the tile's first y
+  float wscale;      // extra per-view weight (FP16 views: 1 / scale)
+  int skip;          // tile footprint misses the detector
+  int pad;
+};
+
+struct BPArgs {
+  float* vol;
+  int nx, ny, nz;
+  int nu, nv, nviews;
+  int kind;
+  double sod, sdd, du, dv, vox;
+  double cu, cv;          // (nu - 1) / 2, (nv - 1) / 2
+  float dvn;              // v step per voxel times D
+  float scale;            // pi / K * filter spacing factor
+  const double2* trig;    // (cos, sin) per view
+  const float* inv_scale; // FP16 per-view 1/scale or nullptr
+  int box_u, box_v, align;
+  int box_bytes;          // smem bytes reserved per staged window (multiple of 128)
+  int tx_bytes;           // bytes one TMA box transfer delivers (box_u * box_v * element)
+  int chunk;              // views per stage
+  int ntx, ntz;           // tiles along x and z
+  int sino_layout;        // tensor coordinates (u, view, v) instead of (u, v, view)
+  int clip_ylimit;        // clip negatives where iy < clip_ylimit
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false (and records kDevTimeout) after kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicCAS(err, 0, kDevTimeout);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) {  // b > 0
+  int q = a / b;
+  return (a % b != 0 && a < 0) ? q - 1 : q;
+}
+
+// Tile geometry for view k in FP64: the affine coefficients of D (= L/SOD
+// for cone beam, 1 for parallel beam), of u*D and of v*D in tile-local voxel
+// offsets (x', z', y'), and the detector extremes over the tile's corner
+// voxels. A projective map attains its extremes over a box at the corners.
+struct TileGeo {
+  double Dx, Dz, D0, Ux, Uz, U0, G, Yc;
+  double umin, umax, vmin, vmax, dmin;
+};
+
+__device__ void tile_geo(const BPArgs& a, int k, int ix0, int iy0, int iz0, int ex, int ey, int ez, TileGeo& t) {
+  const double c = a.trig[k].x, s = a.trig[k].y;
+  const double Xc = (ix0 + 0.5 - 0.5 * a.nx) * a.vox;
+  const double Zc = (iz0 + 0.5 - 0.5 * a.nz) * a.vox;
+  t.Yc = (iy0 + 0.5 - 0.5 * a.ny) * a.vox;
+  if (a.kind == FBP_GEOMETRY_CONE) {
+    const double K = a.sdd / (a.sod * a.du);
+    t.Dx = a.vox * c / a.sod;
+    t.Dz = a.vox * s / a.sod;
+    t.D0 = (a.sod + Xc * c + Zc * s) / a.sod;
+    t.Ux = -a.vox * s * K;
+    t.Uz = a.vox * c * K;
+    t.U0 = (-Xc * s + Zc * c) * K;
+    t.G = a.sdd / (a.sod * a.dv);
+  } else {
+    t.Dx = 0.0;
+    t.Dz = 0.0;
+    t.D0 = 1.0;
+    t.Ux = -a.vox * s / a.du;
+    t.Uz = a.vox * c / a.du;
+    t.U0 = (-Xc * s + Zc * c) / a.du;
+    t.G = 1.0 / a.dv;
+  }
+  t.umin = 1e300;
+  t.umax = -1e300;
+  t.vmin = 1e300;
+  t.vmax = -1e300;
+  t.dmin = 1e300;
+#pragma unroll
+  for (int cx = 0; cx < 2; ++cx)
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz) {
+      const double x = cx ? ex : 0, z = cz ? ez : 0;
+      const double D = t.Dx * x + t.Dz * z + t.D0;
+      t.dmin = fmin(t.dmin, D);
+      const double u = (t.Ux * x + t.Uz * z + t.U0) / D + a.cu;
+      t.umin = fmin(t.umin, u);
+      t.umax = fmax(t.umax, u);
+#pragma unroll
+      for (int cy = 0; cy < 2; ++cy) {
+        const double y = cy ? ey : 0;
+        const double v = t.G * (t.Yc + a.vox * y) / D + a.cv;
+        t.vmin = fmin(t.vmin, v);
+        t.vmax = fmax(t.vmax, v);
+      }
+    }
+}
+
+constexpr double kSlack = 1.0 / 64;  // detector samples of margin around the footprint
+
+__device__ __forceinline__ bool tile_skip(const BPArgs& a, const TileGeo& t) {
+  return t.dmin <= 1e-6 || t.umax <= -1.0 || t.umin >= (double)a.nu || t.vmax <= -1.0 || t.vmin >= (double)a.nv;
+}
+
+// Window origin (u0 aligned down for TMA) and the samples the tile needs.
+__device__ __forceinline__ void tile_window(const BPArgs& a, const TileGeo& t, int& u0, int& v0, int& need_u,
+                                            int& need_v) {
+  u0 = floor_div((int)floor(t.umin - kSlack), a.align) * a.align;
+  v0 = (int)floor(t.vmin - kSlack);
+  need_u = (int)floor(t.umax + kSlack) + 2 - u0;
+  need_v = (int)floor(t.vmax + kSlack) + 2 - v0;
+}
+
+// Coefficients for view k of this tile; returns skip.
+__device__ bool tile_view_coef(const BPArgs& a, int k, int ix0, int iy0, int iz0, int ex, int ey, int ez,
+                               ViewCoef& vc, int& u0, int& v0, bool& overflow, bool& behind) {
+  TileGeo t;
+  tile_geo(a, k, ix0, iy0, iz0, ex, ey, ez, t);
+  behind = t.dmin <= 1e-6;
+  const bool skip = tile_skip(a, t);
+  int need_u, need_v;
+  tile_window(a, t, u0, v0, need_u, need_v);
+  overflow = !skip && (need_u > a.box_u || need_v > a.box_v);
+  const double du0 = a.cu - u0, dv0 = a.cv - v0;
+  vc.Dx = (float)t.Dx;
+  vc.Dz = (float)t.Dz;
+  vc.D0 = (float)t.D0;
+  vc.Nx = (float)(t.Ux + du0 * t.Dx);
+  vc.Nz = (float)(t.Uz + du0 * t.Dz);
+  vc.N0 = (float)(t.U0 + du0 * t.D0);
+  vc.Vx = (float)(dv0 * t.Dx);
+  vc.Vz = (float)(dv0 * t.Dz);
+  vc.V0 = (float)(t.G * t.Yc + dv0 * t.D0);
+  vc.wscale = a.inv_scale ? a.inv_scale[k] : 1.0f;
+  vc.skip = skip;
+  return skip;
+}
+
+template <typename T>
+__device__ __forceinline__ float ldv(const T* p);
+template <>
+__device__ __forceinline__ float ldv<float>(const float* p) {
+  return *p;
+}
+template <>
+__device__ __forceinline__ float ldv<__half>(const __half* p) {
+  return __half2float(*p);
+}
+
+template <typename T, int TX, int TZ, int NY, bool KAHAN>
+__global__ void __launch_bounds__(TX* TZ, 1) bp_kernel(const __grid_constant__ CUtensorMap tmap, const BPArgs a) {
+  static_assert(TX % 8 == 0 && TZ % 4 == 0, "warp tile is 8 x 4 columns");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  // columns: warp covers 8 (x) x 4 (z)
+  constexpr int WX = TX / 8;
+  const int tx = (warp % WX) * 8 + (lane & 7);
+  const int tz = (warp / WX) * 4 + (lane >> 3);
+  const int bx = blockIdx.x % a.ntx, bz = blockIdx.x / a.ntx;
+  const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
+  const int ex = min(TX, a.nx - ix0) - 1, ez = min(TZ, a.nz - iz0) - 1, ey = min(NY, a.ny - iy0) - 1;
+
+  unsigned char* stage_base[2] = {smem, smem + (size_t)a.chunk * a.box_bytes};
+  ViewCoef* coef = reinterpret_cast<ViewCoef*>(smem + 2 * (size_t)a.chunk * a.box_bytes);  // [2][kMaxChunk]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(coef + 2 * kMaxChunk);
+  int& s_abort = *reinterpret_cast<int*>(bars + 2);
+
+  if (tid == 0) {
+    s_abort = *(volatile int*)a.err != 0;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (s_abort) return;
+
+  const int nchunks = (a.nviews + a.chunk - 1) / a.chunk;
+  const uint32_t tx_bytes = (uint32_t)a.tx_bytes;
+
+  // producer: warp 0 fills stage st with chunk ch
+  auto produce = [&](int ch, int st) {
+    const int k = ch * a.chunk + lane;
+    const bool active = lane < a.chunk && k < a.nviews;
+    ViewCoef vc;
+    int u0 = 0, v0 = 0;
+    bool skip = true, overflow = false, behind = false;
+    if (active) skip = tile_view_coef(a, k, ix0, iy0, iz0, ex, ey, ez, vc, u0, v0, overflow, behind);
+    if (lane < a.chunk) {
+      if (!active) vc.skip = 1;
+      coef[st * kMaxChunk + lane] = vc;
+    }
+    if (active && overflow) atomicCAS(a.err, 0, kDevFootprint);
+    if (active && behind) atomicCAS(a.err, 0, kDevGeometry);
+    const unsigned issue = __ballot_sync(0xffffffffu, active && !skip);
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(&bars[st], __popc(issue) * tx_bytes);
+    __syncwarp();
+    if (active && !skip) {
+      void* dst = stage_base[st] + (size_t)lane * a.box_bytes;
+      if (a.sino_layout)
+        tma_load_3d(dst, &tmap, u0, k, v0, &bars[st]);
+      else
+        tma_load_3d(dst, &tmap, u0, v0, k, &bars[st]);
+    }
+  };
+
+  if (warp == 0) produce(0, 0);
+
+  float acc[NY];
+  float comp[NY];
+#pragma unroll
+  for (int j = 0; j < NY; ++j) {
+    acc[j] = 0.f;
+    comp[j] = 0.f;
+  }
+  const float fx = (float)tx, fz = (float)tz;
+  const int BU = a.box_u, BV = a.box_v;
+
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int st = ch & 1;
+    if (warp == 0 && ch + 1 < nchunks) produce(ch + 1, st ^ 1);
+    if (!mbar_wait(&bars[st], (ch >> 1) & 1, a.err)) {
+      s_abort = 1;
+    }
+    float part[NY];
+#pragma unroll
+    for (int j = 0; j < NY; ++j) part[j] = 0.f;
+    const int nv_chunk = min(a.chunk, a.nviews - ch * a.chunk);
+    for (int vi = 0; vi < nv_chunk; ++vi) {
+      const ViewCoef g = coef[st * kMaxChunk + vi];
+      if (g.skip) continue;
+      const T* win = reinterpret_cast<const T*>(stage_base[st] + (size_t)vi * a.box_bytes);
+      const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
+      const float rD = __frcp_rn(D);
+      const float ul = fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)) * rD;
+      const float vl = fmaf(g.Vx, fx, fmaf(g.Vz, fz, g.V0)) * rD;
+      const float dvv = a.dvn * rD;
+      const float W = rD * rD * g.wscale;
+      const float fuf = floorf(ul);
+      const float fu = ul - fuf;
+      const int iu = min(max((int)fuf, 0), BU - 2);
+      const float wa = W - W * fu, wb = W * fu;
+      const T* col = win + iu;
+#pragma unroll
+      for (int j = 0; j < NY; ++j) {
+        const float v = fmaf((float)j, dvv, vl);
+        const float fvf = floorf(v);
+        const float fv = v - fvf;
+        const int iv = min(max((int)fvf, 0), BV - 2);
+        const T* p = col + iv * BU;
+        const float r0 = fmaf(wb, ldv(p + 1), wa * ldv(p));
+        const float r1 = fmaf(wb, ldv(p + BU + 1), wa * ldv(p + BU));
+        part[j] += fmaf(fv, r1 - r0, r0);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NY; ++j) {
+      if (KAHAN) {
+        const float y = part[j] - comp[j];
+        const float t = acc[j] + y;
+        comp[j] = (t - acc[j]) - y;
+        acc[j] = t;
+      } else {
+        acc[j] += part[j];
+      }
+    }
+    __syncthreads();  // stage st fully consumed before warp 0 refills it
+    if (s_abort) {
+      // leave only after the copy already issued into the other stage lands
+      if (ch + 1 < nchunks) mbar_wait(&bars[st ^ 1], ((ch + 1) >> 1) & 1, a.err);
+      return;
+    }
+  }
+
+  const int ix = ix0 + tx, iz = iz0 + tz;
+  if (ix < a.nx && iz < a.nz) {
+    float* out = a.vol + ((size_t)iz * a.ny) * a.nx + ix;
+#pragma unroll
+    for (int j = 0; j < NY; ++j) {
+      const int iy = iy0 + j;
+      if (iy < a.ny) {
+        float r = acc[j] * a.scale;
+        if (iy < a.clip_ylimit) r = fmaxf(r, 0.f);
+        out[(size_t)iy * a.nx] = r;
+      }
+    }
+  }
+}
+
+// Footprint pre-pass: for every (tile, view) the window each tile needs,
+// max-reduced into spans[0] (u) and spans[1] (v). Uses the same FP64 code as
+// the backprojector, so the chosen window always fits.
+template <int TX, int TZ, int NY>
+__global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
+  const long long total = (long long)a.ntx * a.ntz * nty * a.nviews;
+  int mu = 0, mv = 0;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(w % a.nviews);
+    long long t = w / a.nviews;
+    const int by = (int)(t % nty);
+    t /= nty;
+    const int bx = (int)(t % a.ntx), bz = (int)(t / a.ntx);
+    const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = by * NY;
+    const int ex = min(TX, a.nx - ix0) - 1, ez = min(TZ, a.nz - iz0) - 1, ey = min(NY, a.ny - iy0) - 1;
+    TileGeo g;
+    tile_geo(a, k, ix0, iy0, iz0, ex, ey, ez, g);
+    if (g.dmin <= 1e-6) atomicCAS(a.err, 0, kDevGeometry);
+    if (tile_skip(a, g)) continue;
+    int u0, v0, need_u, need_v;
+    tile_window(a, g, u0, v0, need_u, need_v);
+    mu = max(mu, need_u);
+    mv = max(mv, need_v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = max(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(spans, mu);
+    atomicMax(spans + 1, mv);
+  }
+}
+
+__global__ void clip_kernel(float* vol, int nx, int ny, int nz, int ylim) {
+  const long long total = (long long)nx * ny * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long iy = (e / nx) % ny;
+    if (iy < ylim) vol[e] = fmaxf(vol[e], 0.f);
+  }
+}
+
+// Fan (flat detector) -> parallel rebinning; see the C ABI comment.
+__global__ void rebin_fan_kernel(const float* fan, int bins, int views, double sod, double sdd, double du,
+                                 double span, double offset, float* par, int out_bins, double du_out) {
+  const long long total = (long long)views * out_bins;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int k = (int)(e / out_bins), j = (int)(e % out_bins);
+    double th = offset + span * k / views;
+    double s = (j + 0.5 - out_bins / 2.0) * du_out;
+    float val = 0.f;
+    if (fabs(s) < sod) {
+      double gam = asin(s / sod);
+      double beta = th - gam;
+      double ui = sdd * tan(gam) / du + bins / 2.0 - 0.5;
+      double bi = (beta - offset) / (span / views);
+      double bf = floor(bi), ab = bi - bf;
+      long long b0 = (long long)bf;
+      double fu = floor(ui), au = ui - fu;
+      long long iu = (long long)fu;
+      double acc = 0.0;
+      for (int t = 0; t < 2; ++t) {
+        long long bb = (((b0 + t) % views) + views) % views;
+        const float* row = fan + bb * bins;
+        double p0 = (iu >= 0 && iu < bins) ? row[iu] : 0.0;
+        double p1 = (iu + 1 >= 0 && iu + 1 < bins) ? row[iu + 1] : 0.0;
+        double r = p0 * (1 - au) + p1 * au;
+        acc += t ? r * ab : r * (1 - ab);
+      }
+      val = (float)acc;
+    }
+    par[e] = val;
+  }
+}
+
+struct Config {
+  int tx, tz, ny;
+};
+
+template <typename T, int TX, int TZ, int NY, bool KAHAN>
+cudaError_t launch_cfg(const CUtensorMap& map, const BPArgs& a, size_t smem, cudaStream_t stream) {
+  auto kern = bp_kernel<T, TX, TZ, NY, KAHAN>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(a.ntx * a.ntz, (a.ny + NY - 1) / NY);
+  kern<<<grid, TX * TZ, smem, stream>>>(map, a);
+  return cudaGetLastError();
+}
+
+template <typename T, int TX, int TZ, int NY>
+cudaError_t launch_typed(const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
+  return kahan ? launch_cfg<T, TX, TZ, NY, true>(map, a, smem, stream)
+               : launch_cfg<T, TX, TZ, NY, false>(map, a, smem, stream);
+}
+
+}  // namespace
+
+int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit, bool kahan) {
+  const bool f16 = st.state == kFilteredF16;
+  const int esize = f16 ? 2 : 4;
+  BPArgs a{};
+  a.vol = vol;
+  a.nx = g.nx;
+  a.ny = g.ny;
+  a.nz = g.nz;
+  a.nu = g.nu;
+  a.nv = g.nv;
+  a.nviews = g.nviews;
+  a.kind = g.kind;
+  a.sod = g.sod;
+  a.sdd = g.sdd;
+  a.du = g.du;
+  a.dv = g.dv;
+  a.vox = g.vox;
+  a.cu = 0.5 * g.nu - 0.5;
+  a.cv = 0.5 * g.nv - 0.5;
+  const double pi = 3.14159265358979323846;
+  if (g.kind == FBP_GEOMETRY_CONE) {
+    a.dvn = (float)(g.sdd / (g.sod * g.dv) * g.vox);
+    a.scale = (float)(pi / g.nviews * g.sdd / (g.sod * g.du));
+  } else {
+    a.dvn = (float)(g.vox / g.dv);
+    a.scale = (float)(pi / g.nviews / g.du);
+  }
+  a.inv_scale = f16 ? st.inv_scale : nullptr;
+  a.align = f16 ? 8 : 4;
+  a.sino_layout = st.sinogram ? 1 : 0;
+  a.clip_ylimit = clip_ylimit;
+  a.err = ctx->d_err;
+
+  // per-view trig in FP64
+  if (ctx->trig_cap < g.nviews) {
+    cudaFree(ctx->d_trig);
+    ctx->d_trig = nullptr;
+    ctx->trig_cap = 0;
+    ctx->trig_key[0] = -1;
+    if (cuda_check(ctx, cudaMalloc(&ctx->d_trig, sizeof(double2) * g.nviews), "cudaMalloc(trig)"))
+      return FBP_ERR_OUT_OF_MEMORY;
+    ctx->trig_cap = g.nviews;
+  }
+  const bool trig_same = ctx->trig_key[0] == g.nviews && ctx->trig_key[1] == g.span && ctx->trig_key[2] == g.offset;
+  if (!trig_same) {
+    size_t need = sizeof(double2) * g.nviews;
+    if (ctx->h_pinned_bytes < need) {
+      cudaFreeHost(ctx->h_pinned);
+      ctx->h_pinned = nullptr;
+      ctx->h_pinned_bytes = 0;
+      if (cuda_check(ctx, cudaMallocHost(&ctx->h_pinned, need), "cudaMallocHost")) return FBP_ERR_OUT_OF_MEMORY;
+      ctx->h_pinned_bytes = need;
+    }
+    // the pinned buffer may still be read by an earlier copy on this stream
+    if (int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync before trig upload")) return rc;
+    double2* h = static_cast<double2*>(ctx->h_pinned);
+    for (int k = 0; k < g.nviews; ++k) {
+      double th = g.offset + g.span * k / g.nviews;
+      h[k] = make_double2(cos(th), sin(th));
+    }
+    if (int rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_trig, h, need, cudaMemcpyHostToDevice, ctx->stream),
+                            "trig upload"))
+      return rc;
+    ctx->trig_key[0] = g.nviews;
+    ctx->trig_key[1] = g.span;
+    ctx->trig_key[2] = g.offset;
+  }
+  a.trig = ctx->d_trig;
+
+  // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
+  const bool is2d = g.ny == 1;
+  const int TX = 16, TZ = 16, NY = is2d ? 1 : 16;
+  a.ntx = (g.nx + TX - 1) / TX;
+  a.ntz = (g.nz + TZ - 1) / TZ;
+  const int nty = (g.ny + NY - 1) / NY;
+
+  // footprint pre-pass (cached per geometry)
+  double key[16] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
+                    (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz,
+                    (double)a.align, (double)NY};
+  bool hit = ctx->plan.valid;
+  for (int i = 0; i < 16 && hit; ++i) hit = ctx->plan.key[i] == key[i];
+  if (!hit) {
+    if (!ctx->d_span && cuda_check(ctx, cudaMalloc(&ctx->d_span, 4 * sizeof(int)), "cudaMalloc(span)"))
+      return FBP_ERR_OUT_OF_MEMORY;
+    cudaMemsetAsync(ctx->d_span, 0, 4 * sizeof(int), ctx->stream);
+    long long total = (long long)a.ntx * a.ntz * nty * g.nviews;
+    int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 32);
+    if (is2d)
+      footprint_kernel<16, 16, 1><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
+    else
+      footprint_kernel<16, 16, 16><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
+    int spans[4] = {0, 0, 0, 0};
+    if (int rc = cuda_check(ctx, cudaGetLastError(), "footprint_kernel")) return rc;
+    if (int rc = cuda_check(ctx, cudaMemcpyAsync(spans, ctx->d_span, sizeof(spans), cudaMemcpyDeviceToHost,
+                                                 ctx->stream),
+                            "footprint readback"))
+      return rc;
+    if (int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync")) return rc;
+    int bu = std::max(spans[0], 2), bv = std::max(spans[1], 2);
+    bu = (bu + a.align - 1) / a.align * a.align;
+    ctx->plan.valid = true;
+    for (int i = 0; i < 16; ++i) ctx->plan.key[i] = key[i];
+    ctx->plan.box_u = bu;
+    ctx->plan.box_v = bv;
+  }
+  a.box_u = ctx->plan.box_u;
+  a.box_v = ctx->plan.box_v;
+  if (a.box_u > 256 || a.box_v > 256)
+    return set_error(ctx, FBP_ERR_UNSUPPORTED,
+                     "detector footprint of a 16x16x16 voxel tile exceeds 256 samples; geometry magnification too "
+                     "large for the staged backprojector");
+  a.tx_bytes = a.box_u * a.box_v * esize;
+  a.box_bytes = (a.tx_bytes + 127) / 128 * 128;
+  const size_t smem_cap = 227 * 1024 - 1024;
+  const size_t fixed = sizeof(ViewCoef) * 2 * kMaxChunk + 2 * sizeof(uint64_t) + 64;
+  int chunk = kMaxChunk;
+  while (chunk > 1 && 2 * (size_t)chunk * a.box_bytes + fixed > smem_cap) chunk >>= 1;
+  if (2 * (size_t)chunk * a.box_bytes + fixed > smem_cap)
+    return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
+  a.chunk = chunk;
+  const size_t smem = 2 * (size_t)chunk * a.box_bytes + fixed;
+
+  // tensor map over the filtered stack
+  CUtensorMap map;
+  uint64_t dims[3], strides[2];
+  uint32_t box[3];
+  void* base;
+  const uint64_t pitch_bytes = (uint64_t)(f16 ? st.pitch16 : st.pitch) * esize;
+  base = f16 ? (void*)st.f16 : (void*)st.f32;
+  if (st.sinogram) {  // [v][view][u]
+    dims[0] = st.u;
+    dims[1] = st.n;
+    dims[2] = st.v;
+    strides[0] = pitch_bytes;
+    strides[1] = pitch_bytes * st.n;
+    box[0] = a.box_u;
+    box[1] = 1;
+    box[2] = a.box_v;
+  } else {  // [view][v][u]
+    dims[0] = st.u;
+    dims[1] = st.v;
+    dims[2] = st.n;
+    strides[0] = pitch_bytes;
+    strides[1] = pitch_bytes * st.v;
+    box[0] = a.box_u;
+    box[1] = a.box_v;
+    box[2] = 1;
+  }
+  if (int rc = make_tensor_map_3d(ctx, &map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                  base, dims, strides, box))
+    return rc;
+
+  cudaError_t e;
+  if (is2d) {
+    e = f16 ? launch_typed<__half, 16, 16, 1>(map, a, smem, kahan, ctx->stream)
+            : launch_typed<float, 16, 16, 1>(map, a, smem, kahan, ctx->stream);
+  } else {
+    e = f16 ? launch_typed<__half, 16, 16, 16>(map, a, smem, kahan, ctx->stream)
+            : launch_typed<float, 16, 16, 16>(map, a, smem, kahan, ctx->stream);
+  }
+  return cuda_check(ctx, e, "bp_kernel");
+}
+
+int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit) {
+  long long total = (long long)nx * ny * nz;
+  int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
+  if (total == 0) return FBP_OK;
+  clip_kernel<<<blocks, 256, 0, ctx->stream>>>(vol, nx, ny, nz, y_limit);
+  return cuda_check(ctx, cudaGetLastError(), "clip_kernel");
+}
+
+int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g, float* par,
+                     int out_bins, double du_out) {
+  long long total = (long long)views * out_bins;
+  if (total == 0) return FBP_OK;
+  int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
+  rebin_fan_kernel<<<blocks, 256, 0, ctx->stream>>>(fan, bins, views, g.sod, g.sdd, g.du, g.span, g.offset, par,
+                                                    out_bins, du_out);
+  return cuda_check(ctx, cudaGetLastError(), "rebin_fan_kernel");
+}
+
+}  // namespace fbp

@@ -1,0 +1,456 @@
+// Detector-row filtering: FDK cosine weight + ramp-type filter.
+//
+// Replaces the reference's per-view chain (FBP3D::apply_filter_to_projections,
+// Source/FilteredBackProjection/FBP3D.cpp:389-414): load, real->complex blit,
+// pad, FFFT::fft (radix-2 over texture rows, FastFourierTransformGPU.cpp:3-52),
+// fft_shift, FBP2D::apply_filter (FBP2D.cpp:124-144), inverse shift, inverse
+// FFT (conj-FFT-conj-divide, FastFourierTransformGPU.cpp:30-36), blit, store:
+// ~45 full-texture passes per view. Here one kernel reads each row once and
+// writes it once.
+//
+// Algorithm: two real rows are packed as the real and imaginary parts of one
+// complex row (the filter response H is real and even, so the filtered rows
+// come back as the real and imaginary parts). Forward transform is a
+// decimation-in-frequency radix-2 FFT (natural order in, bit-reversed out),
+// the spectrum is multiplied by H[bitrev(k)]/n, and the inverse is a
+// decimation-in-time radix-2 FFT (bit-reversed in, natural order out), so no
+// bit-reversal permutation is ever executed. Row padding to n samples is the
+// reference's (next power of two >= width, FastFourierTransformGPU.cpp:258-262).
+//
+// The filter response and the spatial kernel are generated on the GPU in
+// FP64 from the band-limited ramp kernel (h(0) = 1/4, h(odd k) = -1/(pi k)^2,
+// Kak & Slaney eq. 3.61) wrapped onto the n-point circle, times the window.
+
+#include "fbp_internal.h"
+
+#include <cmath>
+#include <cstdio>
+
+namespace fbp {
+namespace {
+
+__device__ __forceinline__ double ramp_tap(long long k) {
+  if (k == 0) return 0.25;
+  if ((k & 1) == 0) return 0.0;
+  const double pi = 3.14159265358979323846;
+  double kk = (double)k;
+  return -1.0 / (pi * pi * kk * kk);
+}
+
+__device__ __forceinline__ double filter_window(int filter, double f) {
+  const double pi = 3.14159265358979323846;
+  switch (filter) {
+    case FBP_FILTER_SHEPP_LOGAN:
+      return f == 0.0 ? 1.0 : sin(pi * f) / (pi * f);
+    case FBP_FILTER_COSINE:
+      return cospi(f);
+    case FBP_FILTER_HANN:
+      return 0.5 * (1.0 + cospi(2.0 * f));
+    default:
+      return 1.0;
+  }
+}
+
+// H[k] for k < n (one thread per k), FP64.
+__global__ void response_kernel(int n, int filter, double* H) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  long long kk = k <= n / 2 ? k : (long long)k - n;
+  double f = fabs((double)kk) / n;
+  if (filter == FBP_FILTER_RAMP_SAMPLED) {
+    H[k] = f;
+    return;
+  }
+  double s = 0.25;  // j = 0 term (cos 0 = 1)
+  for (int j = 1; j < n; j += 2) {
+    long long jj = j <= n / 2 ? j : (long long)j - n;
+    long long p = ((long long)j * k) % n;
+    s += ramp_tap(jj) * cospi(2.0 * (double)p / n);
+  }
+  H[k] = s * filter_window(filter, f);
+}
+
+// From H: hbr (bit-reversed, divided by n), twiddles, spatial kernel g.
+__global__ void tables_kernel(int n, int log2n, const double* H, float* hbr, float2* tw, float* g) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  unsigned r = __brev((unsigned)k) >> (32 - log2n);
+  hbr[k] = (float)(H[r] / n);
+  if (k < n / 2) {
+    double s, c;
+    sincospi(-2.0 * (double)k / n, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+  double acc = 0.0;
+  for (int j = 0; j < n; j++) {
+    long long p = ((long long)j * k) % n;
+    acc += H[j] * cospi(2.0 * (double)p / n);
+  }
+  g[k] = (float)(acc / n);
+}
+
+__global__ void twiddle_kernel(int n, float2* tw) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n / 2) return;
+  double s, c;
+  sincospi(-2.0 * (double)k / n, &s, &c);
+  tw[k] = make_float2((float)c, (float)s);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+struct FilterKArgs {
+  RowSet rs;
+  int n, log2n, pairs_per_cta;
+  long long npairs;
+  const float2* tw;
+  const float* hbr;
+};
+
+__device__ __forceinline__ float load_pre(const RowSet& rs, long long r, int i) {
+  float x = rs.data[r * rs.pitch + i];
+  if (rs.log_norm) {
+    float y = fmaxf(x, 1e-30f * rs.log_base);
+    x = -logf(y / rs.log_base);
+  }
+  if (rs.weight) {
+    int iv = rs.sinogram ? (int)(r / rs.n_views) : (int)(r % rs.n_v);
+    float u = (i + 0.5f - 0.5f * rs.m) * rs.w_du;
+    float v = (iv + 0.5f - 0.5f * rs.n_v) * rs.w_dv;
+    x *= rs.w_sdd * rsqrtf(rs.w_sdd * rs.w_sdd + u * u + v * v);
+  }
+  return x;
+}
+
+__device__ __forceinline__ int row_view(const RowSet& rs, long long r) {
+  return rs.sinogram ? (int)(r % rs.n_views) : (int)(r / rs.n_v);
+}
+
+// One CTA filters `pairs_per_cta` row pairs per iteration, grid-stride.
+__global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = a.n, half = n >> 1;
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float* hb = reinterpret_cast<float*>(tw + half);
+  float2* buf = reinterpret_cast<float2*>(hb + n);
+  for (int i = threadIdx.x; i < half; i += blockDim.x) tw[i] = a.tw[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) hb[i] = a.hbr[i];
+  const RowSet& rs = a.rs;
+  const int P = a.pairs_per_cta;
+  const long long ngroups = (a.npairs + P - 1) / P;
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();
+    // load P pairs: real part row 2p, imaginary part row 2p + 1, zero padded
+    for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
+      int p = idx / n, i = idx - p * n;
+      long long pr = grp * P + p;
+      float re = 0.f, im = 0.f;
+      if (pr < a.npairs && i < rs.m) {
+        long long r0 = 2 * pr;
+        re = load_pre(rs, r0, i);
+        if (r0 + 1 < rs.rows) im = load_pre(rs, r0 + 1, i);
+      }
+      buf[idx] = make_float2(re, im);
+    }
+    __syncthreads();
+    // forward DIF
+    for (int lh = a.log2n - 1; lh >= 0; --lh) {
+      const int h = 1 << lh;
+      const int tsh = a.log2n - 1 - lh;  // twiddle stride n/(2h) = 2^tsh
+      for (int b = threadIdx.x; b < P * half; b += blockDim.x) {
+        int p = b >> (a.log2n - 1), q = b & (half - 1);
+        int j = q & (h - 1), blk = q >> lh;
+        float2* d = buf + p * n + (blk << (lh + 1)) + j;
+        float2 x0 = d[0], x1 = d[h];
+        d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
+        d[h] = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), tw[j << tsh]);
+      }
+      __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
+      float hv = hb[idx & (n - 1)];
+      float2 x = buf[idx];
+      buf[idx] = make_float2(x.x * hv, x.y * hv);
+    }
+    __syncthreads();
+    // inverse DIT
+    for (int lh = 0; lh < a.log2n; ++lh) {
+      const int h = 1 << lh;
+      const int tsh = a.log2n - 1 - lh;
+      for (int b = threadIdx.x; b < P * half; b += blockDim.x) {
+        int p = b >> (a.log2n - 1), q = b & (half - 1);
+        int j = q & (h - 1), blk = q >> lh;
+        float2* d = buf + p * n + (blk << (lh + 1)) + j;
+        float2 x0 = d[0];
+        float2 x1 = cmulc(d[h], tw[j << tsh]);
+        d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
+        d[h] = make_float2(x0.x - x1.x, x0.y - x1.y);
+      }
+      __syncthreads();
+    }
+    // store
+    for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
+      int p = idx / n, i = idx - p * n;
+      long long pr = grp * P + p;
+      if (pr >= a.npairs || i >= rs.m) continue;
+      float2 y = buf[idx];
+      long long r0 = 2 * pr;
+      if (rs.out16) {
+        rs.out16[r0 * rs.pitch16 + i] = __float2half_rn(y.x * rs.view_scale[row_view(rs, r0)]);
+        if (r0 + 1 < rs.rows)
+          rs.out16[(r0 + 1) * rs.pitch16 + i] = __float2half_rn(y.y * rs.view_scale[row_view(rs, r0 + 1)]);
+      } else {
+        rs.data[r0 * rs.pitch + i] = y.x;
+        if (r0 + 1 < rs.rows) rs.data[(r0 + 1) * rs.pitch + i] = y.y;
+      }
+    }
+  }
+}
+
+__global__ void elementwise_pre_kernel(RowSet rs) {
+  long long total = rs.rows * (long long)rs.m;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e / rs.m;
+    int i = (int)(e - r * rs.m);
+    rs.data[r * rs.pitch + i] = load_pre(rs, r, i);
+  }
+}
+
+// Per-view max |pre-processed sample| (as float bits: non-negative floats
+// order like integers).
+__global__ void view_absmax_kernel(RowSet rs, unsigned* vmax) {
+  long long total = rs.rows * (long long)rs.m;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e / rs.m;
+    int i = (int)(e - r * rs.m);
+    float x = fabsf(load_pre(rs, r, i));
+    if (x > 0.f) atomicMax(vmax + row_view(rs, r), __float_as_uint(x));
+  }
+}
+
+// scale = largest power of two with scale * bound <= 2^15, bound = L1 norm of
+// the filter kernel times the view's max |input|; that bounds every filtered
+// value, so FP16 (max 65504) cannot overflow.
+__global__ void view_scale_kernel(const unsigned* vmax, int nviews, const float* l1, float* scale, float* inv) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nviews) return;
+  float bound = __uint_as_float(vmax[k]) * (*l1);
+  float s = 1.f;
+  if (bound > 0.f && isfinite(bound)) {
+    int e = (int)floorf(log2f(32768.f / bound));
+    e = max(-100, min(100, e));
+    s = ldexpf(1.f, e);
+  }
+  scale[k] = s;
+  inv[k] = 1.f / s;
+}
+
+__global__ void l1_kernel(const float* g, int n, float* out) {
+  __shared__ float red[256];
+  float s = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += fabsf(g[i]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// Natural-order complex FFT of rows (FFFT::fft_radix2 / inverse_fft_radix2,
+// FastFourierTransformGPU.cpp:3-36): inverse = conj, FFT, conj, divide by n.
+__global__ void __launch_bounds__(256) fft_rows_kernel(float2* data, int n, int log2n, int rows,
+                                                       int inverse, const float2* twg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int half = n >> 1;
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* buf = tw + half;
+  for (int i = threadIdx.x; i < half; i += blockDim.x) tw[i] = twg[i];
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    __syncthreads();
+    float2* row = data + (long long)r * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      float2 x = row[i];
+      if (inverse) x.y = -x.y;
+      buf[i] = x;
+    }
+    __syncthreads();
+    for (int lh = log2n - 1; lh >= 0; --lh) {
+      const int h = 1 << lh, tsh = log2n - 1 - lh;
+      for (int q = threadIdx.x; q < half; q += blockDim.x) {
+        int j = q & (h - 1), blk = q >> lh;
+        float2* d = buf + (blk << (lh + 1)) + j;
+        float2 x0 = d[0], x1 = d[h];
+        d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
+        d[h] = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), tw[j << tsh]);
+      }
+      __syncthreads();
+    }
+    const float sc = inverse ? 1.f / n : 1.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      unsigned br = __brev((unsigned)i) >> (32 - log2n);
+      float2 x = buf[br];
+      if (inverse) x = make_float2(x.x * sc, -x.y * sc);
+      row[i] = x;
+    }
+  }
+}
+
+// out[(i + s) mod n] = in[i] per row (FFFT::fft_shift, FastFourierTransformGPU.cpp:93-142).
+__global__ void fft_shift_kernel(float2* data, int n, int rows, int shift) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* buf = reinterpret_cast<float2*>(smem_raw);
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    __syncthreads();
+    float2* row = data + (long long)r * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = row[i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      int j = (int)((((long long)i + shift) % n + n) % n);
+      row[j] = buf[i];
+    }
+  }
+}
+
+__global__ void f16_to_f32_kernel(const __half* src, long long pitch16, const float* inv_scale, int n_views,
+                                  int n_v, bool sinogram, long long row0, long long nrows, int m, float* dst,
+                                  long long dpitch) {
+  long long total = nrows * m;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e / m;
+    int i = (int)(e - r * m);
+    long long gr = row0 + r;
+    int view = sinogram ? (int)(gr % n_views) : (int)(gr / n_v);
+    dst[r * dpitch + i] = __half2float(src[gr * pitch16 + i]) * inv_scale[view];
+  }
+}
+
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
+int grid_for(fbp_context* ctx, long long work, int per_block) {
+  long long b = (work + per_block - 1) / per_block;
+  long long cap = (long long)ctx->num_sms * 16;
+  return (int)std::max(1LL, std::min(b, cap));
+}
+
+}  // namespace
+
+int ensure_filter_tables(fbp_context* ctx, int n, int filter) {
+  FilterTables& t = ctx->ftab;
+  if (t.n == n && t.filter == filter) return FBP_OK;
+  if (n < 2 || (n & (n - 1)) || n > 8192)
+    return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "filter length must be a power of two in [2, 8192]");
+  if (filter < 0 || filter > FBP_FILTER_RAMP_SAMPLED)
+    return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
+  if (t.n != n) {
+    cudaFree(t.twiddle);
+    cudaFree(t.hbr);
+    cudaFree(t.kernel);
+    t.twiddle = nullptr;
+    t.hbr = nullptr;
+    t.kernel = nullptr;
+    t.n = 0;
+    if (cuda_check(ctx, cudaMalloc(&t.twiddle, sizeof(float2) * (n / 2 + 1)), "cudaMalloc(twiddle)") ||
+        cuda_check(ctx, cudaMalloc(&t.hbr, sizeof(float) * n), "cudaMalloc(hbr)") ||
+        cuda_check(ctx, cudaMalloc(&t.kernel, sizeof(float) * n), "cudaMalloc(kernel)"))
+      return FBP_ERR_OUT_OF_MEMORY;
+  }
+  double* H = static_cast<double*>(scratch(ctx, sizeof(double) * n));
+  if (!H) return FBP_ERR_OUT_OF_MEMORY;
+  int blocks = (n + 127) / 128;
+  response_kernel<<<blocks, 128, 0, ctx->stream>>>(n, filter, H);
+  tables_kernel<<<blocks, 128, 0, ctx->stream>>>(n, ilog2(n), H, t.hbr, t.twiddle, t.kernel);
+  if (int rc = cuda_check(ctx, cudaGetLastError(), "filter tables")) return rc;
+  t.n = n;
+  t.filter = filter;
+  return FBP_OK;
+}
+
+int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n) {
+  if (n < rs.m) return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length smaller than the row");
+  if (n > 4096) return set_error(ctx, FBP_ERR_UNSUPPORTED, "FFT filter supports padded lengths up to 4096");
+  if (rs.rows == 0) return FBP_OK;
+  FilterKArgs a;
+  a.rs = rs;
+  a.n = n;
+  a.log2n = ilog2(n);
+  a.pairs_per_cta = std::max(1, std::min(8, 4096 / n));
+  a.npairs = (rs.rows + 1) / 2;
+  a.tw = ctx->ftab.twiddle;
+  a.hbr = ctx->ftab.hbr;
+  size_t smem = sizeof(float2) * (n / 2) + sizeof(float) * n + sizeof(float2) * n * a.pairs_per_cta;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    attr_set = true;
+  }
+  long long groups = (a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta;
+  int grid = (int)std::min<long long>(groups, (long long)ctx->num_sms * 4);
+  filter_fft_kernel<<<grid, 256, smem, ctx->stream>>>(a);
+  return cuda_check(ctx, cudaGetLastError(), "filter_fft_kernel");
+}
+
+int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs) {
+  if (rs.rows == 0) return FBP_OK;
+  elementwise_pre_kernel<<<grid_for(ctx, rs.rows * rs.m, 256), 256, 0, ctx->stream>>>(rs);
+  return cuda_check(ctx, cudaGetLastError(), "elementwise_pre_kernel");
+}
+
+int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale) {
+  unsigned* vmax = static_cast<unsigned*>(scratch(ctx, sizeof(unsigned) * rs.n_views + 64));
+  if (!vmax) return FBP_ERR_OUT_OF_MEMORY;
+  float* l1 = reinterpret_cast<float*>(vmax + rs.n_views);
+  if (int rc = cuda_check(ctx, cudaMemsetAsync(vmax, 0, sizeof(unsigned) * rs.n_views, ctx->stream), "memset"))
+    return rc;
+  view_absmax_kernel<<<grid_for(ctx, rs.rows * rs.m, 256), 256, 0, ctx->stream>>>(rs, vmax);
+  l1_kernel<<<1, 256, 0, ctx->stream>>>(ctx->ftab.kernel, ctx->ftab.n, l1);
+  view_scale_kernel<<<(rs.n_views + 127) / 128, 128, 0, ctx->stream>>>(vmax, rs.n_views, l1, view_scale, inv_scale);
+  return cuda_check(ctx, cudaGetLastError(), "view scale kernels");
+}
+
+int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse) {
+  if (n < 2 || (n & (n - 1)) || n > 8192)
+    return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "FFT length must be a power of two in [2, 8192]");
+  if (rows <= 0) return FBP_OK;
+  // twiddles for n (independent of the filter tables' n)
+  float2* tw = static_cast<float2*>(scratch(ctx, sizeof(float2) * (n / 2)));
+  if (!tw) return FBP_ERR_OUT_OF_MEMORY;
+  twiddle_kernel<<<(n / 2 + 127) / 128, 128, 0, ctx->stream>>>(n, tw);
+  size_t smem = sizeof(float2) * (n / 2 + n);
+  cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  fft_rows_kernel<<<std::min(rows, ctx->num_sms * 4), 256, smem, ctx->stream>>>(data, n, ilog2(n), rows, inverse,
+                                                                                 tw);
+  return cuda_check(ctx, cudaGetLastError(), "fft_rows_kernel");
+}
+
+int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift) {
+  if (n <= 0 || n > 8192) return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "row length must be in [1, 8192]");
+  if (rows <= 0) return FBP_OK;
+  cudaFuncSetAttribute(fft_shift_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  fft_shift_kernel<<<std::min(rows, ctx->num_sms * 4), 256, sizeof(float2) * n, ctx->stream>>>(data, n, rows,
+                                                                                                shift);
+  return cuda_check(ctx, cudaGetLastError(), "fft_shift_kernel");
+}
+
+int launch_f16_to_f32(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst,
+                      long long dst_pitch) {
+  if (nrows == 0) return FBP_OK;
+  f16_to_f32_kernel<<<grid_for(ctx, (long long)nrows * s.u, 256), 256, 0, ctx->stream>>>(
+      s.f16, s.pitch16, s.inv_scale, s.n, s.v, s.sinogram, (long long)row0, (long long)nrows, s.u, dst, dst_pitch);
+  return cuda_check(ctx, cudaGetLastError(), "f16_to_f32_kernel");
+}
+
+}  // namespace fbp

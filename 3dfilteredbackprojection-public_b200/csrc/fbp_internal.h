@@ -1,0 +1,161 @@
+// Internal declarations shared by the CUDA translation units of libfbp_b200.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fbp_b200.h"
+
+namespace fbp {
+
+// Device-side error codes written to the context's error word.
+enum DeviceError : int {
+  kDevOk = 0,
+  kDevTimeout = 1,    // an mbarrier / flag wait ran out of iterations
+  kDevFootprint = 2,  // a staged detector window was smaller than a tile's footprint
+  kDevGeometry = 3,   // a voxel lies at or behind the source plane
+};
+
+// State of a stack of detector rows (projections or sinograms).
+enum StackState : int {
+  kRawF32 = 0,       // f32 holds the data
+  kFilteredF32 = 1,  // f32 holds filtered rows
+  kFilteredF16 = 2,  // f16 + inv_scale hold filtered rows; f32 is stale
+};
+
+// A stack of detector rows. Projections are [view][v][u] (rows ordered view
+// major), sinograms [v][view][u] (rows ordered v major). Rows of u samples
+// are padded to `pitch` elements so that every row starts 16-byte aligned.
+struct Stack {
+  float* f32 = nullptr;
+  __half* f16 = nullptr;
+  float* inv_scale = nullptr;  // per view, multiplies the f16 values
+  int u = 0, v = 0, n = 0;
+  int pitch = 0;    // f32 row pitch in elements (multiple of 4)
+  int pitch16 = 0;  // f16 row pitch in elements (multiple of 8)
+  bool sinogram = false;
+  int state = kRawF32;
+  // Log normalisation and FDK weights recorded by their calls and applied
+  // inside the filter kernel's load (log first, then weight), or by a
+  // standalone pass when something else reads the rows first.
+  bool log_pending = false;
+  double log_base = 1.0;
+  bool weights_pending = false;
+  double w_sdd = 0, w_du = 0, w_dv = 0;
+  size_t rows() const { return (size_t)v * n; }
+  size_t bytes32() const { return (size_t)pitch * rows() * sizeof(float); }
+  size_t bytes16() const { return (size_t)pitch16 * rows() * sizeof(__half); }
+  // row r -> detector row index iv and view index
+  int row_v(size_t r) const { return sinogram ? (int)(r / n) : (int)(r % v); }
+};
+
+struct FilterTables {
+  int n = 0, filter = -1;
+  float2* twiddle = nullptr;  // n/2 entries exp(-2 pi i k / n)
+  float* hbr = nullptr;       // n entries H[bitrev(k)] / n
+  float* kernel = nullptr;    // n entries: spatial kernel g = IDFT(H) (circular)
+};
+
+}  // namespace fbp
+
+struct fbp_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int precision = FBP_PRECISION_FP32;
+  int filter_impl = FBP_FILTER_IMPL_AUTO;
+  int pad_len = 0;
+  int clip_after_bp = 1;
+  int num_sms = 148;
+
+  float* vol = nullptr;
+  int vx = 0, vy = 0, vz = 0;
+
+  fbp::Stack proj;
+  fbp::Stack sino;
+
+  int* d_err = nullptr;          // device error word
+  double2* d_trig = nullptr;     // per-view (cos, sin) in FP64
+  int trig_cap = 0;
+  double trig_key[3] = {-1, 0, 0};  // (views, span, offset) of the table in d_trig
+  int* d_span = nullptr;         // footprint pre-pass results
+  fbp::FilterTables ftab;
+  void* d_scratch = nullptr;     // generic scratch (row shifts, Toeplitz operands)
+  size_t scratch_bytes = 0;
+  void* h_pinned = nullptr;      // small pinned staging for per-call tables
+  size_t h_pinned_bytes = 0;
+
+  // cached footprint plan
+  struct BPPlan {
+    bool valid = false;
+    double key[16] = {0};
+    int box_u = 0, box_v = 0;
+  } plan;
+};
+
+namespace fbp {
+
+// ---- error helpers (fbp_api.cu) ----
+int set_error(fbp_context* ctx, int code, const std::string& msg);
+int cuda_check(fbp_context* ctx, cudaError_t e, const char* what);
+void* scratch(fbp_context* ctx, size_t bytes);
+
+// ---- filter (fbp_filter.cu) ----
+struct RowSet {
+  float* data;          // f32 rows (input; also output when out16 == nullptr)
+  long long pitch;      // elements
+  long long rows;
+  int m;                // samples per row
+  // row -> (view, iv) for weights and per-view scales
+  int n_views, n_v;
+  bool sinogram;        // rows ordered v-major
+  // optional fused pre-ops
+  bool log_norm = false;
+  float log_base = 1.f;
+  bool weight = false;
+  float w_sdd = 0, w_du = 0, w_dv = 0;
+  // optional FP16 output
+  __half* out16 = nullptr;
+  long long pitch16 = 0;
+  const float* view_scale = nullptr;  // values are multiplied by it before rounding to FP16
+};
+int ensure_filter_tables(fbp_context* ctx, int n, int filter);
+int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n);
+int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter);
+int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs);  // weight / log-norm only
+int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale);
+int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse);
+int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift);
+int launch_f16_to_f32(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst, long long dst_pitch);
+bool toeplitz_supported(int m);
+
+// ---- backprojection (fbp_backproject.cu) ----
+struct BPGeom {
+  int kind;           // FBP_GEOMETRY_CONE / FBP_GEOMETRY_PARALLEL
+  double sod, sdd;    // cone only
+  double du, dv, vox;
+  double span, offset;
+  int nu, nv, nviews;
+  int nx, ny, nz;
+};
+int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit,
+                       bool kahan);
+int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit);
+int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g,
+                     float* par, int out_bins, double du_out);
+
+// ---- phantoms (fbp_phantom.cu) ----
+int launch_project_ellipsoids(fbp_context* ctx, const double* d_ell, int count, const BPGeom& g,
+                              float* out, int pitch);
+
+// ---- TMA helpers ----
+int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
+                       const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]);
+
+}  // namespace fbp

@@ -1,0 +1,214 @@
+/*
+ * fbp_b200.h - C ABI of the B200 CT reconstruction core (FDK cone-beam,
+ * 3D parallel-beam, 2D parallel-beam and 2D flat-detector fan-beam FBP).
+ *
+ * Every entry point returns an int status (FBP_OK == 0) and never aborts;
+ * fbp_last_error() gives the message of the last failure. Pointers passed in
+ * are borrowed for the duration of the call only. A context owns its device
+ * buffers (volume, projections, sinograms) the way class FBP3D owns its
+ * textures (reference Source/FilteredBackProjection/FBP3D.h:87-89), is bound
+ * to one CUDA device and one stream, and must be used from one host thread
+ * at a time.
+ *
+ * Reference citations are paths inside furkanunsal42/3DFilteredBackProjection-Public.
+ *
+ * Conventions: volume buffers are x-fastest [z][y][x] with y the rotation
+ * axis (reference Texture3D(h, v, h), FBP3D.cpp:531); projection stacks are
+ * [view][v][u] (Texture2DArray(u, v, N), FBP3D.cpp:40); sinogram stacks are
+ * [v][view][u] (Texture3D(u, N, v), FBP3D.cpp:54); 2D sinograms are
+ * [view][bin] and 2D images [row][column].
+ */
+#ifndef FBP_B200_H
+#define FBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define FBP_OK 0
+#define FBP_ERR_INVALID_ARGUMENT (-1)
+#define FBP_ERR_STATE (-2)        /* required buffer missing; the reference prints and ASSERTs (FBP3D.cpp:214-217) */
+#define FBP_ERR_CUDA (-3)
+#define FBP_ERR_OUT_OF_MEMORY (-4)
+#define FBP_ERR_DEVICE_TIMEOUT (-5) /* a bounded device-side wait expired */
+#define FBP_ERR_UNSUPPORTED (-6)
+#define FBP_ERR_DEVICE_CHECK (-7)   /* a device-side bounds / footprint check failed */
+
+/* ---- filter types: 0..2 keep the values of FBP2D::FilterType (FBP2D.h:10-14) */
+#define FBP_FILTER_RAM_LAK 0
+#define FBP_FILTER_SHEPP_LOGAN 1
+#define FBP_FILTER_COSINE 2
+#define FBP_FILTER_HANN 3
+#define FBP_FILTER_RAMP_SAMPLED 4 /* |k|/n sampled in frequency (FastFourierTransformImage.cpp:35,45) */
+
+/* ---- precision forms ------------------------------------------------------ */
+/* FP32: FP32 FFT filter, FP32 filtered views, FP32 accumulation.           */
+/* MIXED: split-BF16 tensor-core Toeplitz filter (FP32 accumulate), FP16    */
+/*        filtered views with a per-view power-of-two scale, Kahan-          */
+/*        compensated FP32 accumulation over view chunks.                    */
+#define FBP_PRECISION_FP32 0
+#define FBP_PRECISION_MIXED 1
+
+/* ---- filter implementations ---------------------------------------------- */
+#define FBP_FILTER_IMPL_AUTO 0     /* FFT for FP32, Toeplitz GEMM for MIXED */
+#define FBP_FILTER_IMPL_FFT 1      /* batched shared-memory FFT             */
+#define FBP_FILTER_IMPL_TOEPLITZ 2 /* tcgen05 split-BF16 Toeplitz GEMM       */
+
+/* ---- geometry kinds ------------------------------------------------------- */
+#define FBP_GEOMETRY_CONE 0     /* flat-panel cone beam, circular orbit         */
+#define FBP_GEOMETRY_PARALLEL 1 /* parallel beam (3D: stacked 2D)               */
+
+typedef struct fbp_context fbp_context;
+
+/* Geometry of one backprojection, in the reference's terms
+ * (FBP3D.h:58, FBP3D.cpp:536-552). Lengths in any unit (mm in the tests).
+ *   source_distance    source to rotation axis (xray_source_distance, SOD)
+ *   detector_distance  rotation axis to detector (detector_panel_distance);
+ *                      SDD = source_distance + detector_distance
+ *   detector_width     width of the nu detector columns; pixels are square
+ *   volume_width       width of the nx voxels; voxels are isotropic
+ *   views cover angles offset + 2*pi*full_rotation_count*k/K, k < K.
+ * For FBP_GEOMETRY_PARALLEL the two distances are ignored. */
+typedef struct fbp_geometry {
+  int kind;
+  float source_distance;
+  float detector_distance;
+  float detector_width;
+  float volume_width;
+  float full_rotation_count;
+  float rotation_offset_radian;
+} fbp_geometry;
+
+/* ---- context ---------------------------------------------------------------
+ * Replaces the FBP3D object (FBP3D.h:16-20): fbp_create ~ FBP3D(), which in
+ * the reference compiles ~40 compute shaders in member initialisers. */
+int fbp_create(fbp_context** ctx, int device);
+int fbp_destroy(fbp_context* ctx);
+/* Last error message of ctx (or of the calling thread when ctx is NULL). */
+const char* fbp_last_error(const fbp_context* ctx);
+/* Run all work of ctx on this cudaStream_t (NULL: the context's own stream). */
+int fbp_set_stream(fbp_context* ctx, void* cuda_stream);
+int fbp_synchronize(fbp_context* ctx);
+int fbp_set_precision(fbp_context* ctx, int precision);
+int fbp_set_filter_impl(fbp_context* ctx, int impl);
+/* Padding of detector rows before filtering: 0 = the reference's next power
+ * of two >= width (FastFourierTransformGPU.cpp:258-262, circular wrap-around
+ * included), otherwise an explicit power of two >= width. */
+int fbp_set_filter_padding(fbp_context* ctx, int padded_length);
+/* 1 (default): project_backward_* end with clip_negatives_of_volume as the
+ * reference does (FBP3D.cpp:489,521,558,592); 0: leave negatives. */
+int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable);
+/* Device bytes held by ctx's buffers. */
+int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
+
+/* ---- buffers (FBP3D.cpp:16-56, 197-210) ----------------------------------- */
+int fbp_generate_blank_volume(fbp_context* ctx, int x_size, int y_size, int z_size);
+int fbp_generate_blank_projections(fbp_context* ctx, int x_size, int y_size, int projection_amount);
+int fbp_generate_blank_sinograms(fbp_context* ctx, int x_size, int y_size, int projection_amount);
+int fbp_free_volume(fbp_context* ctx);
+int fbp_free_projections(fbp_context* ctx);
+int fbp_free_sinograms(fbp_context* ctx);
+int fbp_get_volume_size(const fbp_context* ctx, int* x, int* y, int* z);
+int fbp_get_projections_size(const fbp_context* ctx, int* u, int* v, int* count);
+
+/* ---- transfers --------------------------------------------------------------
+ * `*_on_device` = 1: the pointer is device memory of ctx's device, else host
+ * memory (pinned memory gives asynchronous copies). Host-memory transfers
+ * are complete when the call returns. */
+/* Whole stack [view][v][u]; (re)allocates the projections. Replaces the
+ * per-batch upload + store_projection loop of read_projections
+ * (FBP3D.cpp:105-118). */
+int fbp_upload_projections(fbp_context* ctx, const float* src, int u, int v, int count, int src_on_device);
+/* Whole stack [v][view][u]; (re)allocates the sinograms (FBP3D.cpp:126-176). */
+int fbp_upload_sinograms(fbp_context* ctx, const float* src, int u, int v, int count, int src_on_device);
+int fbp_download_projections(fbp_context* ctx, float* dst, int dst_on_device);
+int fbp_download_sinograms(fbp_context* ctx, float* dst, int dst_on_device);
+int fbp_store_projection(fbp_context* ctx, const float* src, int projection_index, int src_on_device); /* FBP3D.cpp:718-728 */
+int fbp_load_projection(fbp_context* ctx, int projection_index, float* dst, int dst_on_device);      /* FBP3D.cpp:706-716 */
+int fbp_store_sinogram(fbp_context* ctx, const float* src, int y_index, int src_on_device);           /* FBP3D.cpp:742-753 */
+int fbp_load_sinogram(fbp_context* ctx, int y_index, float* dst, int dst_on_device);                  /* FBP3D.cpp:730-740 */
+/* Slices of the volume: x-slice is [z][y], y-slice [z][x], z-slice [y][x]
+ * (FBP3D.cpp:639-704). */
+int fbp_load_volume_slice_x(fbp_context* ctx, int x_index, float* dst, int dst_on_device);
+int fbp_load_volume_slice_y(fbp_context* ctx, int y_index, float* dst, int dst_on_device);
+int fbp_load_volume_slice_z(fbp_context* ctx, int z_index, float* dst, int dst_on_device);
+int fbp_store_volume_slice_x(fbp_context* ctx, const float* src, int x_index, int src_on_device);
+int fbp_store_volume_slice_y(fbp_context* ctx, const float* src, int y_index, int src_on_device);
+int fbp_store_volume_slice_z(fbp_context* ctx, const float* src, int z_index, int src_on_device);
+/* Whole volume [z][y][x] (replaces the per-y-slice readback of write_volume,
+ * FBP3D.cpp:178-195, without the file output). */
+int fbp_read_volume(fbp_context* ctx, float* dst, int dst_on_device);
+int fbp_write_volume_data(fbp_context* ctx, const float* src, int src_on_device);
+/* Device pointers of ctx's buffers (valid until the buffer is reallocated or
+ * freed). Projections may be row-padded: *row_pitch is in floats. */
+int fbp_volume_device_ptr(fbp_context* ctx, float** ptr);
+int fbp_projections_device_ptr(fbp_context* ctx, float** ptr, int* row_pitch);
+
+/* ---- pipeline stages (FBP3D.cpp) ------------------------------------------- */
+int fbp_log_normalize_projections(fbp_context* ctx, float base_value);                                 /* :333-349 */
+int fbp_log_normalize_sinograms(fbp_context* ctx, float base_value);                                   /* :351-367 */
+int fbp_apply_fdk_weights_to_projections(fbp_context* ctx, float xray_source_distance,
+                                         float detector_panel_distance, float detector_width);         /* :369-387 */
+int fbp_apply_fdk_weights_to_sinograms(fbp_context* ctx, float xray_source_distance,
+                                       float detector_panel_distance, float detector_width);           /* FBP3D.h:53 */
+int fbp_apply_filter_to_projections(fbp_context* ctx, int filter_type);                               /* :389-414 */
+int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type);                                 /* :417-442 */
+int fbp_clip_negatives_of_volume(fbp_context* ctx);                                                    /* :444-458 */
+int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float xray_source_distance,
+    float detector_panel_distance, float detector_width, float volume_width, float full_rotation_count,
+    int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :524-559 */
+int fbp_project_backward_cone_fdk_from_sinograms(fbp_context* ctx, float xray_source_distance,
+    float detector_panel_distance, float detector_width, float volume_width, float full_rotation_count,
+    int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :561-593 */
+int fbp_project_backward_parallel_from_projections(fbp_context* ctx, float full_rotation_count,
+    int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :460-490 */
+int fbp_project_backward_parallel_from_sinograms(fbp_context* ctx, float full_rotation_count,
+    int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :492-522 */
+/* One call for the whole cone-beam FDK (weight + filter + backprojection +
+ * optional clip) on the resident projections, geometry as above. */
+int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* geometry, int filter_type,
+                        int volume_resolution_horizontal, int volume_resolution_vertical);
+
+/* ---- 2D (FBP2D.h:17-41) on caller-owned device buffers ---------------------
+ * sinogram [views][bins], image [rows][cols]; filtered in place. */
+/* Weight (fan: SDD/sqrt(SDD^2+u^2)) and filter every row; fan_sdd <= 0 means
+ * parallel beam (no weight). Combines FBP2D::apply_filter on the shifted
+ * spectrum with the surrounding FFFT calls (Mains/fbp_parallel2d_main.cpp:31-41). */
+int fbp2d_filter_sinogram(fbp_context* ctx, float* sinogram, int bins, int views, int filter_type,
+                          float fan_sdd, float detector_width);
+/* 2D backprojection (FBP2D.cpp:96-122 for parallel beam; flat-detector fan
+ * beam for FBP_GEOMETRY_CONE). image has cols x rows = nx x nz pixels of
+ * size volume_width/nx. */
+int fbp2d_project_backward(fbp_context* ctx, const float* sinogram, int bins, int views,
+                           const fbp_geometry* geometry, float* image, int nx, int nz);
+/* Fan (flat detector) -> parallel sinogram rebinning (FBP2D.cpp:31-52).
+ * Output has out_bins bins of pitch out_detector_width/out_bins and the same
+ * number of views. */
+int fbp2d_parallelize_fan_beam_sinogram(fbp_context* ctx, const float* fan, int bins, int views,
+                                        const fbp_geometry* geometry, float* parallel, int out_bins,
+                                        float out_detector_width);
+
+/* ---- GPU FFT over rows (FastFourierTransformGPU.h:13-48) -------------------
+ * Interleaved complex64 rows [rows][n], n a power of two <= 4096. */
+int fbp_fft_rows(fbp_context* ctx, float* complex_rows, int n, int rows, int inverse);
+int fbp_fft_shift_rows(fbp_context* ctx, float* complex_rows, int n, int rows, int shift_amount);
+
+/* ---- analytic phantom projections (test/bench input generator) -------------
+ * Line integrals of ellipsoids (rows of 16 doubles: density, semi-axes a b c,
+ * centre x y z, 3x3 rotation row-major whose columns are the axes) through
+ * the cone geometry, FP64 arithmetic, written as FP32 into the resident
+ * projections (which must already be allocated with u, v, count). Replaces
+ * render_ellipsoid + project_forward_cone_to_projections (FBP3D.cpp:609-628,
+ * 269-299) for generating inputs. */
+int fbp_project_ellipsoids_to_projections(fbp_context* ctx, const double* ellipsoids, int count,
+                                          const fbp_geometry* geometry);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FBP_B200_H */

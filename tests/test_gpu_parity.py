@@ -1,0 +1,314 @@
+"""Parity of the CUDA library (through the C ABI) with the FP64 oracle.
+
+Tolerances (relative RMSE = ||x - oracle|| / ||oracle||):
+  FP32 form:   1e-5 for whole reconstructions, 1e-6 for filtered rows
+  MIXED form:  1e-4 (FP16 filtered views with per-view scale, Kahan sums)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import relative_rmse
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-5
+TOL_ROWS = 1e-6
+TOL_MIXED = 1e-4
+
+
+@pytest.fixture(scope="module")
+def fbp():
+    import build as B
+    B.build()
+    import fbp_b200
+    return fbp_b200
+
+
+@pytest.fixture()
+def solver(fbp):
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    yield s
+    s.ctx.close()
+
+
+def _cone_args(c):
+    return (c["sod"], c["sdd"] - c["sod"], c["nu"] * c["du"], c["nx"] * c["vox"], c["span"] / (2 * math.pi))
+
+
+# ----------------------------------------------------------------- filtering
+@pytest.mark.parametrize("m,filt", [(367, 0), (384, 1), (768, 2), (1536, 3), (512, 0), (100, 4)])
+def test_filter_rows_fp32(solver, oracle, m, filt):
+    rng = np.random.default_rng(m + filt)
+    proj = (rng.standard_normal((5, 7, m)) + 2.0).astype(np.float32)
+    solver.upload_projections(proj)
+    solver.apply_filter_to_projections(filt)
+    got = solver.download_projections()
+    ref = oracle.filter_rows(proj.astype(np.float64).reshape(-1, m), filt).reshape(proj.shape)
+    assert relative_rmse(got, ref) < TOL_ROWS
+
+
+def test_fdk_weight_fused_into_filter(solver, oracle):
+    rng = np.random.default_rng(3)
+    proj = rng.random((4, 6, 384)).astype(np.float32)
+    sod, odd, w = 750.0, 450.0, 614.4
+    solver.upload_projections(proj)
+    solver.apply_fdk_weights_to_projections(sod, odd, w)
+    solver.apply_filter_to_projections(0)
+    got = solver.download_projections()
+    du = w / 384
+    # the detector has 6 rows here: v pitch = u pitch (square pixels)
+    pw = oracle.fdk_weight(proj, sod + odd, du, du)
+    ref = oracle.filter_rows(pw.reshape(-1, 384), 0).reshape(proj.shape)
+    assert relative_rmse(got, ref) < TOL_ROWS
+
+
+def test_weights_alone_are_materialized_on_read(solver, oracle):
+    rng = np.random.default_rng(4)
+    proj = rng.random((3, 5, 64)).astype(np.float32)
+    solver.upload_projections(proj)
+    solver.apply_fdk_weights_to_projections(100.0, 50.0, 64.0)
+    got = solver.load_projection(1)
+    ref = oracle.fdk_weight(proj, 150.0, 1.0, 1.0)[1]
+    assert np.abs(got - ref).max() < 1e-6 * np.abs(ref).max()
+
+
+def test_log_normalize_then_weight_then_filter(solver, oracle):
+    rng = np.random.default_rng(6)
+    proj = (0.2 + rng.random((3, 4, 128))).astype(np.float32)
+    base = 97.0 / 255
+    solver.upload_projections(proj)
+    solver.log_normalize_projections(base)
+    solver.apply_fdk_weights_to_projections(400.0, 400.0, 128.0)
+    solver.apply_filter_to_projections(1)
+    got = solver.download_projections()
+    p = oracle.log_normalize(proj, base)
+    p = oracle.fdk_weight(p, 800.0, 1.0, 1.0)
+    ref = oracle.filter_rows(p.reshape(-1, 128), 1).reshape(proj.shape)
+    assert relative_rmse(got, ref) < TOL_ROWS
+
+
+def test_explicit_padding(solver, oracle):
+    rng = np.random.default_rng(8)
+    proj = rng.standard_normal((2, 3, 300)).astype(np.float32)
+    solver.set_filter_padding(1024)
+    solver.upload_projections(proj)
+    solver.apply_filter_to_projections(0)
+    got = solver.download_projections()
+    ref = oracle.filter_rows(proj.astype(np.float64).reshape(-1, 300), 0, n=1024).reshape(proj.shape)
+    assert relative_rmse(got, ref) < TOL_ROWS
+
+
+# ------------------------------------------------------------ reconstructions
+def _cone_case(phantoms, oracle, factor):
+    c = phantoms.scaled_cone(phantoms.config_cone256(), factor)
+    E = phantoms.ellipsoids_for(c)
+    return c, oracle.project_ellipsoids_cone(E, c)
+
+
+def _gpu_fdk(solver, c, proj, filt):
+    sod, odd, w, vw, rot = _cone_args(c)
+    solver.upload_projections(proj)
+    solver.apply_fdk_weights_to_projections(sod, odd, w)
+    solver.apply_filter_to_projections(filt)
+    solver.project_backward_cone_fdk_from_projections(sod, odd, w, vw, rot, c["nx"], c["ny"], c["offset"])
+    return solver.read_volume()
+
+
+@pytest.mark.parametrize("factor", [4, 2])
+def test_cone_fdk_fp32(solver, oracle, phantoms, factor):
+    c, proj = _cone_case(phantoms, oracle, factor)
+    got = _gpu_fdk(solver, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    assert relative_rmse(got, ref) < TOL_FP32
+
+
+def test_cone256_fdk_fp32_full_size(solver, oracle, phantoms):
+    """256^3, 360 views, 384^2 detector: every voxel against the oracle."""
+    c = phantoms.config_cone256()
+    proj = oracle.project_ellipsoids_cone(phantoms.ellipsoids_for(c), c)
+    got = _gpu_fdk(solver, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    err = relative_rmse(got, ref)
+    print(f"cone256 FP32 rel RMSE {err:.3e} max abs {np.abs(got - ref).max():.3e}")
+    assert err < TOL_FP32
+
+
+def test_cone_non_cubic_and_offset(solver, oracle):
+    """ny != nx, an odd detector width, a rotation offset, views over 1.5 turns."""
+    c = dict(sod=300.0, sdd=520.0, du=1.3, dv=1.3, span=3 * math.pi, offset=0.37, nu=97, nv=61, nviews=75,
+             nx=40, ny=23, nz=40, vox=1.9)
+    rng = np.random.default_rng(11)
+    proj = rng.random((c["nviews"], c["nv"], c["nu"])).astype(np.float32)
+    got = _gpu_fdk(solver, c, proj, 2)
+    ref = oracle.fdk(proj, c, 2)
+    assert relative_rmse(got, ref) < TOL_FP32
+
+
+def test_clip_matches_reference_extent(solver, oracle):
+    """clip_negatives clips y-slices below the z size (FBP3D.cpp:448)."""
+    c = dict(sod=300.0, sdd=500.0, du=1.0, dv=1.0, span=2 * math.pi, offset=0.0, nu=64, nv=64, nviews=40,
+             nx=24, ny=40, nz=24, vox=1.5)
+    rng = np.random.default_rng(12)
+    proj = rng.standard_normal((c["nviews"], c["nv"], c["nu"])).astype(np.float32)
+    solver.set_clip_after_backprojection(True)
+    got = _gpu_fdk(solver, c, proj, 0)
+    ref = oracle.clip_negatives(oracle.fdk(proj, c, 0), y_limit=c["nz"])
+    assert relative_rmse(got, ref) < TOL_FP32
+    assert (got[:, c["nz"]:, :] < 0).any()  # slices y >= z are not clipped
+    assert (got[:, : c["nz"], :] >= 0).all()
+
+
+def test_sinogram_layout_equals_projection_layout(fbp, solver, oracle, phantoms):
+    c, proj = _cone_case(phantoms, oracle, 4)
+    sod, odd, w, vw, rot = _cone_args(c)
+    a = _gpu_fdk(solver, c, proj, 0)
+    s2 = fbp.FBP3D(0)
+    s2.set_clip_after_backprojection(False)
+    s2.upload_sinograms(np.ascontiguousarray(proj.transpose(1, 0, 2)))
+    s2.apply_fdk_weights_to_sinograms(sod, odd, w)
+    s2.apply_filter_to_sinograms(0)
+    s2.project_backward_cone_fdk_from_sinograms(sod, odd, w, vw, rot, c["nx"], c["ny"], 0.0)
+    b = s2.read_volume()
+    assert relative_rmse(b, a) < 1e-6
+
+
+def test_parallel3d(solver, oracle):
+    rng = np.random.default_rng(13)
+    n, nv, nu, h, v = 60, 20, 48, 48, 20
+    proj = rng.standard_normal((n, nv, nu)).astype(np.float32)
+    solver.upload_projections(proj)
+    solver.apply_filter_to_projections(0)
+    solver.project_backward_parallel_from_projections(0.5, h, v, 0.1)
+    got = solver.read_volume()
+    q = oracle.filter_rows(proj.astype(np.float64).reshape(-1, nu), 0).reshape(proj.shape)
+    ref = oracle.bp_parallel3d(q, dict(du=h / nu, dv=v / nv, span=math.pi, offset=0.1, nx=h, ny=v, nz=h, vox=1.0))
+    assert relative_rmse(got, ref) < TOL_FP32
+
+
+def test_parallel2d_config(fbp, oracle, phantoms):
+    c = phantoms.config_parallel2d()
+    sino = oracle.project_ellipses_parallel2d(phantoms.ellipses_for(c), c["nu"], c["nviews"], c["du"], c["span"])
+    f2 = fbp.FBP2D(0)
+    filt = f2.apply_filter(sino, 0)
+    g = fbp.Geometry.parallel(c["nu"] * c["du"], c["nx"] * c["vox"], 0.5, 0.0)
+    img = f2.project_backward(filt, g, (c["nx"], c["nz"]))
+    ref = oracle.fbp_parallel2d(sino, c, 0)
+    assert relative_rmse(img, ref) < TOL_FP32
+
+
+def test_fan2d_config(fbp, oracle, phantoms):
+    c = phantoms.config_fan2d()
+    E = phantoms.ellipses_for(c)
+    sino = oracle.project_ellipses_fan2d(E, c["nu"], c["nviews"], c["sod"], c["sdd"], c["du"], c["span"])
+    sino = phantoms.poisson_log(sino, c["i0"], np.random.default_rng(c["seed"]))
+    f2 = fbp.FBP2D(0)
+    filt = f2.apply_filter(sino, 1, fan_sdd=c["sdd"], detector_width=c["nu"] * c["du"])
+    g = fbp.Geometry.cone(c["sod"], c["sdd"] - c["sod"], c["nu"] * c["du"], c["nx"] * c["vox"], 1.0, 0.0)
+    img = f2.project_backward(filt, g, (c["nx"], c["nz"]))
+    ref = oracle.fbp_fan2d(sino, c, 1)
+    assert relative_rmse(img, ref) < TOL_FP32
+
+
+def test_fan_rebinning(fbp, oracle):
+    E = np.array([[1.0, 40.0, 25.0, 10.0, -5.0, 0.3]])
+    sod, sdd = 500.0, 1000.0
+    fan = oracle.project_ellipses_fan2d(E, 512, 720, sod, sdd, 0.5, 2 * np.pi)
+    f2 = fbp.FBP2D(0)
+    g = fbp.Geometry.cone(sod, sdd - sod, 256.0, 128.0, 1.0, 0.0)
+    par = f2.parallelize_fan_beam_sinogram(fan, g, 256, 128.0)
+    ref = oracle.rebin_fan_to_parallel(fan, dict(sod=sod, sdd=sdd, du=0.5, span=2 * np.pi, offset=0.0), 256, 0.5)
+    assert relative_rmse(par, ref) < 1e-6
+
+
+# ------------------------------------------------------------ mixed precision
+def test_mixed_precision_cone(fbp, oracle, phantoms):
+    c, proj = _cone_case(phantoms, oracle, 2)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED)
+    got = _gpu_fdk(s, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    err = relative_rmse(got, ref)
+    print(f"mixed cone128 rel RMSE {err:.3e}")
+    assert err < TOL_MIXED
+
+
+# ----------------------------------------------------------- API behaviour
+def test_state_errors(fbp):
+    s = fbp.FBP3D(0)
+    with pytest.raises(fbp.FBPError) as e:
+        s.project_backward_cone_fdk_from_projections(400, 400, 100, 100, 1, 16, 16, 0)
+    assert e.value.status == -2 and "not allocated" in str(e.value)
+    s.generate_blank_projections(8, 8, 4)
+    with pytest.raises(fbp.FBPError) as e:
+        s.load_projection(4)
+    assert e.value.status == -1
+    with pytest.raises(fbp.FBPError):
+        s.apply_filter_to_projections(17)
+
+
+def test_blank_buffers_are_cleared_and_sized(solver):
+    solver.generate_blank_projections(10, 6, 3)
+    assert solver.projections_size() == (10, 6, 3)
+    assert not solver.download_projections().any()
+    solver.generate_blank_volume(5, 7, 9)
+    assert solver.volume_size() == (5, 7, 9)
+    assert not solver.read_volume().any()
+
+
+def test_store_load_projection_roundtrip(solver):
+    rng = np.random.default_rng(14)
+    solver.generate_blank_projections(33, 9, 5)
+    img = rng.standard_normal((9, 33)).astype(np.float32)
+    solver.store_projection(img, 3)
+    assert np.array_equal(solver.load_projection(3), img)
+    assert not solver.load_projection(2).any()
+
+
+def test_volume_slices(solver):
+    rng = np.random.default_rng(15)
+    vol = rng.standard_normal((6, 5, 7)).astype(np.float32)  # [z][y][x]
+    solver.generate_blank_volume(7, 5, 6)
+    solver.write_volume_data(vol)
+    assert np.array_equal(solver.load_volume_slice_y(2), vol[:, 2, :])
+    assert np.array_equal(solver.load_volume_slice_z(4), vol[4])
+    assert np.array_equal(solver.load_volume_slice_x(3), vol[:, :, 3])
+    sl = rng.standard_normal((6, 7)).astype(np.float32)
+    solver.store_volume_slice_y(sl, 1)
+    vol[:, 1, :] = sl
+    assert np.array_equal(solver.read_volume(), vol)
+
+
+def test_deterministic(solver, oracle, phantoms):
+    c, proj = _cone_case(phantoms, oracle, 4)
+    a = _gpu_fdk(solver, c, proj, 0)
+    b = _gpu_fdk(solver, c, proj, 0)
+    assert np.array_equal(a, b)
+
+
+def test_gpu_ellipsoid_projector(fbp, oracle, phantoms):
+    c = phantoms.scaled_cone(phantoms.config_cone1440(), 8)
+    E = phantoms.ellipsoids_for(c)
+    s = fbp.FBP3D(0)
+    s.generate_blank_projections(c["nu"], c["nv"], c["nviews"])
+    args = phantoms.geometry_args(c)
+    s.project_ellipsoids(E, fbp.Geometry.cone(args["sod"], args["odd"], args["detector_width"],
+                                              args["volume_width"], args["full_rotation_count"], 0.0))
+    got = s.download_projections()
+    ref = oracle.project_ellipsoids_cone(E, c)
+    assert relative_rmse(got, ref) < 1e-6
+
+
+def test_fft_rows_mirror(fbp):
+    rng = np.random.default_rng(16)
+    z = (rng.standard_normal((5, 256)) + 1j * rng.standard_normal((5, 256))).astype(np.complex64)
+    f = fbp.FFFT(0)
+    assert np.abs(f.fft_radix2(z) - np.fft.fft(z, axis=1)).max() < 1e-4 * np.abs(z).sum() / 5
+    assert np.allclose(f.inverse_fft_radix2(f.fft_radix2(z)), z, atol=1e-5)
+    assert np.array_equal(f.fft_shift(z), np.roll(z, 128, axis=1))
+    assert np.array_equal(f.inverse_fft_shift(z, 3), np.roll(z, -3, axis=1))
