@@ -93,7 +93,7 @@ int sync_host(fbp_context* ctx, bool host_involved) {
 
 void free_stack(Stack& s) {
   cudaFree(s.f32);
-  cudaFree(s.f16);
+  cudaFree(s.filt);
   cudaFree(s.inv_scale);
   bool sino = s.sinogram;
   s = Stack();
@@ -104,7 +104,7 @@ int alloc_stack(fbp_context* ctx, Stack& s, int u, int v, int n) {
   if (u <= 0 || v <= 0 || n <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "stack sizes must be positive");
   if (s.f32 && s.u == u && s.v == v && s.n == n) {
     // same size: keep the allocation and clear it (FBP3D.cpp:30-38)
-    s.state = fbp::kRawF32;
+    s.filtered = false;
     s.log_pending = s.weights_pending = false;
     return fbp::cuda_check(ctx, cudaMemsetAsync(s.f32, 0, s.bytes32(), ctx->stream), "clear stack");
   }
@@ -113,7 +113,6 @@ int alloc_stack(fbp_context* ctx, Stack& s, int u, int v, int n) {
   s.v = v;
   s.n = n;
   s.pitch = round_up(u, 4);
-  s.pitch16 = round_up(u, 8);
   cudaError_t e = cudaMalloc(&s.f32, s.bytes32());
   if (e != cudaSuccess) {
     s.f32 = nullptr;
@@ -150,11 +149,12 @@ int flush_pending(fbp_context* ctx, Stack& s) {
   return FBP_OK;
 }
 
-// Bring the data back into f32 (from FP16 filtered storage) and flush.
+// Bring the content back into the f32 rows (from the filtered buffer) and
+// apply anything pending.
 int materialize_f32(fbp_context* ctx, Stack& s) {
-  if (s.state == fbp::kFilteredF16) {
-    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, 0, s.rows(), s.f32, s.pitch));
-    s.state = fbp::kFilteredF32;
+  if (s.filtered) {
+    FBP_TRY(fbp::launch_unpack_rows(ctx, s, 0, s.rows(), s.f32, s.pitch));
+    s.filtered = false;
   }
   return flush_pending(ctx, s);
 }
@@ -190,7 +190,7 @@ int ensure_volume(fbp_context* ctx, int x, int y, int z, bool clear) {
 int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int n, int on_dev) {
   if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
   if (!(s.f32 && s.u == u && s.v == v && s.n == n)) FBP_TRY(alloc_stack(ctx, s, u, v, n));
-  s.state = fbp::kRawF32;
+  s.filtered = false;
   s.log_pending = s.weights_pending = false;
   FBP_TRY(fbp::cuda_check(ctx,
                           cudaMemcpy2DAsync(s.f32, (size_t)s.pitch * 4, src, (size_t)u * 4, (size_t)u * 4,
@@ -202,11 +202,11 @@ int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int
 int download_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, float* dst, int on_dev) {
   if (!dst) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null destination pointer");
   FBP_TRY(flush_pending(ctx, s));
-  if (s.state == fbp::kFilteredF16) {
-    // convert just these rows into a scratch f32 block
+  if (s.filtered) {
+    // unpack just these rows into a scratch f32 block
     float* tmp = static_cast<float*>(fbp::scratch(ctx, sizeof(float) * nrows * s.pitch));
     if (!tmp) return FBP_ERR_OUT_OF_MEMORY;
-    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, row0, nrows, tmp, s.pitch));
+    FBP_TRY(fbp::launch_unpack_rows(ctx, s, row0, nrows, tmp, s.pitch));
     FBP_TRY(fbp::cuda_check(ctx,
                             cudaMemcpy2DAsync(dst, (size_t)s.u * 4, tmp, (size_t)s.pitch * 4, (size_t)s.u * 4, nrows,
                                               kind_of(true, on_dev), ctx->stream),
@@ -230,38 +230,45 @@ int upload_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, const flo
   return sync_host(ctx, !on_dev);
 }
 
-// Run weights / log (pending) + filter on a stack.
+// Run weights / log (pending) + filter on a stack; the result goes to the
+// stack's filtered buffer in the backprojector's pair layout (FP32 pairs for
+// the FP32 form, FP16 pairs with a per-view scale for the MIXED form).
 int filter_stack(fbp_context* ctx, Stack& s, int filter_type) {
   if (filter_type < 0 || filter_type > FBP_FILTER_RAMP_SAMPLED)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
-  if (s.state == fbp::kFilteredF16) {
-    FBP_TRY(fbp::launch_f16_to_f32(ctx, s, 0, s.rows(), s.f32, s.pitch));
-    s.state = fbp::kFilteredF32;
-  }
+  if (s.filtered) FBP_TRY(materialize_f32(ctx, s));  // filtering filtered data
   const int n = ctx->pad_len > 0 ? ctx->pad_len : next_pow2_reference(s.u);
   if (n < s.u || (n & (n - 1)))
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length must be a power of two >= the row width");
   FBP_TRY(fbp::ensure_filter_tables(ctx, n, filter_type));
-  fbp::RowSet rs = rowset_of(s);
   const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  const int layout = mixed ? fbp::kLayoutPair16 : fbp::kLayoutPair32;
+  const int fpitch = round_up(s.u, 4);
+  const size_t need = (size_t)fpitch * s.filt_rows() * Stack::elem_bytes(layout);
+  if (!s.filt || s.filt_bytes < need) {
+    cudaFree(s.filt);
+    s.filt = nullptr;
+    s.filt_bytes = 0;
+    if (fbp::cuda_check(ctx, cudaMalloc(&s.filt, need), "cudaMalloc(filtered views)")) return FBP_ERR_OUT_OF_MEMORY;
+    s.filt_bytes = need;
+  }
+  s.filt_layout = layout;
+  s.filt_pitch = fpitch;
+  fbp::RowSet rs = rowset_of(s);
+  rs.out = s.filt;
+  rs.out_layout = layout;
+  rs.out_pitch = fpitch;
   int impl = ctx->filter_impl;
   if (impl == FBP_FILTER_IMPL_AUTO)
     impl = (mixed && fbp::toeplitz_supported(s.u)) ? FBP_FILTER_IMPL_TOEPLITZ : FBP_FILTER_IMPL_FFT;
   if (mixed) {
-    if (!s.f16) {
-      if (fbp::cuda_check(ctx, cudaMalloc(&s.f16, s.bytes16()), "cudaMalloc(f16 stack)")) {
-        s.f16 = nullptr;
-        return FBP_ERR_OUT_OF_MEMORY;
-      }
-      if (fbp::cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
-        s.inv_scale = nullptr;
-        return FBP_ERR_OUT_OF_MEMORY;
-      }
+    if (!s.inv_scale &&
+        fbp::cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
+      s.inv_scale = nullptr;
+      return FBP_ERR_OUT_OF_MEMORY;
     }
     float* scale = s.inv_scale + s.n;
     FBP_TRY(fbp::launch_view_absmax(ctx, rs, scale, s.inv_scale));
-    rs.out16 = s.f16;
-    rs.pitch16 = s.pitch16;
     rs.view_scale = scale;
   }
   if (impl == FBP_FILTER_IMPL_TOEPLITZ)
@@ -269,7 +276,7 @@ int filter_stack(fbp_context* ctx, Stack& s, int filter_type) {
   else
     FBP_TRY(fbp::launch_filter_fft(ctx, rs, n));
   s.log_pending = s.weights_pending = false;
-  s.state = mixed ? fbp::kFilteredF16 : fbp::kFilteredF32;
+  s.filtered = true;
   return FBP_OK;
 }
 
@@ -277,7 +284,7 @@ int record_weights(fbp_context* ctx, Stack& s, float sod, float odd, float det_w
   FBP_TRY(require_stack(ctx, s, what));
   if (!(sod > 0.f) || !(odd >= 0.f) || !(det_w > 0.f))
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "distances and detector width must be positive");
-  if (s.state == fbp::kFilteredF16) FBP_TRY(materialize_f32(ctx, s));
+  if (s.filtered) FBP_TRY(materialize_f32(ctx, s));
   if (s.weights_pending) FBP_TRY(flush_pending(ctx, s));
   s.weights_pending = true;
   s.w_sdd = (double)sod + (double)odd;
@@ -289,7 +296,7 @@ int record_weights(fbp_context* ctx, Stack& s, float sod, float odd, float det_w
 int record_log(fbp_context* ctx, Stack& s, float base, const char* what) {
   FBP_TRY(require_stack(ctx, s, what));
   if (!(base > 0.f)) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "base_value must be positive");
-  if (s.state == fbp::kFilteredF16) FBP_TRY(materialize_f32(ctx, s));
+  if (s.filtered) FBP_TRY(materialize_f32(ctx, s));
   // log must run before weights; if weights are already pending (or a log
   // is), materialise them first so that the call order is honoured
   if (s.weights_pending || s.log_pending) FBP_TRY(flush_pending(ctx, s));
@@ -519,7 +526,8 @@ int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes) {
   if (ctx->vol) b += sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
   for (const Stack* s : {&ctx->proj, &ctx->sino}) {
     if (s->f32) b += s->bytes32();
-    if (s->f16) b += s->bytes16() + sizeof(float) * 2 * s->n;
+    if (s->filt) b += s->filt_bytes;
+    if (s->inv_scale) b += sizeof(float) * 2 * s->n;
   }
   b += ctx->scratch_bytes;
   *bytes = b;
@@ -816,7 +824,7 @@ static int stage_2d(fbp_context* ctx, const float* sino, int bins, int views, St
   st.v = 1;
   st.n = views;
   st.pitch = round_up(bins, 4);
-  st.state = fbp::kFilteredF32;
+  st.filtered = false;
   char* base = static_cast<char*>(fbp::scratch(ctx, offset_bytes + st.bytes32()));
   if (!base) return FBP_ERR_OUT_OF_MEMORY;
   st.f32 = reinterpret_cast<float*>(base + offset_bytes);
@@ -932,7 +940,7 @@ int fbp_project_ellipsoids_to_projections(fbp_context* ctx, const double* ell, i
   if (count > 0)
     FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(d, ell, sizeof(double) * 16 * count, cudaMemcpyHostToDevice, ctx->stream),
                             "ellipsoid upload"));
-  s.state = fbp::kRawF32;
+  s.filtered = false;
   s.log_pending = s.weights_pending = false;
   FBP_TRY(fbp::launch_project_ellipsoids(ctx, d, count, g, s.f32, s.pitch));
   // the host array is only borrowed for the call

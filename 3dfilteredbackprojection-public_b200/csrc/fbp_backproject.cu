@@ -10,22 +10,25 @@
 //
 // Design (one launch for all views):
 //   * A CTA owns a TX x TZ tile of voxel columns and NY voxels along the
-//     rotation axis (y); each thread owns one column segment of NY voxels and
-//     keeps its NY sums in registers across every view, so the volume is
-//     written exactly once.
-//   * Views are processed in chunks. For every (tile, view) one lane of warp 0
-//     computes, in FP64, the tile's detector footprint and the tile-local
-//     projective coefficients (the tile's rows of the projection matrix,
-//     re-based on the tile corner and on the staged window so that the FP32
-//     detector coordinates the threads form stay small and accurate). The
-//     footprint window (box_u x box_v detector samples) is copied into shared
-//     memory by TMA (cp.async.bulk.tensor, no multicast), double-buffered
-//     through mbarriers; samples outside the detector arrive as zeros from the
-//     TMA out-of-bounds fill.
-//   * Per view a thread forms 1/D, its detector column u (constant along the
-//     column), the distance weight and the v step once, then walks its NY
-//     voxels with one FMA per voxel for v: four shared-memory taps and three
-//     lerps per update.
+//     rotation axis (y); each consumer thread owns one column segment of NY
+//     voxels and keeps its NY sums in registers across every view, so the
+//     volume is written exactly once (clip epilogue fused into the store).
+//   * Warp specialisation: one producer warp computes, in FP64, the tile's
+//     detector footprint and tile-local projective coefficients for 32 views
+//     at a time (one view per lane), re-based on the tile corner and on the
+//     staged window so that the FP32 coordinates the consumers form stay small
+//     and accurate, and copies each view's footprint window (box_u x box_v
+//     elements) into a ring of shared-memory stages with TMA
+//     (cp.async.bulk.tensor, no multicast). Samples outside the detector
+//     arrive as zeros from the TMA out-of-bounds fill. Full / empty mbarriers
+//     per stage replace block barriers; consumer warps never wait for one
+//     another.
+//   * Filtered views are stored in a pair layout (element (v, u) holds rows v
+//     and v + 1), so a bilinear tap is two shared-memory loads (8-byte float2
+//     or 4-byte half2). Per view a consumer thread forms 1/D, its detector
+//     column u (constant along the column), the distance weight and the v
+//     step once; per voxel it steps v with one FMA and takes floor / fraction
+//     with the 1.5 * 2^23 rounding constant (no conversion instructions).
 //   * Every mbarrier wait is bounded; on expiry the CTA records an error and
 //     leaves, and every CTA checks the error word before starting.
 
@@ -38,8 +41,8 @@
 namespace fbp {
 namespace {
 
-constexpr int kMaxChunk = 8;            // views per pipeline stage (upper bound)
-constexpr uint32_t kWaitLimit = 1u << 24;  // mbarrier polls before giving up
+constexpr int kMaxStages = 8;           // shared-memory ring stages (one view each)
+constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
 
 struct ViewCoef {
   float Dx, Dz, D0;  // D = L / SOD (cone) or 1 (parallel), affine in (x', z')
@@ -64,9 +67,10 @@ struct BPArgs {
   int box_u, box_v, align;
   int box_bytes;          // smem bytes reserved per staged window (multiple of 128)
   int tx_bytes;           // bytes one TMA box transfer delivers (box_u * box_v * element)
-  int chunk;              // views per stage
+  int chunk;              // ring stages
   int ntx, ntz;           // tiles along x and z
   int sino_layout;        // tensor coordinates (u, view, v) instead of (u, v, view)
+  int pair_rows;          // 1: an element carries rows v and v + 1 (pair layouts)
   int clip_ylimit;        // clip negatives where iy < clip_ylimit
   int* err;
 };
@@ -198,7 +202,7 @@ __device__ bool tile_view_coef(const BPArgs& a, int k, int ix0, int iy0, int iz0
   const bool skip = tile_skip(a, t);
   int need_u, need_v;
   tile_window(a, t, u0, v0, need_u, need_v);
-  overflow = !skip && (need_u > a.box_u || need_v > a.box_v);
+  overflow = !skip && (need_u > a.box_u || need_v - a.pair_rows > a.box_v);
   const double du0 = a.cu - u0, dv0 = a.cv - v0;
   vc.Dx = (float)t.Dx;
   vc.Dz = (float)t.Dz;
@@ -214,102 +218,165 @@ __device__ bool tile_view_coef(const BPArgs& a, int k, int ix0, int iy0, int iz0
   return skip;
 }
 
-template <typename T>
-__device__ __forceinline__ float ldv(const T* p);
-template <>
-__device__ __forceinline__ float ldv<float>(const float* p) {
-  return *p;
-}
-template <>
-__device__ __forceinline__ float ldv<__half>(const __half* p) {
-  return __half2float(*p);
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <typename T, int TX, int TZ, int NY, bool KAHAN>
-__global__ void __launch_bounds__(TX* TZ, 1) bp_kernel(const __grid_constant__ CUtensorMap tmap, const BPArgs a) {
+__device__ __forceinline__ float lds_f32(uint32_t addr) {
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ __half2 lds_h2(uint32_t addr) {
+  uint32_t v;
+  asm("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return *reinterpret_cast<__half2*>(&v);
+}
+
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: x + kMagic rounds x to an integer
+constexpr uint32_t kMagicBits = 0x4B400000u;
+
+// One bilinear update of voxel j: returns the distance-weighted sample.
+// w = v - 0.5 (v the window-local row coordinate); c0 + bits(w + kMagic) * RB
+// is the address of the element at row floor(v), column iu of the window.
+template <int LAYOUT>
+__device__ __forceinline__ float tap(float w, uint32_t c0, uint32_t RB, float wa, float wb, __half2 fu2, float W) {
+  const float t = w + kMagic;
+  const float fr = w - (t - kMagic);  // v - floor(v) - 0.5, in [-0.5, 0.5]
+  const uint32_t addr = __float_as_uint(t) * RB + c0;
+  if constexpr (LAYOUT == kLayoutRaw32) {
+    const float p00 = lds_f32(addr), p01 = lds_f32(addr + 4);
+    const float p10 = lds_f32(addr + RB), p11 = lds_f32(addr + RB + 4);
+    const float r0 = fmaf(wb, p01, wa * p00);
+    const float r1 = fmaf(wb, p11, wa * p10);
+    const float d = r1 - r0;
+    return fmaf(fr, d, fmaf(0.5f, d, r0));
+  } else if constexpr (LAYOUT == kLayoutPair32) {
+    const float2 X = lds_f32x2(addr), Y = lds_f32x2(addr + 8);  // (p00, p10), (p01, p11)
+    const float r0 = fmaf(wb, Y.x, wa * X.x);
+    const float r1 = fmaf(wb, Y.y, wa * X.y);
+    const float d = r1 - r0;
+    return fmaf(fr, d, fmaf(0.5f, d, r0));
+  } else {
+    const __half2 X = lds_h2(addr), Y = lds_h2(addr + 4);
+    const float2 R = __half22float2(__hfma2(fu2, __hsub2(Y, X), X));  // (row v, row v + 1) lerped in u
+    const float d = R.y - R.x;
+    return W * fmaf(fr, d, fmaf(0.5f, d, R.x));
+  }
+}
+
+template <int LAYOUT, int TX, int TZ, int NY, bool KAHAN>
+__global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constant__ CUtensorMap tmap, const BPArgs a) {
   static_assert(TX % 8 == 0 && TZ % 4 == 0, "warp tile is 8 x 4 columns");
+  constexpr int NCW = TX * TZ / 32;  // consumer warps
+  constexpr int KC = 8;              // views per Kahan fold
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  // columns: warp covers 8 (x) x 4 (z)
-  constexpr int WX = TX / 8;
-  const int tx = (warp % WX) * 8 + (lane & 7);
-  const int tz = (warp / WX) * 4 + (lane >> 3);
+  const int S = a.chunk;  // ring stages (one view each)
   const int bx = blockIdx.x % a.ntx, bz = blockIdx.x / a.ntx;
   const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
-  const int ex = min(TX, a.nx - ix0) - 1, ez = min(TZ, a.nz - iz0) - 1, ey = min(NY, a.ny - iy0) - 1;
 
-  unsigned char* stage_base[2] = {smem, smem + (size_t)a.chunk * a.box_bytes};
-  ViewCoef* coef = reinterpret_cast<ViewCoef*>(smem + 2 * (size_t)a.chunk * a.box_bytes);  // [2][kMaxChunk]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(coef + 2 * kMaxChunk);
-  int& s_abort = *reinterpret_cast<int*>(bars + 2);
+  ViewCoef* coef = reinterpret_cast<ViewCoef*>(smem + (size_t)S * a.box_bytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(coef + S);
+  uint64_t* empty = full + S;
+  volatile int* s_abort = reinterpret_cast<volatile int*>(empty + S);
 
   if (tid == 0) {
-    s_abort = *(volatile int*)a.err != 0;
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    *s_abort = *(volatile int*)a.err != 0;
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NCW);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
-  if (s_abort) return;
+  if (*s_abort) return;
 
-  const int nchunks = (a.nviews + a.chunk - 1) / a.chunk;
-  const uint32_t tx_bytes = (uint32_t)a.tx_bytes;
-
-  // producer: warp 0 fills stage st with chunk ch
-  auto produce = [&](int ch, int st) {
-    const int k = ch * a.chunk + lane;
-    const bool active = lane < a.chunk && k < a.nviews;
-    ViewCoef vc;
-    int u0 = 0, v0 = 0;
-    bool skip = true, overflow = false, behind = false;
-    if (active) skip = tile_view_coef(a, k, ix0, iy0, iz0, ex, ey, ez, vc, u0, v0, overflow, behind);
-    if (lane < a.chunk) {
-      if (!active) vc.skip = 1;
-      coef[st * kMaxChunk + lane] = vc;
+  if (warp == NCW) {
+    // ---------------------------------------------------------------- producer
+    int issued = 0;
+    for (int kb = 0; kb < a.nviews && !*s_abort; kb += 32) {
+      const int k = kb + lane;
+      ViewCoef vc;
+      int u0 = 0, v0 = 0;
+      bool skip = true, overflow = false, behind = false;
+      if (k < a.nviews) {
+        // full tile extents: every consumer thread's samples lie in the window
+        skip = tile_view_coef(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, overflow, behind);
+        if (overflow) atomicCAS(a.err, 0, kDevFootprint);
+        if (behind) atomicCAS(a.err, 0, kDevGeometry);
+        if (overflow || behind) skip = true, vc.skip = 1;
+      }
+      const int nb = min(32, a.nviews - kb);
+      for (int i = 0; i < nb; ++i) {
+        const int kk = kb + i;
+        const int s = kk % S;
+        if (kk >= S && !mbar_wait(&empty[s], ((kk / S) & 1) ^ 1, a.err)) {
+          *s_abort = 1;
+          break;
+        }
+        if (lane == i) coef[s] = vc;
+        const int sk = __shfl_sync(0xffffffffu, (int)skip, i);
+        const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
+        __syncwarp();
+        if (lane == 0) {
+          if (sk) {
+            mbar_arrive(&full[s]);
+          } else {
+            mbar_arrive_expect_tx(&full[s], (uint32_t)a.tx_bytes);
+            void* dst = smem + (size_t)s * a.box_bytes;
+            const int x = LAYOUT == kLayoutPair32 ? 2 * cu0 : cu0;  // float2 elements are two floats
+            const int e0 = cv0 + a.pair_rows;  // pair layouts: row v lives in element row v + 1
+            if (a.sino_layout)
+              tma_load_3d(dst, &tmap, x, kk, e0, &full[s]);
+            else
+              tma_load_3d(dst, &tmap, x, e0, kk, &full[s]);
+          }
+        }
+        __syncwarp();
+        issued = kk + 1;
+      }
     }
-    if (active && overflow) atomicCAS(a.err, 0, kDevFootprint);
-    if (active && behind) atomicCAS(a.err, 0, kDevGeometry);
-    const unsigned issue = __ballot_sync(0xffffffffu, active && !skip);
-    __syncwarp();
-    if (lane == 0) mbar_arrive_expect_tx(&bars[st], __popc(issue) * tx_bytes);
-    __syncwarp();
-    if (active && !skip) {
-      void* dst = stage_base[st] + (size_t)lane * a.box_bytes;
-      if (a.sino_layout)
-        tma_load_3d(dst, &tmap, u0, k, v0, &bars[st]);
-      else
-        tma_load_3d(dst, &tmap, u0, v0, k, &bars[st]);
-    }
-  };
-
-  if (warp == 0) produce(0, 0);
-
-  float acc[NY];
-  float comp[NY];
-#pragma unroll
-  for (int j = 0; j < NY; ++j) {
-    acc[j] = 0.f;
-    comp[j] = 0.f;
+    // leave only when every copy issued into this CTA's memory has landed
+    for (int kk = max(0, issued - S); kk < issued; ++kk) mbar_wait(&full[kk % S], (kk / S) & 1, a.err);
+    return;
   }
+
+  // ------------------------------------------------------------------ consumers
+  constexpr int WX = TX / 8;
+  const int tx = (warp % WX) * 8 + (lane & 7);
+  const int tz = (warp / WX) * 4 + (lane >> 3);
   const float fx = (float)tx, fz = (float)tz;
   const int BU = a.box_u, BV = a.box_v;
+  constexpr int ESZ = LAYOUT == kLayoutPair32 ? 8 : 4;
+  const uint32_t RB = (uint32_t)(BU * ESZ);
+  // exclusive bound on v, kSlack / 2 inside the window: the footprint pass
+  // leaves kSlack, so the guard never trips for a voxel of the tile, and the
+  // rounded row index can never pass the last staged row
+  const float vmax_ok = (LAYOUT == kLayoutRaw32 ? (float)(BV - 1) : (float)BV) - (float)(kSlack / 2);
 
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const int st = ch & 1;
-    if (warp == 0 && ch + 1 < nchunks) produce(ch + 1, st ^ 1);
-    if (!mbar_wait(&bars[st], (ch >> 1) & 1, a.err)) {
-      s_abort = 1;
-    }
-    float part[NY];
+  float acc[NY], part[NY], comp[NY];
 #pragma unroll
-    for (int j = 0; j < NY; ++j) part[j] = 0.f;
-    const int nv_chunk = min(a.chunk, a.nviews - ch * a.chunk);
-    for (int vi = 0; vi < nv_chunk; ++vi) {
-      const ViewCoef g = coef[st * kMaxChunk + vi];
-      if (g.skip) continue;
-      const T* win = reinterpret_cast<const T*>(stage_base[st] + (size_t)vi * a.box_bytes);
+  for (int j = 0; j < NY; ++j) acc[j] = part[j] = comp[j] = 0.f;
+
+  int s = 0;
+  uint32_t ph = 0;
+  int kc = 0;
+  bool bad = false;
+  for (int k = 0; k < a.nviews; ++k) {
+    if (!mbar_wait(&full[s], ph, a.err)) {
+      *s_abort = 1;
+      break;
+    }
+    const ViewCoef g = coef[s];
+    if (!g.skip) {
       const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
       const float rD = __frcp_rn(D);
       const float ul = fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)) * rD;
@@ -317,40 +384,53 @@ __global__ void __launch_bounds__(TX* TZ, 1) bp_kernel(const __grid_constant__ C
       const float dvv = a.dvn * rD;
       const float W = rD * rD * g.wscale;
       const float fuf = floorf(ul);
+      const int iu = (int)fuf;
       const float fu = ul - fuf;
-      const int iu = min(max((int)fuf, 0), BU - 2);
-      const float wa = W - W * fu, wb = W * fu;
-      const T* col = win + iu;
+      const float vlast = fmaf((float)(NY - 1), dvv, vl);
+      if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
+        const float wa = W - W * fu, wb = W * fu;
+        const __half2 fu2 = __float2half2_rn(fu);
+        const uint32_t c0 = smem_u32(smem + (size_t)s * a.box_bytes) + (uint32_t)(iu * ESZ) - kMagicBits * RB;
+        const float vlm = vl - 0.5f;
 #pragma unroll
-      for (int j = 0; j < NY; ++j) {
-        const float v = fmaf((float)j, dvv, vl);
-        const float fvf = floorf(v);
-        const float fv = v - fvf;
-        const int iv = min(max((int)fvf, 0), BV - 2);
-        const T* p = col + iv * BU;
-        const float r0 = fmaf(wb, ldv(p + 1), wa * ldv(p));
-        const float r1 = fmaf(wb, ldv(p + BU + 1), wa * ldv(p + BU));
-        part[j] += fmaf(fv, r1 - r0, r0);
+        for (int j = 0; j < NY; ++j) {
+          const float val = tap<LAYOUT>(fmaf((float)j, dvv, vlm), c0, RB, wa, wb, fu2, W);
+          if (KAHAN)
+            part[j] += val;
+          else
+            acc[j] += val;
+        }
+      } else {
+        bad = true;  // cannot happen when the footprint pass is right; recorded below
       }
     }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (++s == S) {
+      s = 0;
+      ph ^= 1;
+    }
+    if (KAHAN && ++kc == KC) {
+      kc = 0;
 #pragma unroll
-    for (int j = 0; j < NY; ++j) {
-      if (KAHAN) {
+      for (int j = 0; j < NY; ++j) {
         const float y = part[j] - comp[j];
         const float t = acc[j] + y;
         comp[j] = (t - acc[j]) - y;
         acc[j] = t;
-      } else {
-        acc[j] += part[j];
+        part[j] = 0.f;
       }
     }
-    __syncthreads();  // stage st fully consumed before warp 0 refills it
-    if (s_abort) {
-      // leave only after the copy already issued into the other stage lands
-      if (ch + 1 < nchunks) mbar_wait(&bars[st ^ 1], ((ch + 1) >> 1) & 1, a.err);
-      return;
+  }
+  if (bad) atomicCAS(a.err, 0, kDevFootprint);
+  if (KAHAN) {
+#pragma unroll
+    for (int j = 0; j < NY; ++j) {
+      const float y = part[j] - comp[j];
+      acc[j] += y;
     }
   }
+  if (*s_abort) return;
 
   const int ix = ix0 + tx, iz = iz0 + tz;
   if (ix < a.nx && iz < a.nz) {
@@ -382,9 +462,9 @@ __global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
     t /= nty;
     const int bx = (int)(t % a.ntx), bz = (int)(t / a.ntx);
     const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = by * NY;
-    const int ex = min(TX, a.nx - ix0) - 1, ez = min(TZ, a.nz - iz0) - 1, ey = min(NY, a.ny - iy0) - 1;
+    // full tile extents, as the backprojector's producer uses them
     TileGeo g;
-    tile_geo(a, k, ix0, iy0, iz0, ex, ey, ez, g);
+    tile_geo(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, g);
     if (g.dmin <= 1e-6) atomicCAS(a.err, 0, kDevGeometry);
     if (tile_skip(a, g)) continue;
     int u0, v0, need_u, need_v;
@@ -445,31 +525,34 @@ __global__ void rebin_fan_kernel(const float* fan, int bins, int views, double s
   }
 }
 
-struct Config {
-  int tx, tz, ny;
-};
-
-template <typename T, int TX, int TZ, int NY, bool KAHAN>
-cudaError_t launch_cfg(const CUtensorMap& map, const BPArgs& a, size_t smem, cudaStream_t stream) {
-  auto kern = bp_kernel<T, TX, TZ, NY, KAHAN>;
+template <int LAYOUT, int TX, int TZ, int NY>
+cudaError_t launch_cfg(const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
+  auto kern = kahan ? bp_kernel<LAYOUT, TX, TZ, NY, true> : bp_kernel<LAYOUT, TX, TZ, NY, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.ntx * a.ntz, (a.ny + NY - 1) / NY);
-  kern<<<grid, TX * TZ, smem, stream>>>(map, a);
+  kern<<<grid, TX * TZ + 32, smem, stream>>>(map, a);
   return cudaGetLastError();
 }
 
-template <typename T, int TX, int TZ, int NY>
-cudaError_t launch_typed(const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
-  return kahan ? launch_cfg<T, TX, TZ, NY, true>(map, a, smem, stream)
-               : launch_cfg<T, TX, TZ, NY, false>(map, a, smem, stream);
+template <int TX, int TZ, int NY>
+cudaError_t launch_layout(int layout, const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan,
+                          cudaStream_t stream) {
+  switch (layout) {
+    case kLayoutPair32:
+      return launch_cfg<kLayoutPair32, TX, TZ, NY>(map, a, smem, kahan, stream);
+    case kLayoutPair16:
+      return launch_cfg<kLayoutPair16, TX, TZ, NY>(map, a, smem, kahan, stream);
+    default:
+      return launch_cfg<kLayoutRaw32, TX, TZ, NY>(map, a, smem, kahan, stream);
+  }
 }
 
 }  // namespace
 
 int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit, bool kahan) {
-  const bool f16 = st.state == kFilteredF16;
-  const int esize = f16 ? 2 : 4;
+  const int layout = st.filtered ? st.filt_layout : kLayoutRaw32;
+  const int esize = Stack::elem_bytes(layout);
   BPArgs a{};
   a.vol = vol;
   a.nx = g.nx;
@@ -494,13 +577,14 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
     a.dvn = (float)(g.vox / g.dv);
     a.scale = (float)(pi / g.nviews / g.du);
   }
-  a.inv_scale = f16 ? st.inv_scale : nullptr;
-  a.align = f16 ? 8 : 4;
+  a.inv_scale = layout == kLayoutPair16 ? st.inv_scale : nullptr;
+  a.align = layout == kLayoutPair32 ? 2 : 4;  // TMA: x * element size must be a multiple of 16 bytes
   a.sino_layout = st.sinogram ? 1 : 0;
+  a.pair_rows = layout == kLayoutRaw32 ? 0 : 1;
   a.clip_ylimit = clip_ylimit;
   a.err = ctx->d_err;
 
-  // per-view trig in FP64
+  // per-view trig in FP64 (cached per view set)
   if (ctx->trig_cap < g.nviews) {
     cudaFree(ctx->d_trig);
     ctx->d_trig = nullptr;
@@ -543,7 +627,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   a.ntz = (g.nz + TZ - 1) / TZ;
   const int nty = (g.ny + NY - 1) / NY;
 
-  // footprint pre-pass (cached per geometry)
+  // footprint pre-pass (cached per geometry and layout)
   double key[16] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
                     (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz,
                     (double)a.align, (double)NY};
@@ -560,74 +644,72 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
     else
       footprint_kernel<16, 16, 16><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
     int spans[4] = {0, 0, 0, 0};
-    if (int rc = cuda_check(ctx, cudaGetLastError(), "footprint_kernel")) return rc;
+    if (int rc = launched(ctx, "footprint_kernel")) return rc;
     if (int rc = cuda_check(ctx, cudaMemcpyAsync(spans, ctx->d_span, sizeof(spans), cudaMemcpyDeviceToHost,
                                                  ctx->stream),
                             "footprint readback"))
       return rc;
     if (int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync")) return rc;
-    int bu = std::max(spans[0], 2), bv = std::max(spans[1], 2);
-    bu = (bu + a.align - 1) / a.align * a.align;
     ctx->plan.valid = true;
     for (int i = 0; i < 16; ++i) ctx->plan.key[i] = key[i];
-    ctx->plan.box_u = bu;
-    ctx->plan.box_v = bv;
+    ctx->plan.box_u = std::max(spans[0], 2);
+    ctx->plan.box_v = std::max(spans[1], 2);
   }
-  a.box_u = ctx->plan.box_u;
-  a.box_v = ctx->plan.box_v;
-  if (a.box_u > 256 || a.box_v > 256)
+  int bu = (ctx->plan.box_u + a.align - 1) / a.align * a.align;
+  // a pair element carries row v + 1 with it: one row less to stage
+  int bv = layout == kLayoutRaw32 ? ctx->plan.box_v : std::max(1, ctx->plan.box_v - 1);
+  a.box_u = bu;
+  a.box_v = bv;
+  const int box_x = layout == kLayoutPair32 ? 2 * bu : bu;  // TMA box inner extent in 4-byte elements
+  if (box_x > 256 || bv > 256)
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
-                     "detector footprint of a 16x16x16 voxel tile exceeds 256 samples; geometry magnification too "
-                     "large for the staged backprojector");
-  a.tx_bytes = a.box_u * a.box_v * esize;
+                     "detector footprint of a voxel tile exceeds the 256-element TMA box; geometry magnification "
+                     "too large for the staged backprojector");
+  a.tx_bytes = bu * bv * esize;
   a.box_bytes = (a.tx_bytes + 127) / 128 * 128;
-  const size_t smem_cap = 227 * 1024 - 1024;
-  const size_t fixed = sizeof(ViewCoef) * 2 * kMaxChunk + 2 * sizeof(uint64_t) + 64;
-  int chunk = kMaxChunk;
-  while (chunk > 1 && 2 * (size_t)chunk * a.box_bytes + fixed > smem_cap) chunk >>= 1;
-  if (2 * (size_t)chunk * a.box_bytes + fixed > smem_cap)
-    return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
-  a.chunk = chunk;
-  const size_t smem = 2 * (size_t)chunk * a.box_bytes + fixed;
+  // two CTAs per SM: each gets half of the 228 KB shared memory
+  const size_t smem_cap = 113 * 1024;
+  const size_t per_stage = a.box_bytes + sizeof(ViewCoef) + 2 * sizeof(uint64_t);
+  int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
+  if (stages < 2) return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
+  a.chunk = stages;
+  const size_t smem = (size_t)stages * per_stage + 64;
 
-  // tensor map over the filtered stack
-  CUtensorMap map;
+  // tensor map over the filtered stack (4-byte elements; float2 as two floats)
+  const void* base = st.filtered ? st.filt : (const void*)st.f32;
+  const int pitch_el = st.filtered ? st.filt_pitch : st.pitch;
+  const uint64_t pitch_bytes = (uint64_t)pitch_el * esize;
+  const uint64_t ux = layout == kLayoutPair32 ? 2ull * st.u : (uint64_t)st.u;
+  const uint64_t rows_v = layout == kLayoutRaw32 ? (uint64_t)st.v : (uint64_t)st.v + 1;  // element rows per view
   uint64_t dims[3], strides[2];
   uint32_t box[3];
-  void* base;
-  const uint64_t pitch_bytes = (uint64_t)(f16 ? st.pitch16 : st.pitch) * esize;
-  base = f16 ? (void*)st.f16 : (void*)st.f32;
   if (st.sinogram) {  // [v][view][u]
-    dims[0] = st.u;
+    dims[0] = ux;
     dims[1] = st.n;
-    dims[2] = st.v;
+    dims[2] = rows_v;
     strides[0] = pitch_bytes;
     strides[1] = pitch_bytes * st.n;
-    box[0] = a.box_u;
+    box[0] = box_x;
     box[1] = 1;
-    box[2] = a.box_v;
+    box[2] = bv;
   } else {  // [view][v][u]
-    dims[0] = st.u;
-    dims[1] = st.v;
+    dims[0] = ux;
+    dims[1] = rows_v;
     dims[2] = st.n;
     strides[0] = pitch_bytes;
-    strides[1] = pitch_bytes * st.v;
-    box[0] = a.box_u;
-    box[1] = a.box_v;
+    strides[1] = pitch_bytes * rows_v;
+    box[0] = box_x;
+    box[1] = bv;
     box[2] = 1;
   }
-  if (int rc = make_tensor_map_3d(ctx, &map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                  base, dims, strides, box))
+  CUtensorMap map;
+  if (int rc = make_tensor_map_3d(ctx, &map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, const_cast<void*>(base), dims, strides,
+                                  box))
     return rc;
 
-  cudaError_t e;
-  if (is2d) {
-    e = f16 ? launch_typed<__half, 16, 16, 1>(map, a, smem, kahan, ctx->stream)
-            : launch_typed<float, 16, 16, 1>(map, a, smem, kahan, ctx->stream);
-  } else {
-    e = f16 ? launch_typed<__half, 16, 16, 16>(map, a, smem, kahan, ctx->stream)
-            : launch_typed<float, 16, 16, 16>(map, a, smem, kahan, ctx->stream);
-  }
+  cudaError_t e = is2d ? launch_layout<16, 16, 1>(layout, map, a, smem, kahan, ctx->stream)
+                       : launch_layout<16, 16, 16>(layout, map, a, smem, kahan, ctx->stream);
+  if (e == cudaSuccess) ctx->launches++;
   return cuda_check(ctx, e, "bp_kernel");
 }
 
@@ -636,7 +718,7 @@ int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limi
   int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
   if (total == 0) return FBP_OK;
   clip_kernel<<<blocks, 256, 0, ctx->stream>>>(vol, nx, ny, nz, y_limit);
-  return cuda_check(ctx, cudaGetLastError(), "clip_kernel");
+  return launched(ctx, "clip_kernel");
 }
 
 int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g, float* par,
@@ -646,7 +728,7 @@ int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, co
   int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
   rebin_fan_kernel<<<blocks, 256, 0, ctx->stream>>>(fan, bins, views, g.sod, g.sdd, g.du, g.span, g.offset, par,
                                                     out_bins, du_out);
-  return cuda_check(ctx, cudaGetLastError(), "rebin_fan_kernel");
+  return launched(ctx, "rebin_fan_kernel");
 }
 
 }  // namespace fbp

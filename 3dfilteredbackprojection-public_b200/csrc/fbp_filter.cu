@@ -131,6 +131,41 @@ __device__ __forceinline__ int row_view(const RowSet& rs, long long r) {
   return rs.sinogram ? (int)(r % rs.n_views) : (int)(r / rs.n_v);
 }
 
+// Write filtered sample i of row r: in place (FP32 rows) or into a pair
+// layout of nv + 1 element rows per view, element e = (row e - 1, row e).
+// Sample (view, iv) is the .x half of element iv + 1 and the .y half of
+// element iv; row 0 also zeroes the .x half of element 0 and the last row
+// the .y half of element nv.
+__device__ __forceinline__ long long pair_row(const RowSet& rs, int view, int e) {
+  return rs.sinogram ? (long long)e * rs.n_views + view : (long long)view * (rs.n_v + 1) + e;
+}
+
+__device__ __forceinline__ void store_row_sample(const RowSet& rs, long long r, int i, float y) {
+  if (rs.out_layout == kLayoutRaw32) {
+    rs.data[r * rs.pitch + i] = y;
+    return;
+  }
+  const int iv = rs.sinogram ? (int)(r / rs.n_views) : (int)(r % rs.n_v);
+  const int view = row_view(rs, r);
+  const long long below = pair_row(rs, view, iv + 1) * rs.out_pitch + i;  // element iv + 1: .x
+  const long long here = pair_row(rs, view, iv) * rs.out_pitch + i;       // element iv: .y
+  if (rs.out_layout == kLayoutPair32) {
+    float2* o = static_cast<float2*>(rs.out);
+    o[below].x = y;
+    o[here].y = y;
+    if (iv == 0) o[here].x = 0.f;
+    if (iv == rs.n_v - 1) o[below].y = 0.f;
+  } else {
+    __half2* o = static_cast<__half2*>(rs.out);
+    const __half h = __float2half_rn(y * rs.view_scale[view]);
+    const __half z = __float2half_rn(0.f);
+    o[below].x = h;
+    o[here].y = h;
+    if (iv == 0) o[here].x = z;
+    if (iv == rs.n_v - 1) o[below].y = z;
+  }
+}
+
 // One CTA filters `pairs_per_cta` row pairs per iteration, grid-stride.
 __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -200,14 +235,8 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
       if (pr >= a.npairs || i >= rs.m) continue;
       float2 y = buf[idx];
       long long r0 = 2 * pr;
-      if (rs.out16) {
-        rs.out16[r0 * rs.pitch16 + i] = __float2half_rn(y.x * rs.view_scale[row_view(rs, r0)]);
-        if (r0 + 1 < rs.rows)
-          rs.out16[(r0 + 1) * rs.pitch16 + i] = __float2half_rn(y.y * rs.view_scale[row_view(rs, r0 + 1)]);
-      } else {
-        rs.data[r0 * rs.pitch + i] = y.x;
-        if (r0 + 1 < rs.rows) rs.data[(r0 + 1) * rs.pitch + i] = y.y;
-      }
+      store_row_sample(rs, r0, i, y.x);
+      if (r0 + 1 < rs.rows) store_row_sample(rs, r0 + 1, i, y.y);
     }
   }
 }
@@ -223,16 +252,23 @@ __global__ void elementwise_pre_kernel(RowSet rs) {
 }
 
 // Per-view max |pre-processed sample| (as float bits: non-negative floats
-// order like integers).
+// order like integers). One warp reduces one row, lane 0 folds it into a
+// shared per-view table, and each block flushes its table once.
 __global__ void view_absmax_kernel(RowSet rs, unsigned* vmax) {
-  long long total = rs.rows * (long long)rs.m;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    long long r = e / rs.m;
-    int i = (int)(e - r * rs.m);
-    float x = fabsf(load_pre(rs, r, i));
-    if (x > 0.f) atomicMax(vmax + row_view(rs, r), __float_as_uint(x));
+  extern __shared__ unsigned smax[];
+  for (int i = threadIdx.x; i < rs.n_views; i += blockDim.x) smax[i] = 0u;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  for (long long r = blockIdx.x * (long long)warps + (threadIdx.x >> 5); r < rs.rows;
+       r += (long long)gridDim.x * warps) {
+    float m = 0.f;
+    for (int i = lane; i < rs.m; i += 32) m = fmaxf(m, fabsf(load_pre(rs, r, i)));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0 && m > 0.f) atomicMax(smax + row_view(rs, r), __float_as_uint(m));
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < rs.n_views; i += blockDim.x)
+    if (smax[i]) atomicMax(vmax + i, smax[i]);
 }
 
 // scale = largest power of two with scale * bound <= 2^15, bound = L1 norm of
@@ -320,17 +356,25 @@ __global__ void fft_shift_kernel(float2* data, int n, int rows, int shift) {
   }
 }
 
-__global__ void f16_to_f32_kernel(const __half* src, long long pitch16, const float* inv_scale, int n_views,
-                                  int n_v, bool sinogram, long long row0, long long nrows, int m, float* dst,
-                                  long long dpitch) {
+__global__ void unpack_rows_kernel(const void* src, int layout, long long spitch, const float* inv_scale,
+                                   int n_views, int n_v, bool sinogram, long long row0, long long nrows, int m,
+                                   float* dst, long long dpitch) {
   long long total = nrows * m;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     long long r = e / m;
     int i = (int)(e - r * m);
     long long gr = row0 + r;
-    int view = sinogram ? (int)(gr % n_views) : (int)(gr / n_v);
-    dst[r * dpitch + i] = __half2float(src[gr * pitch16 + i]) * inv_scale[view];
+    const int view = sinogram ? (int)(gr % n_views) : (int)(gr / n_v);
+    const int iv = sinogram ? (int)(gr / n_views) : (int)(gr % n_v);
+    // row iv is the .x half of element iv + 1
+    const long long er = sinogram ? (long long)(iv + 1) * n_views + view : (long long)view * (n_v + 1) + iv + 1;
+    float x;
+    if (layout == kLayoutPair32)
+      x = static_cast<const float2*>(src)[er * spitch + i].x;
+    else
+      x = __half2float(static_cast<const __half2*>(src)[er * spitch + i].x) * inv_scale[view];
+    dst[r * dpitch + i] = x;
   }
 }
 
@@ -373,7 +417,8 @@ int ensure_filter_tables(fbp_context* ctx, int n, int filter) {
   int blocks = (n + 127) / 128;
   response_kernel<<<blocks, 128, 0, ctx->stream>>>(n, filter, H);
   tables_kernel<<<blocks, 128, 0, ctx->stream>>>(n, ilog2(n), H, t.hbr, t.twiddle, t.kernel);
-  if (int rc = cuda_check(ctx, cudaGetLastError(), "filter tables")) return rc;
+  ctx->launches += 1;  // two launches above
+  if (int rc = launched(ctx, "filter tables")) return rc;
   t.n = n;
   t.filter = filter;
   return FBP_OK;
@@ -400,13 +445,13 @@ int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n) {
   long long groups = (a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta;
   int grid = (int)std::min<long long>(groups, (long long)ctx->num_sms * 4);
   filter_fft_kernel<<<grid, 256, smem, ctx->stream>>>(a);
-  return cuda_check(ctx, cudaGetLastError(), "filter_fft_kernel");
+  return launched(ctx, "filter_fft_kernel");
 }
 
 int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs) {
   if (rs.rows == 0) return FBP_OK;
   elementwise_pre_kernel<<<grid_for(ctx, rs.rows * rs.m, 256), 256, 0, ctx->stream>>>(rs);
-  return cuda_check(ctx, cudaGetLastError(), "elementwise_pre_kernel");
+  return launched(ctx, "elementwise_pre_kernel");
 }
 
 int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale) {
@@ -415,10 +460,17 @@ int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, fl
   float* l1 = reinterpret_cast<float*>(vmax + rs.n_views);
   if (int rc = cuda_check(ctx, cudaMemsetAsync(vmax, 0, sizeof(unsigned) * rs.n_views, ctx->stream), "memset"))
     return rc;
-  view_absmax_kernel<<<grid_for(ctx, rs.rows * rs.m, 256), 256, 0, ctx->stream>>>(rs, vmax);
+  if (rs.n_views > 16384) return set_error(ctx, FBP_ERR_UNSUPPORTED, "at most 16384 views in MIXED precision");
+  {
+    const int blocks = (int)std::max(1LL, std::min<long long>((rs.rows + 7) / 8, (long long)ctx->num_sms * 4));
+    const size_t sm = sizeof(unsigned) * rs.n_views;
+    cudaFuncSetAttribute(view_absmax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    view_absmax_kernel<<<blocks, 256, sm, ctx->stream>>>(rs, vmax);
+  }
   l1_kernel<<<1, 256, 0, ctx->stream>>>(ctx->ftab.kernel, ctx->ftab.n, l1);
   view_scale_kernel<<<(rs.n_views + 127) / 128, 128, 0, ctx->stream>>>(vmax, rs.n_views, l1, view_scale, inv_scale);
-  return cuda_check(ctx, cudaGetLastError(), "view scale kernels");
+  ctx->launches += 2;  // three launches above
+  return launched(ctx, "view scale kernels");
 }
 
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse) {
@@ -433,7 +485,8 @@ int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse
   cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   fft_rows_kernel<<<std::min(rows, ctx->num_sms * 4), 256, smem, ctx->stream>>>(data, n, ilog2(n), rows, inverse,
                                                                                  tw);
-  return cuda_check(ctx, cudaGetLastError(), "fft_rows_kernel");
+  ctx->launches += 1;  // twiddle_kernel
+  return launched(ctx, "fft_rows_kernel");
 }
 
 int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift) {
@@ -442,15 +495,16 @@ int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int s
   cudaFuncSetAttribute(fft_shift_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   fft_shift_kernel<<<std::min(rows, ctx->num_sms * 4), 256, sizeof(float2) * n, ctx->stream>>>(data, n, rows,
                                                                                                 shift);
-  return cuda_check(ctx, cudaGetLastError(), "fft_shift_kernel");
+  return launched(ctx, "fft_shift_kernel");
 }
 
-int launch_f16_to_f32(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst,
-                      long long dst_pitch) {
+int launch_unpack_rows(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst,
+                       long long dst_pitch) {
   if (nrows == 0) return FBP_OK;
-  f16_to_f32_kernel<<<grid_for(ctx, (long long)nrows * s.u, 256), 256, 0, ctx->stream>>>(
-      s.f16, s.pitch16, s.inv_scale, s.n, s.v, s.sinogram, (long long)row0, (long long)nrows, s.u, dst, dst_pitch);
-  return cuda_check(ctx, cudaGetLastError(), "f16_to_f32_kernel");
+  unpack_rows_kernel<<<grid_for(ctx, (long long)nrows * s.u, 256), 256, 0, ctx->stream>>>(
+      s.filt, s.filt_layout, s.filt_pitch, s.inv_scale, s.n, s.v, s.sinogram, (long long)row0, (long long)nrows, s.u,
+      dst, dst_pitch);
+  return launched(ctx, "unpack_rows_kernel");
 }
 
 }  // namespace fbp

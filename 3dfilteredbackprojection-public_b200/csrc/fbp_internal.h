@@ -21,25 +21,32 @@ enum DeviceError : int {
   kDevGeometry = 3,   // a voxel lies at or behind the source plane
 };
 
-// State of a stack of detector rows (projections or sinograms).
-enum StackState : int {
-  kRawF32 = 0,       // f32 holds the data
-  kFilteredF32 = 1,  // f32 holds filtered rows
-  kFilteredF16 = 2,  // f16 + inv_scale hold filtered rows; f32 is stale
+// Layout of filtered views kept for the backprojector. A pair layout has
+// nv + 1 element rows per view; element e at column u holds the samples of
+// detector rows e - 1 and e (zero outside the detector), so one
+// shared-memory load yields both rows of a bilinear tap for v in [e-1, e).
+enum FiltLayout : int {
+  kLayoutRaw32 = 0,   // plain FP32 rows (unfiltered data, 2D staging)
+  kLayoutPair32 = 1,  // float2 (8 bytes / sample), FP32 form
+  kLayoutPair16 = 2,  // half2 (4 bytes / sample) with a per-view scale, MIXED form
 };
 
 // A stack of detector rows. Projections are [view][v][u] (rows ordered view
 // major), sinograms [v][view][u] (rows ordered v major). Rows of u samples
 // are padded to `pitch` elements so that every row starts 16-byte aligned.
+// After filtering, the stack's content is the filtered buffer `filt` (in a
+// pair layout) and f32 still holds the unfiltered input.
 struct Stack {
   float* f32 = nullptr;
-  __half* f16 = nullptr;
-  float* inv_scale = nullptr;  // per view, multiplies the f16 values
   int u = 0, v = 0, n = 0;
-  int pitch = 0;    // f32 row pitch in elements (multiple of 4)
-  int pitch16 = 0;  // f16 row pitch in elements (multiple of 8)
+  int pitch = 0;  // f32 row pitch in elements (multiple of 4)
   bool sinogram = false;
-  int state = kRawF32;
+  bool filtered = false;          // content lives in filt
+  void* filt = nullptr;
+  size_t filt_bytes = 0;
+  int filt_layout = kLayoutPair32;
+  int filt_pitch = 0;             // elements per row of filt (multiple of 4)
+  float* inv_scale = nullptr;     // per view (x2: [inv | scale]) for kLayoutPair16
   // Log normalisation and FDK weights recorded by their calls and applied
   // inside the filter kernel's load (log first, then weight), or by a
   // standalone pass when something else reads the rows first.
@@ -49,9 +56,9 @@ struct Stack {
   double w_sdd = 0, w_du = 0, w_dv = 0;
   size_t rows() const { return (size_t)v * n; }
   size_t bytes32() const { return (size_t)pitch * rows() * sizeof(float); }
-  size_t bytes16() const { return (size_t)pitch16 * rows() * sizeof(__half); }
-  // row r -> detector row index iv and view index
-  int row_v(size_t r) const { return sinogram ? (int)(r / n) : (int)(r % v); }
+  static int elem_bytes(int layout) { return layout == kLayoutPair32 ? 8 : 4; }
+  // element rows of the filtered buffer (pair layouts carry one extra row per view)
+  size_t filt_rows() const { return (size_t)(v + 1) * n; }
 };
 
 struct FilterTables {
@@ -73,6 +80,7 @@ struct fbp_context {
   int pad_len = 0;
   int clip_after_bp = 1;
   int num_sms = 148;
+  unsigned long long launches = 0;  // kernels launched by this context
 
   float* vol = nullptr;
   int vx = 0, vy = 0, vz = 0;
@@ -104,6 +112,11 @@ namespace fbp {
 // ---- error helpers (fbp_api.cu) ----
 int set_error(fbp_context* ctx, int code, const std::string& msg);
 int cuda_check(fbp_context* ctx, cudaError_t e, const char* what);
+// Error check after a kernel launch; counts the launch.
+inline int launched(fbp_context* ctx, const char* what) {
+  ctx->launches++;
+  return cuda_check(ctx, cudaGetLastError(), what);
+}
 void* scratch(fbp_context* ctx, size_t bytes);
 
 // ---- filter (fbp_filter.cu) ----
@@ -120,10 +133,11 @@ struct RowSet {
   float log_base = 1.f;
   bool weight = false;
   float w_sdd = 0, w_du = 0, w_dv = 0;
-  // optional FP16 output
-  __half* out16 = nullptr;
-  long long pitch16 = 0;
-  const float* view_scale = nullptr;  // values are multiplied by it before rounding to FP16
+  // output: in place into `data` (out == nullptr) or into a pair layout
+  void* out = nullptr;
+  int out_layout = kLayoutRaw32;
+  long long out_pitch = 0;            // elements
+  const float* view_scale = nullptr;  // kLayoutPair16: values are multiplied by it before rounding
 };
 int ensure_filter_tables(fbp_context* ctx, int n, int filter);
 int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n);
@@ -132,7 +146,8 @@ int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs);  // weight / log
 int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale);
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse);
 int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift);
-int launch_f16_to_f32(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst, long long dst_pitch);
+// Copy filtered rows [row0, row0 + nrows) of a pair layout back to FP32 rows.
+int launch_unpack_rows(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst, long long dst_pitch);
 bool toeplitz_supported(int m);
 
 // ---- backprojection (fbp_backproject.cu) ----
@@ -144,6 +159,7 @@ struct BPGeom {
   int nu, nv, nviews;
   int nx, ny, nz;
 };
+// Backproject the stack's content (filt when filtered, else f32 rows).
 int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit,
                        bool kahan);
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit);

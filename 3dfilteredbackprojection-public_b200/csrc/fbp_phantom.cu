@@ -85,7 +85,7 @@ int launch_project_ellipsoids(fbp_context* ctx, const double* d_ell, int count, 
   if (total == 0) return FBP_OK;
   int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 32);
   project_ellipsoids_kernel<<<blocks, 256, 0, ctx->stream>>>(d_ell, count, g, out, pitch);
-  return cuda_check(ctx, cudaGetLastError(), "project_ellipsoids_kernel");
+  return launched(ctx, "project_ellipsoids_kernel");
 }
 
 }  // namespace fbp

@@ -139,6 +139,8 @@ SIGNATURES = {
     "fbp_fft_rows": [_P, _P, _I, _I, _I],
     "fbp_fft_shift_rows": [_P, _P, _I, _I, _I],
     "fbp_project_ellipsoids_to_projections": [_P, _P, _I, C.POINTER(Geometry)],
+    "fbp_kernel_launch_count": [_P, C.POINTER(C.c_uint64)],
+    "fbp_measure_smem_bandwidth": [_P, C.POINTER(C.c_double)],
 }
 
 
@@ -235,6 +237,17 @@ class FBP3D:
 
     def synchronize(self) -> None:
         self.ctx.call("fbp_synchronize")
+
+    def kernel_launch_count(self) -> int:
+        c = C.c_uint64()
+        self.ctx.call("fbp_kernel_launch_count", C.byref(c))
+        return c.value
+
+    def measure_smem_bandwidth(self) -> float:
+        """Shared-memory load bandwidth of the device in bytes/s."""
+        b = C.c_double()
+        self.ctx.call("fbp_measure_smem_bandwidth", C.byref(b))
+        return b.value
 
     def memory_in_use(self) -> int:
         b = C.c_size_t()

@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""FDK throughput benchmark: cone-beam 1440x1470x1440 volume (x, y, z; y the
+rotation axis) at 0.2 mm, 1440 views over 360 deg, 1536x1536 detector at
+0.254 mm, SOD 400 mm, SDD 800 mm, Hann-windowed ramp; 40 seeded random
+ellipsoids with analytic FP64 line integrals and Poisson noise (I0 = 5e4).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one reconstruction: restore the raw projections (device-to-device,
+the filter works in place), FDK weights, row filter, backprojection with the
+fused clip epilogue. `value` (Gvox*view/s = 1440*1470*1440*1440 / step time)
+is the chosen form (split-precision: FP16 filtered views with per-view scale,
+Kahan-compensated FP32 accumulation) with inputs resident in HBM; the plain
+FP32 form is reported beside it. `e2e` repeats the chosen form through the C
+ABI with pinned host buffers: the projection upload and the volume readback
+are inside the timed region. Multi-GPU runs (torchrun) reconstruct one
+independent volume per rank (weak scaling, no collective on the data path);
+times are the max over ranks.
+
+`--impl reference` times the reference's CPU path on the host cores: row
+filtering with the reference's own FFT compiled from its sources (the
+oracle's PI_MODE_REPO restatement where that build is absent) plus a CPU FP32
+restatement of the backprojector (the reference ships no CPU backprojector),
+on a bounded sample of the same workload, extrapolated to the full job.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "3dfilteredbackprojection-public_b200"
+sys.path.insert(0, str(PKG))
+
+METRIC = "FDK Gvox·view/s"
+UNIT = "Gvox·view/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--scale", type=int, default=1,
+                   help="divide volume, detector and views by this factor (profiling runs); 1 = full workload")
+    p.add_argument("--forms", default="chosen,plain", help="comma list of chosen,plain")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the CPU-baseline sample")
+    return p.parse_args()
+
+
+def workload(scale: int) -> dict:
+    import phantoms as P
+    c = P.config_cone1440()
+    return c if scale == 1 else P.scaled_cone(c, scale)
+
+
+def updates_of(c: dict) -> int:
+    return c["nx"] * c["ny"] * c["nz"] * c["nviews"]
+
+
+# ------------------------------------------------------------------ CPU legs
+def _oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    O.build(with_ref=False)
+    return O
+
+
+def cpu_sample(c: dict, proj_views, view_ids, target_s: float) -> dict:
+    """Time the reference CPU path on a bounded sample and extrapolate.
+
+    Filter stage: FDK weights + row filter of the sampled views with the
+    reference's FFT (compiled from its sources; the oracle's repo-pi
+    restatement where that build is absent), OpenMP over rows.
+    Backprojection stage: the FP32 CPU restatement over four y-slabs spread
+    along the rotation axis for the sampled views, sized so that this stage
+    takes about 60% of `target_s`. Each stage's cost per unit (row, update)
+    is scaled to the full job's units."""
+    import numpy as np
+    O = _oracle()
+    threads = O.num_threads()
+    use_ref = O.ref_available()
+    n = O.padded_length(c["nu"])
+    t0 = time.perf_counter()
+    w = O.fdk_weight(proj_views, c["sdd"], c["du"], c["dv"]).astype(np.float32)
+    rows = w.reshape(-1, c["nu"])
+    if use_ref:
+        filt = O.ref_filter_rows(rows, c["filter"], n)
+    else:
+        filt = O.filter_rows(rows.astype(np.float64), c["filter"], n, pi_mode=O.PI_REPO).astype(np.float32)
+    t_filter = time.perf_counter() - t0
+    per_row = t_filter / rows.shape[0]
+    q = filt.reshape(len(view_ids), c["nv"], c["nu"])
+    nsel = len(view_ids)
+
+    def slabs(height: int):
+        """Four slabs of `height` slices spread along y; returns updates done."""
+        done = 0
+        for f in (0.125, 0.375, 0.625, 0.875):
+            y0 = min(c["ny"] - height, int(f * c["ny"]))
+            vol = np.zeros((c["nz"], height, c["nx"]), np.float32)
+            O.cpu_bp_cone_f32(q, view_ids, c, y0, y0 + height, vol)
+            done += c["nx"] * c["nz"] * height * nsel
+        return done
+
+    t0 = time.perf_counter()
+    probe = slabs(1)
+    t_probe = time.perf_counter() - t0
+    per_update = t_probe / probe
+    height = max(1, min(c["ny"] // 4, int(0.6 * target_s / (per_update * 4 * c["nx"] * c["nz"] * nsel))))
+    t0 = time.perf_counter()
+    nup = slabs(height)
+    t_bp = time.perf_counter() - t0
+    per_update = t_bp / nup
+    t_full = per_row * c["nviews"] * c["nv"] + per_update * updates_of(c)
+    return dict(value=updates_of(c) / t_full / 1e9, cores=threads, use_ref=use_ref, per_row_s=per_row,
+                per_update_s=per_update, sample_rows=int(rows.shape[0]), sample_updates=int(nup),
+                sample_seconds=t_filter + t_bp, full_seconds=t_full)
+
+
+def cpu_inputs(c: dict, nviews_sample: int):
+    """Analytic projections of the benchmark phantom for a few views (FP64 on
+    the CPU), with the workload's Poisson noise."""
+    import numpy as np
+    import phantoms as P
+    O = _oracle()
+    E = P.ellipsoids_for(c)
+    views = np.linspace(0, c["nviews"] - 1, nviews_sample).round().astype(np.int32)
+    proj = O.project_ellipsoids_cone(E, c, views)
+    if "i0" in c:
+        proj = P.poisson_log(proj, c["i0"], np.random.default_rng(c["seed"]))
+    return proj, views
+
+
+def reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    c = workload(args.scale)
+    nsv = 8 if args.scale == 1 else 4
+    proj, views = cpu_inputs(c, nsv)
+    results = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(c, proj, views, target_s=args.cpu_seconds / 3)
+        if i >= args.warmup:
+            results.append(r)
+    val = statistics.mean(r["value"] for r in results)
+    r0 = results[-1]
+    ms = updates_of(c) / (val * 1e9) * 1e3
+    kind = "reference" if r0["use_ref"] else "port"
+    sample = (f"{r0['sample_rows']} detector rows filtered with the reference's FFT::fft_radix2 "
+              f"{'(compiled from its sources)' if r0['use_ref'] else '(oracle restatement, repo pi)'} and "
+              f"{r0['sample_updates']:.3g} voxel-view updates of the CPU FP32 backprojector restatement "
+              f"(the reference has no CPU backprojector), extrapolated linearly to the full job")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 filter / f32 backprojection",
+        "data": "synthetic: seeded random ellipsoids, analytic FP64 line integrals, Poisson noise",
+        "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "views": c["nviews"],
+                   "detector": [c["nu"], c["nv"]], "filter": "hann", "parallelism": "host cores"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": r0["cores"], "kind": kind, "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples of this process's GPU."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.uuid = uuid
+        self.proc = None
+        self.out = Path(os.environ.get("TMPDIR", "/tmp")) / f"fbp_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            if self.uuid and self.uuid not in parts[0]:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        self.out.unlink(missing_ok=True)
+        loaded = sorted(sm)[len(sm) // 4:] if sm else []  # drop the idle quarter
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def main() -> None:
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=dev)
+
+    import build as B
+    B.build()
+    import fbp_b200 as F
+    import phantoms as P
+
+    c = workload(args.scale)
+    U = updates_of(c)
+    ga = P.geometry_args(c)
+    geom = F.Geometry.cone(ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"],
+                           ga["full_rotation_count"], c["offset"])
+    stream = torch.cuda.Stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- inputs: analytic projections on the device + Poisson noise
+    gen = F.FBP3D(local_rank)
+    gen.set_stream(stream)
+    gen.generate_blank_projections(c["nu"], c["nv"], c["nviews"])
+    gen.project_ellipsoids(P.ellipsoids_for(c), geom)
+    pristine = torch.empty((c["nviews"], c["nv"], c["nu"]), dtype=torch.float32, device=dev)
+    gen.download_projections(pristine)
+    gen.synchronize()
+    gen.ctx.close()
+    del gen
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device=dev)
+        g.manual_seed(c["seed"] + 7919 * rank)
+        for k0 in range(0, c["nviews"], 64):
+            blk = pristine[k0:k0 + 64]
+            counts = torch.poisson(c["i0"] * torch.exp(-blk), generator=g)
+            blk.copy_(-torch.log(torch.clamp(counts, min=1.0) / c["i0"]))
+            del counts
+    stream.synchronize()
+
+    sod, odd, w, vw, rot = ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"], ga["full_rotation_count"]
+
+    def make_solver(form: str):
+        s = F.FBP3D(local_rank)
+        s.set_stream(stream)
+        s.set_precision(F.Precision.MIXED if form == "chosen" else F.Precision.FP32)
+        s.set_clip_after_backprojection(True)
+        return s
+
+    def step(s, src, ev=None):
+        s.upload_projections(src)
+        s.apply_fdk_weights_to_projections(sod, odd, w)
+        if ev is not None:
+            ev[0].record(stream)
+        s.apply_filter_to_projections(c["filter"])
+        if ev is not None:
+            ev[1].record(stream)
+        s.project_backward_cone_fdk_from_projections(sod, odd, w, vw, rot, c["nx"], c["ny"], c["offset"])
+        if ev is not None:
+            ev[2].record(stream)
+
+    def timed(s, src, readback=None) -> dict:
+        for _ in range(args.warmup):
+            step(s, src)
+            if readback is not None:
+                s.read_volume(readback)
+        s.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = s.kernel_launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(str(torch.cuda.get_device_properties(dev).uuid) if hasattr(
+            torch.cuda.get_device_properties(dev), "uuid") else "")
+        clocks.start()
+        t_wall = time.perf_counter()
+        start.record(stream)
+        for k in range(args.steps):
+            step(s, src, evs[k])
+            if readback is not None:
+                s.read_volume(readback)
+        end.record(stream)
+        stream.synchronize()
+        t_wall = time.perf_counter() - t_wall
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        launches = s.kernel_launch_count() - launches0
+        ms = max_over_ranks(start.elapsed_time(end) / args.steps)
+        filt_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+        bp_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+        return dict(ms=ms, filter_ms=filt_ms, bp_ms=bp_ms, launches=launches, clocks=clk,
+                    wall_ms=t_wall * 1e3 / args.steps)
+
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    res, vols = {}, {}
+    for form in forms:
+        s = make_solver(form)
+        res[form] = timed(s, pristine)
+        vols[form] = torch.empty((c["nz"], c["ny"], c["nx"]), dtype=torch.float32, device=dev)
+        s.read_volume(vols[form])
+        if form == "chosen":
+            smem_bw = s.measure_smem_bandwidth()
+        s.ctx.close()
+        del s
+        torch.cuda.empty_cache()
+
+    accuracy = {}
+    if "chosen" in vols and "plain" in vols:
+        a, b = vols["chosen"].double(), vols["plain"].double()
+        accuracy["chosen_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        accuracy["chosen_vs_plain_max_abs"] = float((a - b).abs().max())
+        del a, b
+    vols.clear()
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with pinned host buffers (chosen form)
+    e2e = None
+    head = "chosen" if "chosen" in res else forms[0]
+    if not args.no_e2e:
+        host_proj = torch.empty((c["nviews"], c["nv"], c["nu"]), dtype=torch.float32, pin_memory=True)
+        host_proj.copy_(pristine)
+        host_vol = torch.empty((c["nz"], c["ny"], c["nx"]), dtype=torch.float32, pin_memory=True)
+        s = make_solver(head)
+        r = timed(s, host_proj, readback=host_vol)
+        s.ctx.close()
+        del s
+        e2e = {"value": world * U / (r["ms"] * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(host_proj.numel() * 4), "d2h_bytes_per_step": int(host_vol.numel() * 4),
+               "ms_per_step": r["ms"]}
+        del host_proj, host_vol
+
+    h = res[head]
+    value = world * U / (h["ms"] * 1e-3) / 1e9
+    # roofline of the dominant kernel (the backprojector)
+    esize = 2 if head == "chosen" else 4
+    bp_s = h["bp_ms"] * 1e-3
+    hbm_bytes = c["nviews"] * c["nv"] * c["nu"] * esize + 4 * c["nx"] * c["ny"] * c["nz"]
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    gather_bytes = 4 * esize * U  # four bilinear taps per update
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "storage_dtype": "f16 filtered views" if head == "chosen" else "f32",
+        "data": "synthetic: 40 seeded random ellipsoids, analytic FP64 line integrals, Poisson noise I0=5e4",
+        "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "voxel_mm": c["vox"],
+                   "views": c["nviews"], "detector": [c["nu"], c["nv"]], "pitch_mm": c["du"],
+                   "sod_mm": c["sod"], "sdd_mm": c["sdd"], "filter": "hann", "form": head,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (projections %.1f GB)" % (c["nviews"] * c["nv"] * c["nu"] * 4 / 1e9),
+                   "step": "D2D restore of raw projections + weights + filter + backprojection + clip"},
+        "stages_ms": {"filter": h["filter_ms"], "backprojection": h["bp_ms"]},
+        "roofline": {"bound": "hbm", "achieved": hbm_bytes / bp_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": hbm_bytes / bp_s / 1e9 / hbm_peak, "traffic": None,
+                     "note": "backprojector algorithmic HBM bytes (filtered views read once + volume written "
+                             "once); the kernel is bound by shared-memory gathers, see roofline_smem"},
+        "roofline_smem": {"bound": "smem", "achieved": gather_bytes / bp_s / 1e12,
+                          "peak": smem_bw / 1e12 if "chosen" in res else None, "unit": "TB/s",
+                          "frac": (gather_bytes / bp_s) / smem_bw if "chosen" in res else None,
+                          "bytes_per_update": 4 * esize},
+        "gpu_launches": h["launches"],
+        "clocks": h["clocks"],
+        "accuracy": accuracy,
+    }
+    for form, r in res.items():
+        line[f"form_{form}"] = {"value": world * U / (r["ms"] * 1e-3) / 1e9, "ms_per_step": r["ms"],
+                                "filter_ms": r["filter_ms"], "backprojection_ms": r["bp_ms"],
+                                "gpu_launches": r["launches"], "clocks": r["clocks"]}
+    if "chosen" in res and "plain" in res:
+        line["chosen_over_plain"] = res["plain"]["ms"] / res["chosen"]["ms"]
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        proj, views = cpu_inputs(c, 8 if args.scale == 1 else 4)
+        r = cpu_sample(c, proj, views, target_s=args.cpu_seconds)
+        line["cpu_baseline"] = {
+            "value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+            "sample": (f"{r['sample_rows']} detector rows filtered with the reference's own FFT "
+                       f"({'compiled from its sources' if r['use_ref'] else 'oracle restatement'}), "
+                       f"{r['sample_updates']:.3g} updates of the FP32 CPU backprojector restatement, "
+                       f"extrapolated to the full job ({r['full_seconds']:.0f} s)")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

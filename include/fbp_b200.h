@@ -207,6 +207,14 @@ int fbp_fft_shift_rows(fbp_context* ctx, float* complex_rows, int n, int rows, i
 int fbp_project_ellipsoids_to_projections(fbp_context* ctx, const double* ellipsoids, int count,
                                           const fbp_geometry* geometry);
 
+/* ---- diagnostics --------------------------------------------------------- */
+/* Number of kernels ctx has launched since it was created. */
+int fbp_kernel_launch_count(const fbp_context* ctx, uint64_t* count);
+/* Measured shared-memory load bandwidth of the device (bytes/s, all SMs,
+ * conflict-free 32-bit loads): the roofline denominator of the
+ * backprojector, whose bilinear taps are shared-memory gathers. */
+int fbp_measure_smem_bandwidth(fbp_context* ctx, double* bytes_per_second);
+
 #ifdef __cplusplus
 }
 #endif

@@ -642,31 +642,33 @@ void orc_set_num_threads(int n) { omp_set_num_threads(n); }
 // over voxel columns along the rotation axis, the per-view detector column
 // and weights hoisted out of the y loop). It is the timed CPU baseline for
 // the backprojection stage, labelled "CPU restatement, not reference code":
-// the reference ships no CPU backprojector. It accumulates into vol over the
-// y-slab [y0, y1) and views [k0, k1) so that a bounded sample can be timed.
-extern "C" int orc_bp_cone_f32(const float* q, int nu, int nv, int nviews, double sod, double sdd,
-                               double du, double dv, double span, double offset, int nx, int ny,
-                               int nz, double vox, int y0, int y1, int k0, int k1, float* vol) {
-  std::vector<float> cs(nviews), sn(nviews);
-  for (int k = 0; k < nviews; k++) {
-    double th = offset + span * k / nviews;
-    cs[k] = (float)std::cos(th);
-    sn[k] = (float)std::sin(th);
+// the reference ships no CPU backprojector. q holds the filtered images of
+// the listed views (q[s] is view views[s] of nviews); the sums over those
+// views for y-slices [y0, y1) are added into the slab vol[iz][iy - y0][ix].
+extern "C" int orc_bp_cone_f32(const float* q, const int* views, int nsel, int nu, int nv, int nviews,
+                               double sod, double sdd, double du, double dv, double span, double offset,
+                               int nx, int ny, int nz, double vox, int y0, int y1, float* vol) {
+  std::vector<float> cs(nsel), sn(nsel);
+  for (int s = 0; s < nsel; s++) {
+    double th = offset + span * views[s] / nviews;
+    cs[s] = (float)std::cos(th);
+    sn[s] = (float)std::sin(th);
   }
   const float fsod = (float)sod, fsdd = (float)sdd;
   const float rdu = (float)(1.0 / du), rdv = (float)(1.0 / dv);
   const float cu = nu / 2.0f - 0.5f, cv = nv / 2.0f - 0.5f;
   const float scale = (float)(kPiExact / nviews * sdd / (sod * du));
   const long vsz = (long)nu * nv;
+  const int sy = y1 - y0;
 #pragma omp parallel
   {
-    std::vector<float> acc(std::max(0, y1 - y0));
+    std::vector<float> acc(std::max(0, sy));
 #pragma omp for collapse(2) schedule(dynamic, 8)
     for (int iz = 0; iz < nz; iz++)
       for (int ix = 0; ix < nx; ix++) {
         const float X = (float)((ix + 0.5 - nx / 2.0) * vox), Z = (float)((iz + 0.5 - nz / 2.0) * vox);
         std::fill(acc.begin(), acc.end(), 0.0f);
-        for (int k = k0; k < k1; k++) {
+        for (int k = 0; k < nsel; k++) {
           float L = fsod + X * cs[k] + Z * sn[k];
           float s = -X * sn[k] + Z * cs[k];
           float rL = 1.0f / L;
@@ -700,7 +702,7 @@ extern "C" int orc_bp_cone_f32(const float* q, int nu, int nv, int nviews, doubl
           }
         }
         for (int iy = y0; iy < y1; iy++)
-          vol[((long)iz * ny + iy) * nx + ix] += acc[iy - y0] * scale;
+          vol[((long)iz * sy + (iy - y0)) * nx + ix] += acc[iy - y0] * scale;
       }
   }
   return 0;

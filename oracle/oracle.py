@@ -88,7 +88,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_project_ellipsoids_cone.argtypes = [_D, i, i, i, i, d, d, d, d, d, d, _I, i, _F]
     L.orc_rasterize_ellipses.argtypes = [_D, i, i, i, d, _D]
     L.orc_rasterize_ellipsoids.argtypes = [_D, i, i, i, i, d, _D]
-    L.orc_bp_cone_f32.argtypes = [_F, i, i, i, d, d, d, d, d, d, i, i, i, d, i, i, i, i, _F]
+    L.orc_bp_cone_f32.argtypes = [_F, _I, i, i, i, i, d, d, d, d, d, d, i, i, i, d, i, i, _F]
     L.orc_num_threads.restype = i
     L.orc_set_num_threads.argtypes = [i]
 
@@ -305,13 +305,15 @@ def rasterize_ellipsoids(E: np.ndarray, nx: int, ny: int, nz: int, vox: float) -
 
 
 # ----------------------------------------------------------- CPU baseline legs
-def cpu_bp_cone_f32(q: np.ndarray, g: dict, y0: int, y1: int, k0: int, k1: int,
-                    vol: np.ndarray) -> None:
+def cpu_bp_cone_f32(q: np.ndarray, views, g: dict, y0: int, y1: int, vol: np.ndarray) -> None:
+    """FP32 CPU backprojection of the listed views (q[s] = view views[s]) over
+    the y-slab [y0, y1), added into vol[z][y - y0][x]."""
     q = np.ascontiguousarray(q, dtype=np.float32)
-    nviews, nv, nu = q.shape
-    lib().orc_bp_cone_f32(_f(q), nu, nv, nviews, g["sod"], g["sdd"], g["du"], g["dv"], g["span"],
-                          g["offset"], g["nx"], g["ny"], g["nz"], g["vox"], y0, y1, k0, k1,
-                          _f(vol))
+    nsel, nv, nu = q.shape
+    views = np.ascontiguousarray(views, dtype=np.int32)
+    assert len(views) == nsel and vol.shape == (g["nz"], y1 - y0, g["nx"]) and vol.dtype == np.float32
+    lib().orc_bp_cone_f32(_f(q), views.ctypes.data_as(_I), nsel, nu, nv, g["nviews"], g["sod"], g["sdd"], g["du"],
+                          g["dv"], g["span"], g["offset"], g["nx"], g["ny"], g["nz"], g["vox"], y0, y1, _f(vol))
 
 
 def ref_filter_rows(rows: np.ndarray, filt: int, n: int | None = None,
