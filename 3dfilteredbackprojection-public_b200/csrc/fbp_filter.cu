@@ -25,6 +25,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 namespace fbp {
 namespace {
@@ -508,3 +509,123 @@ int launch_unpack_rows(fbp_context* ctx, const Stack& s, size_t row0, size_t nro
 }
 
 }  // namespace fbp
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of fbp2d_filter_sinogram.
+//
+// Some callers cannot allocate device memory while they run: hosts that hand
+// out all GPU memory from their own pool at start-up, real-time acquisition
+// loops where a cudaMalloc / cudaFree would synchronise the device and stall
+// the detector read-out, and plugins whose host forbids allocations after
+// initialisation. This entry point needs no context and allocates nothing:
+// the filter tables it generates (FP64 response, twiddles, bit-reversed
+// response, spatial kernel) live in the file-scope array below, which every
+// GPU that loads the library holds until the process exits.
+//
+// Capacity: padded row lengths up to kNoAllocMaxN = 4096 samples (rows up to
+// 4096 bins with the default padding). The array is shared by all calls on a
+// device and keeps the last call's tables; each call rewrites every table
+// entry it reads before reading it, so nothing needs clearing. Calls whose
+// work overlaps on the GPU (other streams, other host threads) race on the
+// array and must be serialised by the caller.
+
+namespace {
+constexpr int kNoAllocMaxN = 4096;
+constexpr size_t kNoAllocH = 0;                                         // double[4096]
+constexpr size_t kNoAllocTw = kNoAllocH + sizeof(double) * kNoAllocMaxN;  // float2[2048]
+constexpr size_t kNoAllocHbr = kNoAllocTw + sizeof(float2) * (kNoAllocMaxN / 2);  // float[4096]
+constexpr size_t kNoAllocG = kNoAllocHbr + sizeof(float) * kNoAllocMaxN;           // float[4096]
+constexpr size_t kNoAllocBytes = kNoAllocG + sizeof(float) * kNoAllocMaxN;         // 80 KiB
+}  // namespace
+
+static __device__ __align__(256) unsigned char fbp_noalloc_filter_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the array's host-side name is not a device address).
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fbp::cuda_check(nullptr, e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fbp::set_error(nullptr, FBP_ERR_UNSUPPORTED, "device index above 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, fbp_noalloc_filter_scratch);
+    if (e != cudaSuccess) return fbp::cuda_check(nullptr, e, "cudaGetSymbolAddress(filter scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return FBP_OK;
+}
+}  // namespace
+
+extern "C" int fbp2d_filter_sinogram_noalloc(float* sinogram, int bins, int views, int filter_type, float fan_sdd,
+                                              float detector_width, int padded_length, void* cuda_stream) {
+  using namespace fbp;
+  if (!sinogram || bins <= 0 || views <= 0)
+    return set_error(nullptr, FBP_ERR_INVALID_ARGUMENT, "bad sinogram");
+  if (filter_type < 0 || filter_type > FBP_FILTER_RAMP_SAMPLED)
+    return set_error(nullptr, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
+  if (fan_sdd > 0.f && !(detector_width > 0.f))
+    return set_error(nullptr, FBP_ERR_INVALID_ARGUMENT, "detector width must be positive");
+  int n = padded_length;
+  if (n <= 0) {  // the reference's rule: next power of two >= bins
+    int l = 0;
+    for (long t = 2L * bins - 1; t > 1; t >>= 1) l++;
+    n = l < 31 ? 1 << l : 0;
+  }
+  if (n < bins || n < 2 || (n & (n - 1)))
+    return set_error(nullptr, FBP_ERR_INVALID_ARGUMENT, "padded length must be a power of two >= the row width");
+  if (n > kNoAllocMaxN)
+    return set_error(nullptr, FBP_ERR_UNSUPPORTED,
+                     "padded row length " + std::to_string(n) +
+                         " exceeds the 4096-sample maximum of fbp2d_filter_sinogram_noalloc");
+  void* base = nullptr;
+  if (int rc = noalloc_scratch(&base)) return rc;
+  unsigned char* b = static_cast<unsigned char*>(base);
+  double* H = reinterpret_cast<double*>(b + kNoAllocH);
+  float2* tw = reinterpret_cast<float2*>(b + kNoAllocTw);
+  float* hbr = reinterpret_cast<float*>(b + kNoAllocHbr);
+  float* g = reinterpret_cast<float*>(b + kNoAllocG);
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+  const int blocks = (n + 127) / 128;
+  response_kernel<<<blocks, 128, 0, stream>>>(n, filter_type, H);
+  tables_kernel<<<blocks, 128, 0, stream>>>(n, ilog2(n), H, hbr, tw, g);
+
+  RowSet rs{};
+  rs.data = sinogram;
+  rs.pitch = bins;
+  rs.rows = views;
+  rs.m = bins;
+  rs.n_views = views;
+  rs.n_v = 1;
+  rs.sinogram = false;
+  if (fan_sdd > 0.f) {
+    rs.weight = true;
+    rs.w_sdd = fan_sdd;
+    rs.w_du = detector_width / bins;
+    rs.w_dv = 0.f;
+  }
+  FilterKArgs a;
+  a.rs = rs;
+  a.n = n;
+  a.log2n = ilog2(n);
+  a.pairs_per_cta = std::max(1, std::min(8, 4096 / n));
+  a.npairs = (rs.rows + 1) / 2;
+  a.tw = tw;
+  a.hbr = hbr;
+  const size_t smem = sizeof(float2) * (n / 2) + sizeof(float) * n + sizeof(float2) * n * a.pairs_per_cta;
+  cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  const long long groups = (a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta;
+  const int grid = (int)std::min<long long>(groups, (long long)sms * 4);
+  filter_fft_kernel<<<grid, 256, smem, stream>>>(a);
+  return cuda_check(nullptr, cudaGetLastError(), "fbp2d_filter_sinogram_noalloc");
+}

@@ -134,6 +134,7 @@ SIGNATURES = {
     "fbp_project_backward_parallel_from_sinograms": [_P, _F, _I, _I, _F],
     "fbp_reconstruct_fdk": [_P, C.POINTER(Geometry), _I, _I, _I],
     "fbp2d_filter_sinogram": [_P, _P, _I, _I, _I, _F, _F],
+    "fbp2d_filter_sinogram_noalloc": [_P, _I, _I, _I, _F, _F, _I, _P],
     "fbp2d_project_backward": [_P, _P, _I, _I, C.POINTER(Geometry), _P, _I, _I],
     "fbp2d_parallelize_fan_beam_sinogram": [_P, _P, _I, _I, C.POINTER(Geometry), _P, _I, _F],
     "fbp_fft_rows": [_P, _P, _I, _I, _I],

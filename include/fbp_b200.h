@@ -180,6 +180,20 @@ int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* geometry, int filt
  * spectrum with the surrounding FFFT calls (Mains/fbp_parallel2d_main.cpp:31-41). */
 int fbp2d_filter_sinogram(fbp_context* ctx, float* sinogram, int bins, int views, int filter_type,
                           float fan_sdd, float detector_width);
+/* The same filtering without a context and without allocating device memory,
+ * for callers that must not allocate while they run (hosts that own all GPU
+ * memory through their own pool, real-time read-out loops where an
+ * allocation would synchronise the device, plugin hosts that forbid it).
+ * No counterpart in the reference. Runs on the current device and the given
+ * cudaStream_t (NULL: the legacy default stream); its tables live in an
+ * 80 KiB file-scope device array, so padded_length (0: next power of two >=
+ * bins) may be at most 4096 - longer rows are rejected with
+ * FBP_ERR_UNSUPPORTED. The first call on a device looks up that array's
+ * device address; make it before any stream capture. All calls share the
+ * array: calls whose work overlaps on the GPU race and must be serialised.
+ * Errors are reported through fbp_last_error(NULL). */
+int fbp2d_filter_sinogram_noalloc(float* sinogram, int bins, int views, int filter_type, float fan_sdd,
+                                  float detector_width, int padded_length, void* cuda_stream);
 /* 2D backprojection (FBP2D.cpp:96-122 for parallel beam; flat-detector fan
  * beam for FBP_GEOMETRY_CONE). image has cols x rows = nx x nz pixels of
  * size volume_width/nx. */
