@@ -455,6 +455,7 @@ int fbp_destroy(fbp_context* ctx) {
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_trig);
     cudaFree(ctx->d_span);
+    cudaFree(ctx->d_stage2d);
     cudaFree(ctx->ftab.twiddle);
     cudaFree(ctx->ftab.hbr);
     cudaFree(ctx->ftab.kernel);
@@ -825,8 +826,15 @@ static int stage_2d(fbp_context* ctx, const float* sino, int bins, int views, St
   st.n = views;
   st.pitch = round_up(bins, 4);
   st.filtered = false;
-  char* base = static_cast<char*>(fbp::scratch(ctx, offset_bytes + st.bytes32()));
-  if (!base) return FBP_ERR_OUT_OF_MEMORY;
+  const size_t need = offset_bytes + st.bytes32();
+  if (ctx->stage2d_bytes < need) {
+    cudaFree(ctx->d_stage2d);
+    ctx->d_stage2d = nullptr;
+    ctx->stage2d_bytes = 0;
+    if (fbp::cuda_check(ctx, cudaMalloc(&ctx->d_stage2d, need), "cudaMalloc(2D staging)")) return FBP_ERR_OUT_OF_MEMORY;
+    ctx->stage2d_bytes = need;
+  }
+  char* base = reinterpret_cast<char*>(ctx->d_stage2d);
   st.f32 = reinterpret_cast<float*>(base + offset_bytes);
   return fbp::cuda_check(ctx,
                          cudaMemcpy2DAsync(st.f32, (size_t)st.pitch * 4, sino, (size_t)bins * 4, (size_t)bins * 4,

@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <vector>
 
 namespace fbp {
 namespace {
@@ -50,7 +51,18 @@ struct ViewCoef {
   float Vx, Vz, V0;  // v_local * D at the tile's first y
   float wscale;      // extra per-view weight (FP16 views: 1 / scale)
   int skip;          // tile footprint misses the detector
-  int pad;
+  int box;           // staged window: width (elements) | rows << 16
+};
+
+// Per-view window boxes: a grid of tensor maps over the same filtered stack
+// whose boxes are 1/4 .. 4/4 of the largest window in each dimension; the
+// producer stages each (tile, view) window with the smallest box that holds
+// it, so a copy moves about what the view needs.
+constexpr int kNW = 4, kNH = 4;
+struct BoxMaps {
+  CUtensorMap map[kNW * kNH];  // [width index][height index]
+  int w[kNW];                  // box widths in elements of the layout
+  int h[kNH];                  // box heights in element rows
 };
 
 struct BPArgs {
@@ -64,9 +76,8 @@ struct BPArgs {
   float scale;            // pi / K * filter spacing factor
   const double2* trig;    // (cos, sin) per view
   const float* inv_scale; // FP16 per-view 1/scale or nullptr
-  int box_u, box_v, align;
-  int box_bytes;          // smem bytes reserved per staged window (multiple of 128)
-  int tx_bytes;           // bytes one TMA box transfer delivers (box_u * box_v * element)
+  int box_u, box_v, align;  // largest window (elements, element rows)
+  int box_bytes;            // smem bytes reserved per staged window (multiple of 128)
   int chunk;              // ring stages
   int ntx, ntz;           // tiles along x and z
   int sino_layout;        // tensor coordinates (u, view, v) instead of (u, v, view)
@@ -195,12 +206,12 @@ __device__ __forceinline__ void tile_window(const BPArgs& a, const TileGeo& t, i
 
 // Coefficients for view k of this tile; returns skip.
 __device__ bool tile_view_coef(const BPArgs& a, int k, int ix0, int iy0, int iz0, int ex, int ey, int ez,
-                               ViewCoef& vc, int& u0, int& v0, bool& overflow, bool& behind) {
+                               ViewCoef& vc, int& u0, int& v0, int& need_u, int& need_v, bool& overflow,
+                               bool& behind) {
   TileGeo t;
   tile_geo(a, k, ix0, iy0, iz0, ex, ey, ez, t);
   behind = t.dmin <= 1e-6;
   const bool skip = tile_skip(a, t);
-  int need_u, need_v;
   tile_window(a, t, u0, v0, need_u, need_v);
   overflow = !skip && (need_u > a.box_u || need_v - a.pair_rows > a.box_v);
   const double du0 = a.cu - u0, dv0 = a.cv - v0;
@@ -238,40 +249,41 @@ __device__ __forceinline__ __half2 lds_h2(uint32_t addr) {
   return *reinterpret_cast<__half2*>(&v);
 }
 
-constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: x + kMagic rounds x to an integer
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr uint32_t kMagicBits = 0x4B400000u;
 
-// One bilinear update of voxel j: returns the distance-weighted sample.
-// w = v - 0.5 (v the window-local row coordinate); c0 + bits(w + kMagic) * RB
-// is the address of the element at row floor(v), column iu of the window.
+// One bilinear update of a voxel whose window-local row coordinate is v >= 0:
+// accum += W * sample(u, v). v + kMagic rounded toward zero is
+// kMagic + floor(v), so its bit pattern minus kMagicBits is the row index and
+// c0 + bits * RB the address of the element at (floor(v), iu) (c0 folds the
+// window base, the column and -kMagicBits * RB); no conversion instructions.
+// wa, wb already carry W for the FP32 layouts.
 template <int LAYOUT>
-__device__ __forceinline__ float tap(float w, uint32_t c0, uint32_t RB, float wa, float wb, __half2 fu2, float W) {
-  const float t = w + kMagic;
-  const float fr = w - (t - kMagic);  // v - floor(v) - 0.5, in [-0.5, 0.5]
+__device__ __forceinline__ void tap(float v, uint32_t c0, uint32_t RB, float wa, float wb, __half2 fu2, float W,
+                                    float& accum) {
+  const float t = __fadd_rz(v, kMagic);
+  const float fv = v - (t - kMagic);  // in [0, 1)
   const uint32_t addr = __float_as_uint(t) * RB + c0;
   if constexpr (LAYOUT == kLayoutRaw32) {
     const float p00 = lds_f32(addr), p01 = lds_f32(addr + 4);
     const float p10 = lds_f32(addr + RB), p11 = lds_f32(addr + RB + 4);
     const float r0 = fmaf(wb, p01, wa * p00);
     const float r1 = fmaf(wb, p11, wa * p10);
-    const float d = r1 - r0;
-    return fmaf(fr, d, fmaf(0.5f, d, r0));
+    accum += fmaf(fv, r1 - r0, r0);
   } else if constexpr (LAYOUT == kLayoutPair32) {
     const float2 X = lds_f32x2(addr), Y = lds_f32x2(addr + 8);  // (p00, p10), (p01, p11)
     const float r0 = fmaf(wb, Y.x, wa * X.x);
     const float r1 = fmaf(wb, Y.y, wa * X.y);
-    const float d = r1 - r0;
-    return fmaf(fr, d, fmaf(0.5f, d, r0));
+    accum += fmaf(fv, r1 - r0, r0);
   } else {
     const __half2 X = lds_h2(addr), Y = lds_h2(addr + 4);
     const float2 R = __half22float2(__hfma2(fu2, __hsub2(Y, X), X));  // (row v, row v + 1) lerped in u
-    const float d = R.y - R.x;
-    return W * fmaf(fr, d, fmaf(0.5f, d, R.x));
+    accum = fmaf(W, fmaf(fv, R.y - R.x, R.x), accum);
   }
 }
 
 template <int LAYOUT, int TX, int TZ, int NY, bool KAHAN>
-__global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constant__ CUtensorMap tmap, const BPArgs a) {
+__global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
   static_assert(TX % 8 == 0 && TZ % 4 == 0, "warp tile is 8 x 4 columns");
   constexpr int NCW = TX * TZ / 32;  // consumer warps
   constexpr int KC = 8;              // views per Kahan fold
@@ -301,18 +313,28 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
 
   if (warp == NCW) {
     // ---------------------------------------------------------------- producer
+    // Lane l computes view kb + l of each batch of 32; then the views are
+    // staged in order, each with the smallest box of the grid that holds it.
     int issued = 0;
     for (int kb = 0; kb < a.nviews && !*s_abort; kb += 32) {
       const int k = kb + lane;
       ViewCoef vc;
-      int u0 = 0, v0 = 0;
-      bool skip = true, overflow = false, behind = false;
+      int u0 = 0, v0 = 0, wi = 0, hi = 0;
+      bool skip = true;
+      vc.skip = 1;
       if (k < a.nviews) {
+        bool overflow = false, behind = false;
+        int need_u = 0, need_v = 0;
         // full tile extents: every consumer thread's samples lie in the window
-        skip = tile_view_coef(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, overflow, behind);
+        skip = tile_view_coef(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, need_u, need_v, overflow,
+                              behind);
         if (overflow) atomicCAS(a.err, 0, kDevFootprint);
         if (behind) atomicCAS(a.err, 0, kDevGeometry);
         if (overflow || behind) skip = true, vc.skip = 1;
+        const int rows = need_v - a.pair_rows;  // element rows to stage
+        while (wi < kNW - 1 && maps.w[wi] < need_u) ++wi;
+        while (hi < kNH - 1 && maps.h[hi] < rows) ++hi;
+        vc.box = maps.w[wi] | (maps.h[hi] << 16);
       }
       const int nb = min(32, a.nviews - kb);
       for (int i = 0; i < nb; ++i) {
@@ -325,19 +347,22 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
         if (lane == i) coef[s] = vc;
         const int sk = __shfl_sync(0xffffffffu, (int)skip, i);
         const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
+        const int mi = __shfl_sync(0xffffffffu, wi * kNH + hi, i);
         __syncwarp();
         if (lane == 0) {
           if (sk) {
             mbar_arrive(&full[s]);
           } else {
-            mbar_arrive_expect_tx(&full[s], (uint32_t)a.tx_bytes);
-            void* dst = smem + (size_t)s * a.box_bytes;
+            const CUtensorMap* m = &maps.map[mi];
+            const uint32_t bytes = (uint32_t)(maps.w[mi / kNH] * maps.h[mi % kNH] * (LAYOUT == kLayoutPair32 ? 8 : 4));
+            mbar_arrive_expect_tx(&full[s], bytes);
             const int x = LAYOUT == kLayoutPair32 ? 2 * cu0 : cu0;  // float2 elements are two floats
-            const int e0 = cv0 + a.pair_rows;  // pair layouts: row v lives in element row v + 1
+            const int e0 = cv0 + a.pair_rows;                      // pair layouts: row v is element row v + 1
+            void* dst = smem + (size_t)s * a.box_bytes;
             if (a.sino_layout)
-              tma_load_3d(dst, &tmap, x, kk, e0, &full[s]);
+              tma_load_3d(dst, m, x, kk, e0, &full[s]);
             else
-              tma_load_3d(dst, &tmap, x, e0, kk, &full[s]);
+              tma_load_3d(dst, m, x, e0, kk, &full[s]);
           }
         }
         __syncwarp();
@@ -354,13 +379,10 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   const int tx = (warp % WX) * 8 + (lane & 7);
   const int tz = (warp / WX) * 4 + (lane >> 3);
   const float fx = (float)tx, fz = (float)tz;
-  const int BU = a.box_u, BV = a.box_v;
   constexpr int ESZ = LAYOUT == kLayoutPair32 ? 8 : 4;
-  const uint32_t RB = (uint32_t)(BU * ESZ);
-  // exclusive bound on v, kSlack / 2 inside the window: the footprint pass
-  // leaves kSlack, so the guard never trips for a voxel of the tile, and the
-  // rounded row index can never pass the last staged row
-  const float vmax_ok = (LAYOUT == kLayoutRaw32 ? (float)(BV - 1) : (float)BV) - (float)(kSlack / 2);
+  // rows of a window usable as floor(v): all for pair layouts, all but the
+  // last for the raw layout (it also reads row v + 1)
+  constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
 
   float acc[NY], part[NY], comp[NY];
 #pragma unroll
@@ -387,19 +409,18 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
       const int iu = (int)fuf;
       const float fu = ul - fuf;
       const float vlast = fmaf((float)(NY - 1), dvv, vl);
+      const int BU = g.box & 0xffff, BV = g.box >> 16;
+      const uint32_t RB = (uint32_t)(BU * ESZ);
+      // exclusive bound on v, kSlack / 2 inside the window: the footprint pass
+      // leaves kSlack, so the guard never trips for a voxel of the tile, and
+      // the rounded row index can never pass the last staged row
+      const float vmax_ok = (float)(BV - kRowTail) - (float)(kSlack / 2);
       if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
         const float wa = W - W * fu, wb = W * fu;
         const __half2 fu2 = __float2half2_rn(fu);
         const uint32_t c0 = smem_u32(smem + (size_t)s * a.box_bytes) + (uint32_t)(iu * ESZ) - kMagicBits * RB;
-        const float vlm = vl - 0.5f;
 #pragma unroll
-        for (int j = 0; j < NY; ++j) {
-          const float val = tap<LAYOUT>(fmaf((float)j, dvv, vlm), c0, RB, wa, wb, fu2, W);
-          if (KAHAN)
-            part[j] += val;
-          else
-            acc[j] += val;
-        }
+        for (int j = 0; j < NY; ++j) tap<LAYOUT>(fmaf((float)j, dvv, vl), c0, RB, wa, wb, fu2, W, KAHAN ? part[j] : acc[j]);
       } else {
         bad = true;  // cannot happen when the footprint pass is right; recorded below
       }
@@ -447,38 +468,39 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   }
 }
 
-// Footprint pre-pass: for every (tile, view) the window each tile needs,
-// max-reduced into spans[0] (u) and spans[1] (v). Uses the same FP64 code as
-// the backprojector, so the chosen window always fits.
+// Footprint pre-pass: one warp per tile (lanes over views) finds the
+// largest window any (tile, view) needs; same FP64 code as the
+// backprojector's producer, so the largest box always fits.
 template <int TX, int TZ, int NY>
 __global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
-  const long long total = (long long)a.ntx * a.ntz * nty * a.nviews;
-  int mu = 0, mv = 0;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
-       w += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(w % a.nviews);
-    long long t = w / a.nviews;
-    const int by = (int)(t % nty);
-    t /= nty;
-    const int bx = (int)(t % a.ntx), bz = (int)(t / a.ntx);
+  const long long ntiles = (long long)a.ntx * a.ntz * nty;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  int gu = 0, gv = 0;
+  for (long long T = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); T < ntiles; T += warps) {
+    const int by = (int)(T / ((long long)a.ntx * a.ntz));
+    const int rr = (int)(T - (long long)by * a.ntx * a.ntz);
+    const int bz = rr / a.ntx, bx = rr - bz * a.ntx;
     const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = by * NY;
-    // full tile extents, as the backprojector's producer uses them
-    TileGeo g;
-    tile_geo(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, g);
-    if (g.dmin <= 1e-6) atomicCAS(a.err, 0, kDevGeometry);
-    if (tile_skip(a, g)) continue;
-    int u0, v0, need_u, need_v;
-    tile_window(a, g, u0, v0, need_u, need_v);
-    mu = max(mu, need_u);
-    mv = max(mv, need_v);
+    for (int k = lane; k < a.nviews; k += 32) {
+      TileGeo g;
+      // full tile extents, as the backprojector's producer uses them
+      tile_geo(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, g);
+      if (g.dmin <= 1e-6) atomicCAS(a.err, 0, kDevGeometry);
+      if (tile_skip(a, g)) continue;
+      int u0, v0, nu_, nv_;
+      tile_window(a, g, u0, v0, nu_, nv_);
+      gu = max(gu, nu_);
+      gv = max(gv, nv_);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
-    mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
-    mv = max(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    gu = max(gu, __shfl_xor_sync(0xffffffffu, gu, o));
+    gv = max(gv, __shfl_xor_sync(0xffffffffu, gv, o));
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(spans, mu);
-    atomicMax(spans + 1, mv);
+  if (lane == 0) {
+    atomicMax(spans, gu);
+    atomicMax(spans + 1, gv);
   }
 }
 
@@ -526,25 +548,25 @@ __global__ void rebin_fan_kernel(const float* fan, int bins, int views, double s
 }
 
 template <int LAYOUT, int TX, int TZ, int NY>
-cudaError_t launch_cfg(const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
+cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
   auto kern = kahan ? bp_kernel<LAYOUT, TX, TZ, NY, true> : bp_kernel<LAYOUT, TX, TZ, NY, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.ntx * a.ntz, (a.ny + NY - 1) / NY);
-  kern<<<grid, TX * TZ + 32, smem, stream>>>(map, a);
+  kern<<<grid, TX * TZ + 32, smem, stream>>>(maps, a);
   return cudaGetLastError();
 }
 
 template <int TX, int TZ, int NY>
-cudaError_t launch_layout(int layout, const CUtensorMap& map, const BPArgs& a, size_t smem, bool kahan,
+cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
                           cudaStream_t stream) {
   switch (layout) {
     case kLayoutPair32:
-      return launch_cfg<kLayoutPair32, TX, TZ, NY>(map, a, smem, kahan, stream);
+      return launch_cfg<kLayoutPair32, TX, TZ, NY>(maps, a, smem, kahan, stream);
     case kLayoutPair16:
-      return launch_cfg<kLayoutPair16, TX, TZ, NY>(map, a, smem, kahan, stream);
+      return launch_cfg<kLayoutPair16, TX, TZ, NY>(maps, a, smem, kahan, stream);
     default:
-      return launch_cfg<kLayoutRaw32, TX, TZ, NY>(map, a, smem, kahan, stream);
+      return launch_cfg<kLayoutRaw32, TX, TZ, NY>(maps, a, smem, kahan, stream);
   }
 }
 
@@ -631,84 +653,98 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   double key[16] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
                     (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz,
                     (double)a.align, (double)NY};
-  bool hit = ctx->plan.valid;
-  for (int i = 0; i < 16 && hit; ++i) hit = ctx->plan.key[i] == key[i];
+  fbp_context::BPPlan& plan = ctx->plan;
+  bool hit = plan.valid;
+  for (int i = 0; i < 16 && hit; ++i) hit = plan.key[i] == key[i];
   if (!hit) {
-    if (!ctx->d_span && cuda_check(ctx, cudaMalloc(&ctx->d_span, 4 * sizeof(int)), "cudaMalloc(span)"))
-      return FBP_ERR_OUT_OF_MEMORY;
+    plan.valid = false;
+    if (ctx->span_cap < 4) {
+      cudaFree(ctx->d_span);
+      ctx->d_span = nullptr;
+      ctx->span_cap = 0;
+      if (cuda_check(ctx, cudaMalloc(&ctx->d_span, sizeof(int) * 4), "cudaMalloc(footprint spans)"))
+        return FBP_ERR_OUT_OF_MEMORY;
+      ctx->span_cap = 4;
+    }
     cudaMemsetAsync(ctx->d_span, 0, 4 * sizeof(int), ctx->stream);
-    long long total = (long long)a.ntx * a.ntz * nty * g.nviews;
-    int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 32);
+    const long long ntiles = (long long)a.ntx * a.ntz * nty;
+    const int blocks = (int)std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)ctx->num_sms * 16));
     if (is2d)
       footprint_kernel<16, 16, 1><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
     else
       footprint_kernel<16, 16, 16><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
-    int spans[4] = {0, 0, 0, 0};
     if (int rc = launched(ctx, "footprint_kernel")) return rc;
-    if (int rc = cuda_check(ctx, cudaMemcpyAsync(spans, ctx->d_span, sizeof(spans), cudaMemcpyDeviceToHost,
-                                                 ctx->stream),
-                            "footprint readback"))
-      return rc;
-    if (int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync")) return rc;
-    ctx->plan.valid = true;
-    for (int i = 0; i < 16; ++i) ctx->plan.key[i] = key[i];
-    ctx->plan.box_u = std::max(spans[0], 2);
-    ctx->plan.box_v = std::max(spans[1], 2);
+    int hs[4] = {0, 0, 0, 0};
+    if (cuda_check(ctx, cudaMemcpyAsync(hs, ctx->d_span, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream), "spans") ||
+        cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync"))
+      return FBP_ERR_CUDA;
+    plan.box_u = std::max(hs[0], 2);
+    plan.box_v = std::max(hs[1], 2);
+    plan.valid = true;
+    for (int i = 0; i < 16; ++i) plan.key[i] = key[i];
   }
-  int bu = (ctx->plan.box_u + a.align - 1) / a.align * a.align;
+  const int bu = (plan.box_u + a.align - 1) / a.align * a.align;
   // a pair element carries row v + 1 with it: one row less to stage
-  int bv = layout == kLayoutRaw32 ? ctx->plan.box_v : std::max(1, ctx->plan.box_v - 1);
-  a.box_u = bu;
-  a.box_v = bv;
-  const int box_x = layout == kLayoutPair32 ? 2 * bu : bu;  // TMA box inner extent in 4-byte elements
-  if (box_x > 256 || bv > 256)
+  const int bv = layout == kLayoutRaw32 ? plan.box_v : std::max(1, plan.box_v - 1);
+  if ((layout == kLayoutPair32 ? 2 * bu : bu) > 256 || bv > 256)
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
                      "detector footprint of a voxel tile exceeds the 256-element TMA box; geometry magnification "
                      "too large for the staged backprojector");
-  a.tx_bytes = bu * bv * esize;
-  a.box_bytes = (a.tx_bytes + 127) / 128 * 128;
+  a.box_u = bu;
+  a.box_v = bv;
+  a.box_bytes = (bu * bv * esize + 127) / 128 * 128;
   // two CTAs per SM: each gets half of the 228 KB shared memory
   const size_t smem_cap = 113 * 1024;
   const size_t per_stage = a.box_bytes + sizeof(ViewCoef) + 2 * sizeof(uint64_t);
-  int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
+  const int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
   if (stages < 2) return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
   a.chunk = stages;
   const size_t smem = (size_t)stages * per_stage + 64;
 
-  // tensor map over the filtered stack (4-byte elements; float2 as two floats)
+  // the grid of boxes over the filtered stack (4-byte elements; float2 as two floats)
   const void* base = st.filtered ? st.filt : (const void*)st.f32;
   const int pitch_el = st.filtered ? st.filt_pitch : st.pitch;
   const uint64_t pitch_bytes = (uint64_t)pitch_el * esize;
   const uint64_t ux = layout == kLayoutPair32 ? 2ull * st.u : (uint64_t)st.u;
   const uint64_t rows_v = layout == kLayoutRaw32 ? (uint64_t)st.v : (uint64_t)st.v + 1;  // element rows per view
-  uint64_t dims[3], strides[2];
-  uint32_t box[3];
-  if (st.sinogram) {  // [v][view][u]
-    dims[0] = ux;
-    dims[1] = st.n;
-    dims[2] = rows_v;
-    strides[0] = pitch_bytes;
-    strides[1] = pitch_bytes * st.n;
-    box[0] = box_x;
-    box[1] = 1;
-    box[2] = bv;
-  } else {  // [view][v][u]
-    dims[0] = ux;
-    dims[1] = rows_v;
-    dims[2] = st.n;
-    strides[0] = pitch_bytes;
-    strides[1] = pitch_bytes * rows_v;
-    box[0] = box_x;
-    box[1] = bv;
-    box[2] = 1;
+  BoxMaps maps;
+  for (int i = 0; i < kNW; ++i) {
+    const int w = (bu * (i + 1) + kNW - 1) / kNW;
+    maps.w[i] = std::max(a.align, (w + a.align - 1) / a.align * a.align);
   }
-  CUtensorMap map;
-  if (int rc = make_tensor_map_3d(ctx, &map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, const_cast<void*>(base), dims, strides,
-                                  box))
-    return rc;
-
-  cudaError_t e = is2d ? launch_layout<16, 16, 1>(layout, map, a, smem, kahan, ctx->stream)
-                       : launch_layout<16, 16, 16>(layout, map, a, smem, kahan, ctx->stream);
+  for (int j = 0; j < kNH; ++j) maps.h[j] = std::max(1, (bv * (j + 1) + kNH - 1) / kNH);
+  maps.w[kNW - 1] = bu;
+  maps.h[kNH - 1] = bv;
+  for (int i = 0; i < kNW; ++i)
+    for (int j = 0; j < kNH; ++j) {
+      const uint32_t box_x = layout == kLayoutPair32 ? 2 * maps.w[i] : maps.w[i];  // in 4-byte elements
+      uint64_t dims[3], strides[2];
+      uint32_t box[3];
+      if (st.sinogram) {  // [v][view][u]
+        dims[0] = ux;
+        dims[1] = st.n;
+        dims[2] = rows_v;
+        strides[0] = pitch_bytes;
+        strides[1] = pitch_bytes * st.n;
+        box[0] = box_x;
+        box[1] = 1;
+        box[2] = maps.h[j];
+      } else {  // [view][v][u]
+        dims[0] = ux;
+        dims[1] = rows_v;
+        dims[2] = st.n;
+        strides[0] = pitch_bytes;
+        strides[1] = pitch_bytes * rows_v;
+        box[0] = box_x;
+        box[1] = maps.h[j];
+        box[2] = 1;
+      }
+      if (int rc = make_tensor_map_3d(ctx, &maps.map[i * kNH + j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                      const_cast<void*>(base), dims, strides, box))
+        return rc;
+    }
+  cudaError_t e = is2d ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
+                       : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
   return cuda_check(ctx, e, "bp_kernel");
 }

@@ -92,7 +92,10 @@ struct fbp_context {
   double2* d_trig = nullptr;     // per-view (cos, sin) in FP64
   int trig_cap = 0;
   double trig_key[3] = {-1, 0, 0};  // (views, span, offset) of the table in d_trig
-  int* d_span = nullptr;         // footprint pre-pass results
+  int* d_span = nullptr;         // footprint pre-pass results (spans + per-tile needs)
+  size_t span_cap = 0;           // ints in d_span
+  float* d_stage2d = nullptr;    // 2D sinograms restaged with 16-byte row pitch
+  size_t stage2d_bytes = 0;
   fbp::FilterTables ftab;
   void* d_scratch = nullptr;     // generic scratch (row shifts, Toeplitz operands)
   size_t scratch_bytes = 0;
@@ -100,6 +103,8 @@ struct fbp_context {
   size_t h_pinned_bytes = 0;
 
   // cached footprint plan
+  // cached backprojection plan: the largest detector window of any
+  // (tile, view) for the geometry (samples, rows including row v + 1)
   struct BPPlan {
     bool valid = false;
     double key[16] = {0};
