@@ -521,6 +521,15 @@ int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable) {
   return FBP_OK;
 }
 
+int fbp_set_backprojector(fbp_context* ctx, int variant) {
+  FBP_CTX(ctx);
+  if (variant < FBP_BACKPROJECTOR_AUTO || variant > FBP_BACKPROJECTOR_SYMMETRIC)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown backprojector variant");
+  ctx->bp_variant = variant;
+  ctx->plan.valid = false;
+  return FBP_OK;
+}
+
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes) {
   if (!ctx || !bytes) return FBP_ERR_INVALID_ARGUMENT;
   size_t b = 0;

@@ -468,6 +468,280 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   }
 }
 
+// ---------------------------------------------------------------------------
+// Four-fold symmetric backprojector.
+//
+// On a circular orbit with K views over one turn (K % 4 == 0) and a square
+// volume (nx == nz), voxel P = (X, Z) at view k and the voxel rotated by 90
+// degrees, (-Z, X), at view k + K/4 project to the same detector coordinate
+// (t = X cos + Z sin and s = -X sin + Z cos are unchanged). A CTA therefore
+// owns an orbit of four 16 x 16 x NY tiles (a tile of the lower-left quadrant
+// and its three rotations) and walks all K views m of the representative
+// tile: the producer computes the tile footprint and coefficients once per m
+// and stages the windows of views m + r K/4 (mod K), r = 0..3 (same origin
+// and box), which feed the r-th rotated tile; each consumer thread forms its
+// detector column, weights and v steps once per m and applies every
+// floor / fraction / address to four accumulator sets. Windows live in a byte ring
+// (entries of variable size, freed in order), so typical small windows keep
+// several quads in flight while the largest still fits.
+
+constexpr int kQuadEntries = 8;  // outstanding view-quads per CTA
+constexpr int kKahanQuads = 4;   // quads (16 views) per Kahan fold
+
+struct QuadCoef {
+  float Dx, Dz, D0, Nx, Nz, N0, Vx, Vz, V0;
+  float ws[4];  // per-view extra weight of the four views (FP16 views: 1 / scale)
+  int skip;
+  int box;      // staged window: width (elements) | rows << 16
+  int off;      // byte offset of the entry's first window in the ring
+  int sub;      // bytes between the entry's four windows
+  int pad[3];
+};
+
+template <int LAYOUT, int NY, bool KAHAN>
+__global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
+  constexpr int TX = 16, TZ = 16, NCW = 8, E = kQuadEntries;
+  constexpr int ESZ = LAYOUT == kLayoutPair32 ? 8 : 4;
+  constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int R = a.box_bytes;  // ring bytes
+  const int K = a.nviews, Q = K >> 2;
+  const int nbh = a.ntx >> 1;  // representative tiles per axis (lower-left quadrant)
+  const int bx = blockIdx.x % nbh, bz = blockIdx.x / nbh;
+  const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
+
+  QuadCoef* coef = reinterpret_cast<QuadCoef*>(smem + R);
+  uint64_t* full = reinterpret_cast<uint64_t*>(coef + E);
+  uint64_t* empty = full + E;
+  int* end_pos = reinterpret_cast<int*>(empty + E);
+  volatile int* s_abort = end_pos + E;
+  float* comp = reinterpret_cast<float*>(smem + R + E * sizeof(QuadCoef) + E * 16 + E * 4 + 64);
+
+  if (tid == 0) {
+    *s_abort = *(volatile int*)a.err != 0;
+    for (int e = 0; e < E; ++e) {
+      mbar_init(&full[e], 1);
+      mbar_init(&empty[e], NCW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (*s_abort) return;
+
+  if (warp == NCW) {
+    // ---------------------------------------------------------------- producer
+    int head = 0, tail = 0, oldest = 0, issued = 0;
+    for (int kb = 0; kb < K && !*s_abort; kb += 32) {
+      const int k = kb + lane;  // view of the representative tile; rotation r uses view (k + r Q) mod K
+      QuadCoef qc;
+      int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
+      bool skip = true;
+      qc.skip = 1;
+      if (k < K) {
+        ViewCoef vc;
+        bool overflow = false, behind = false;
+        int need_u = 0, need_v = 0;
+        skip = tile_view_coef(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, need_u, need_v, overflow,
+                              behind);
+        if (overflow) atomicCAS(a.err, 0, kDevFootprint);
+        if (behind) atomicCAS(a.err, 0, kDevGeometry);
+        if (overflow || behind) skip = true;
+        int wi = 0, hi = 0;
+        const int rows = need_v - a.pair_rows;
+        while (wi < kNW - 1 && maps.w[wi] < need_u) ++wi;
+        while (hi < kNH - 1 && maps.h[hi] < rows) ++hi;
+        mi = wi * kNH + hi;
+        tx_bytes = maps.w[wi] * maps.h[hi] * ESZ;
+        sub = (tx_bytes + 127) & ~127;
+        need = skip ? 0 : 4 * sub;
+        qc.Dx = vc.Dx; qc.Dz = vc.Dz; qc.D0 = vc.D0;
+        qc.Nx = vc.Nx; qc.Nz = vc.Nz; qc.N0 = vc.N0;
+        qc.Vx = vc.Vx; qc.Vz = vc.Vz; qc.V0 = vc.V0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) qc.ws[r] = a.inv_scale ? a.inv_scale[(k + r * Q) % K] : 1.0f;
+        qc.skip = skip;
+        qc.box = maps.w[wi] | (maps.h[hi] << 16);
+        qc.sub = sub;
+      }
+      const int nb = min(32, K - kb);
+      for (int i = 0; i < nb; ++i) {
+        const int q = kb + i;
+        const int e = q % E;
+        const int qneed = __shfl_sync(0xffffffffu, need, i);
+        // allocate qneed contiguous ring bytes: wrap to 0 when the tail end is too short
+        const int pos = head % R;
+        const int start = pos + qneed > R ? head + (R - pos) : head;
+        bool ok = true;
+        while (oldest < q && (oldest <= q - E || start + qneed - tail > R)) {
+          if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, a.err)) {
+            ok = false;
+            break;
+          }
+          tail = end_pos[oldest % E];
+          ++oldest;
+        }
+        if (!ok) {
+          *s_abort = 1;
+          break;
+        }
+        if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
+        const int off = start % R;
+        if (lane == i) {
+          qc.off = off;
+          coef[e] = qc;
+        }
+        if (lane == 0) end_pos[e] = start + qneed;
+        head = start + qneed;
+        const int sk = __shfl_sync(0xffffffffu, (int)skip, i);
+        const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
+        const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
+        const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
+        __syncwarp();
+        if (lane == 0) {
+          if (sk) {
+            mbar_arrive(&full[e]);
+          } else {
+            mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
+            const CUtensorMap* m = &maps.map[cmi];
+            const int x = LAYOUT == kLayoutPair32 ? 2 * cu0 : cu0;
+            const int e0 = cv0 + a.pair_rows;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              void* dst = smem + off + r * csub;
+              const int kv = (q + r * Q) % K;
+              if (a.sino_layout)
+                tma_load_3d(dst, m, x, kv, e0, &full[e]);
+              else
+                tma_load_3d(dst, m, x, e0, kv, &full[e]);
+            }
+          }
+        }
+        __syncwarp();
+        issued = q + 1;
+      }
+    }
+    // leave only when every copy issued into this CTA's memory has landed
+    for (int q = max(0, issued - E); q < issued; ++q) mbar_wait(&full[q % E], (q / E) & 1, a.err);
+    return;
+  }
+
+  // ------------------------------------------------------------------ consumers
+  const int tx = (warp & 1) * 8 + (lane & 7);
+  const int tz = (warp >> 1) * 4 + (lane >> 3);
+  const float fx = (float)tx, fz = (float)tz;
+  float acc[4][NY], part[KAHAN ? 4 : 1][KAHAN ? NY : 1];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int j = 0; j < NY; ++j) acc[r][j] = 0.f;
+  if (KAHAN) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int j = 0; j < NY; ++j) {
+        part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
+        comp[(r * NY + j) * 256 + tid] = 0.f;
+      }
+  }
+  const uint32_t ring = smem_u32(smem);
+  int e = 0;
+  uint32_t ph = 0;
+  int kq = 0;
+  bool bad = false;
+  for (int q = 0; q < K; ++q) {
+    if (!mbar_wait(&full[e], ph, a.err)) {
+      *s_abort = 1;
+      break;
+    }
+    const QuadCoef g = coef[e];
+    if (!g.skip) {
+      const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
+      const float rD = __frcp_rn(D);
+      const float ul = fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)) * rD;
+      const float vl = fmaf(g.Vx, fx, fmaf(g.Vz, fz, g.V0)) * rD;
+      const float dvv = a.dvn * rD;
+      const float W = rD * rD;
+      const float fuf = floorf(ul);
+      const int iu = (int)fuf;
+      const float fu = ul - fuf;
+      const float vlast = fmaf((float)(NY - 1), dvv, vl);
+      const int BU = g.box & 0xffff, BV = g.box >> 16;
+      const uint32_t RB = (uint32_t)(BU * ESZ);
+      const float vmax_ok = (float)(BV - kRowTail) - (float)(kSlack / 2);
+      if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
+        const uint32_t sub = (uint32_t)g.sub;
+        const uint32_t c0 = ring + (uint32_t)g.off + (uint32_t)(iu * ESZ) - kMagicBits * RB;
+        float wa[4], wb[4], Wr[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          Wr[r] = W * g.ws[r];
+          wa[r] = Wr[r] - Wr[r] * fu;
+          wb[r] = Wr[r] * fu;
+        }
+        const __half2 fu2 = __float2half2_rn(fu);
+#pragma unroll
+        for (int j = 0; j < NY; ++j) {
+          const float v = fmaf((float)j, dvv, vl);
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu2, Wr[r], KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j]);
+        }
+      } else {
+        bad = true;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[e]);
+    if (++e == E) {
+      e = 0;
+      ph ^= 1;
+    }
+    if (KAHAN && ++kq == kKahanQuads) {
+      kq = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int j = 0; j < NY; ++j) {
+          float& c = comp[(r * NY + j) * 256 + tid];
+          const float y = part[KAHAN ? r : 0][KAHAN ? j : 0] - c;
+          const float t = acc[r][j] + y;
+          c = (t - acc[r][j]) - y;
+          acc[r][j] = t;
+          part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
+        }
+    }
+  }
+  if (bad) atomicCAS(a.err, 0, kDevFootprint);
+  if (KAHAN) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int j = 0; j < NY; ++j) acc[r][j] += part[KAHAN ? r : 0][KAHAN ? j : 0] - comp[(r * NY + j) * 256 + tid];
+  }
+  if (*s_abort) return;
+
+  // four rotated columns: (x, z) -> (n-1-z, x) -> (n-1-x, n-1-z) -> (z, n-1-x)
+  const int n = a.nx;
+  const int ix = ix0 + tx, iz = iz0 + tz;
+  const int cx[4] = {ix, n - 1 - iz, n - 1 - ix, iz};
+  const int cz[4] = {iz, ix, n - 1 - iz, n - 1 - ix};
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    float* out = a.vol + ((size_t)cz[r] * a.ny) * a.nx + cx[r];
+#pragma unroll
+    for (int j = 0; j < NY; ++j) {
+      const int iy = iy0 + j;
+      if (iy < a.ny) {
+        float val = acc[r][j] * a.scale;
+        if (iy < a.clip_ylimit) val = fmaxf(val, 0.f);
+        out[(size_t)iy * a.nx] = val;
+      }
+    }
+  }
+}
+
 // Footprint pre-pass: one warp per tile (lanes over views) finds the
 // largest window any (tile, view) needs; same FP64 code as the
 // backprojector's producer, so the largest box always fits.
@@ -557,6 +831,28 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
   return cudaGetLastError();
 }
 
+template <int LAYOUT>
+cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
+  auto kern = kahan ? bp_quad_kernel<LAYOUT, 8, true> : bp_quad_kernel<LAYOUT, 8, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.ntx / 2) * (a.ntz / 2), (a.ny + 7) / 8);
+  kern<<<grid, 256 + 32, smem, stream>>>(maps, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quad(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
+                        cudaStream_t stream) {
+  switch (layout) {
+    case kLayoutPair32:
+      return launch_quad_cfg<kLayoutPair32>(maps, a, smem, kahan, stream);
+    case kLayoutPair16:
+      return launch_quad_cfg<kLayoutPair16>(maps, a, smem, kahan, stream);
+    default:
+      return launch_quad_cfg<kLayoutRaw32>(maps, a, smem, kahan, stream);
+  }
+}
+
 template <int TX, int TZ, int NY>
 cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
                           cudaStream_t stream) {
@@ -642,9 +938,20 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   }
   a.trig = ctx->d_trig;
 
-  // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
+  // Four-fold symmetric path: square volume, views over one turn (or
+  // 4m + 1 turns) with K % 4 == 0, an even number of 16-wide tiles per axis.
   const bool is2d = g.ny == 1;
-  const int TX = 16, TZ = 16, NY = is2d ? 1 : 16;
+  const double turns = g.span / (2.0 * pi);
+  const long long iturns = llround(turns);
+  const bool symmetric = !is2d && g.nx == g.nz && g.nx % 32 == 0 && g.nviews % 4 == 0 &&
+                         fabs(turns - (double)iturns) < 1e-9 && iturns % 4 == 1;
+  const bool quad = symmetric && ctx->bp_variant != FBP_BACKPROJECTOR_GENERIC;
+  if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC && !symmetric)
+    return set_error(ctx, FBP_ERR_UNSUPPORTED,
+                     "the four-fold symmetric backprojector needs nx == nz (a multiple of 32), views % 4 == 0 and "
+                     "views over one full turn");
+  // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
+  const int TX = 16, TZ = 16, NY = is2d ? 1 : (quad ? 8 : 16);
   a.ntx = (g.nx + TX - 1) / TX;
   a.ntz = (g.nz + TZ - 1) / TZ;
   const int nty = (g.ny + NY - 1) / NY;
@@ -671,6 +978,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
     const int blocks = (int)std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)ctx->num_sms * 16));
     if (is2d)
       footprint_kernel<16, 16, 1><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
+    else if (NY == 8)
+      footprint_kernel<16, 16, 8><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
     else
       footprint_kernel<16, 16, 16><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
     if (int rc = launched(ctx, "footprint_kernel")) return rc;
@@ -692,14 +1001,43 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
                      "too large for the staged backprojector");
   a.box_u = bu;
   a.box_v = bv;
-  a.box_bytes = (bu * bv * esize + 127) / 128 * 128;
   // two CTAs per SM: each gets half of the 228 KB shared memory
   const size_t smem_cap = 113 * 1024;
-  const size_t per_stage = a.box_bytes + sizeof(ViewCoef) + 2 * sizeof(uint64_t);
-  const int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
-  if (stages < 2) return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
-  a.chunk = stages;
-  const size_t smem = (size_t)stages * per_stage + 64;
+  const size_t max_box = (size_t)(bu * bv * esize + 127) / 128 * 128;
+  size_t smem = 0;
+  bool use_quad = quad;
+  if (use_quad) {
+    // byte ring for the windows + entry records (+ Kahan compensations)
+    const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(int)) + 64;
+    const size_t comp = kahan ? (size_t)4 * 8 * 256 * sizeof(float) : 0;
+    const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
+    if (4 * max_box > ring) {
+      use_quad = false;  // the largest quad does not fit: generic path
+      if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC)
+        return set_error(ctx, FBP_ERR_UNSUPPORTED, "detector windows too large for the symmetric backprojector");
+    } else {
+      a.box_bytes = (int)ring;
+      smem = ring + fixed + comp;
+    }
+  }
+  if (!use_quad) {
+    if (quad) {
+      // re-plan with the generic tile height
+      ctx->plan.valid = false;
+      const int saved = ctx->bp_variant;
+      ctx->bp_variant = FBP_BACKPROJECTOR_GENERIC;
+      const int rc = launch_backproject(ctx, g, st, vol, clip_ylimit, kahan);
+      ctx->bp_variant = saved;
+      return rc;
+    }
+    a.box_bytes = (int)max_box;
+    const size_t per_stage = a.box_bytes + sizeof(ViewCoef) + 2 * sizeof(uint64_t);
+    const int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
+    if (stages < 2)
+      return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
+    a.chunk = stages;
+    smem = (size_t)stages * per_stage + 64;
+  }
 
   // the grid of boxes over the filtered stack (4-byte elements; float2 as two floats)
   const void* base = st.filtered ? st.filt : (const void*)st.f32;
@@ -743,8 +1081,9 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
                                       const_cast<void*>(base), dims, strides, box))
         return rc;
     }
-  cudaError_t e = is2d ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
-                       : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
+  cudaError_t e = use_quad ? launch_quad(layout, maps, a, smem, kahan, ctx->stream)
+                 : is2d   ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
+                          : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
   return cuda_check(ctx, e, "bp_kernel");
 }

@@ -79,6 +79,7 @@ struct fbp_context {
   int filter_impl = FBP_FILTER_IMPL_AUTO;
   int pad_len = 0;
   int clip_after_bp = 1;
+  int bp_variant = FBP_BACKPROJECTOR_AUTO;
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched by this context
 

@@ -49,6 +49,12 @@ class Precision(enum.IntEnum):
     MIXED = 1
 
 
+class Backprojector(enum.IntEnum):
+    AUTO = 0
+    GENERIC = 1
+    SYMMETRIC = 2
+
+
 class FilterImpl(enum.IntEnum):
     AUTO = 0
     FFT = 1
@@ -94,6 +100,7 @@ SIGNATURES = {
     "fbp_set_filter_impl": [_P, _I],
     "fbp_set_filter_padding": [_P, _I],
     "fbp_set_clip_after_backprojection": [_P, _I],
+    "fbp_set_backprojector": [_P, _I],
     "fbp_memory_in_use": [_P, C.POINTER(C.c_size_t)],
     "fbp_generate_blank_volume": [_P, _I, _I, _I],
     "fbp_generate_blank_projections": [_P, _I, _I, _I],
@@ -227,6 +234,9 @@ class FBP3D:
 
     def set_filter_padding(self, padded_length: int) -> None:
         self.ctx.call("fbp_set_filter_padding", int(padded_length))
+
+    def set_backprojector(self, variant: int) -> None:
+        self.ctx.call("fbp_set_backprojector", int(variant))
 
     def set_clip_after_backprojection(self, enable: bool) -> None:
         self.ctx.call("fbp_set_clip_after_backprojection", int(bool(enable)))

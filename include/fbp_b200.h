@@ -58,6 +58,12 @@ extern "C" {
 #define FBP_FILTER_IMPL_FFT 1      /* batched shared-memory FFT             */
 #define FBP_FILTER_IMPL_TOEPLITZ 2 /* tcgen05 split-BF16 Toeplitz GEMM       */
 
+/* ---- backprojector variants ----------------------------------------------- */
+#define FBP_BACKPROJECTOR_AUTO 0      /* symmetric when the geometry allows it      */
+#define FBP_BACKPROJECTOR_GENERIC 1   /* one 16x16x16 tile per CTA, any geometry    */
+#define FBP_BACKPROJECTOR_SYMMETRIC 2 /* four-fold orbit of tiles per CTA: square  */
+                                      /* volume, views % 4 == 0 over one full turn */
+
 /* ---- geometry kinds ------------------------------------------------------- */
 #define FBP_GEOMETRY_CONE 0     /* flat-panel cone beam, circular orbit         */
 #define FBP_GEOMETRY_PARALLEL 1 /* parallel beam (3D: stacked 2D)               */
@@ -102,6 +108,8 @@ int fbp_set_filter_padding(fbp_context* ctx, int padded_length);
 /* 1 (default): project_backward_* end with clip_negatives_of_volume as the
  * reference does (FBP3D.cpp:489,521,558,592); 0: leave negatives. */
 int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable);
+/* Backprojector variant (FBP_BACKPROJECTOR_*); AUTO by default. */
+int fbp_set_backprojector(fbp_context* ctx, int variant);
 /* Device bytes held by ctx's buffers. */
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
 

@@ -312,3 +312,66 @@ def test_fft_rows_mirror(fbp):
     assert np.allclose(f.inverse_fft_radix2(f.fft_radix2(z)), z, atol=1e-5)
     assert np.array_equal(f.fft_shift(z), np.roll(z, 128, axis=1))
     assert np.array_equal(f.inverse_fft_shift(z, 3), np.roll(z, -3, axis=1))
+
+
+# ----------------------------------------------------- backprojector variants
+def _sym_case(oracle, nviews=96, n=64, ny=40, offset=0.2):
+    c = dict(sod=300.0, sdd=520.0, du=1.25, dv=1.25, span=2 * math.pi, offset=offset, nu=96, nv=72,
+             nviews=nviews, nx=n, ny=ny, nz=n, vox=2.0)
+    from phantoms import random_ellipsoids
+    E = random_ellipsoids(np.random.default_rng(31), 12, 0.5 * n * c["vox"])
+    return c, oracle.project_ellipsoids_cone(E, c)
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_backprojector_variants_fp32(fbp, oracle, variant):
+    """Generic (1) and four-fold symmetric (2) backprojectors against the
+    oracle on a geometry both accept (square volume, 96 views, one turn)."""
+    c, proj = _sym_case(oracle)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_backprojector(variant)
+    got = _gpu_fdk(s, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    assert relative_rmse(got, ref) < TOL_FP32
+
+
+@pytest.mark.parametrize("factor", [2, 1])
+def test_symmetric_backprojector_mixed(fbp, oracle, phantoms, factor):
+    """MIXED form through the four-fold symmetric backprojector on the 256^3
+    workload geometry (360 views) and its half-size version (180 views)."""
+    c, proj = _cone_case(phantoms, oracle, factor) if factor > 1 else (
+        phantoms.config_cone256(),
+        oracle.project_ellipsoids_cone(phantoms.ellipsoids_for(phantoms.config_cone256()), phantoms.config_cone256()))
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED)
+    s.set_backprojector(fbp.Backprojector.SYMMETRIC)
+    got = _gpu_fdk(s, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    err = relative_rmse(got, ref)
+    print(f"mixed symmetric {c['nx']}^3 rel RMSE {err:.3e}")
+    assert err < TOL_MIXED
+
+
+def test_symmetric_backprojector_sinograms_and_clip(fbp, oracle):
+    c, proj = _sym_case(oracle, nviews=64, n=64, ny=20, offset=0.0)
+    sod, odd, w, vw, rot = _cone_args(c)
+    s = fbp.FBP3D(0)
+    s.set_backprojector(fbp.Backprojector.SYMMETRIC)
+    s.upload_sinograms(np.ascontiguousarray(proj.transpose(1, 0, 2)))
+    s.apply_fdk_weights_to_sinograms(sod, odd, w)
+    s.apply_filter_to_sinograms(2)
+    s.project_backward_cone_fdk_from_sinograms(sod, odd, w, vw, rot, c["nx"], c["ny"], 0.0)
+    got = s.read_volume()
+    ref = oracle.clip_negatives(oracle.fdk(proj, c, 2), y_limit=c["nz"])
+    assert relative_rmse(got, ref) < TOL_FP32
+
+
+def test_symmetric_backprojector_rejects_other_geometries(fbp, oracle):
+    c, proj = _sym_case(oracle, nviews=90)
+    s = fbp.FBP3D(0)
+    s.set_backprojector(fbp.Backprojector.SYMMETRIC)
+    with pytest.raises(fbp.FBPError) as e:
+        _gpu_fdk(s, c, proj, 0)
+    assert e.value.status == -6
