@@ -397,6 +397,27 @@ int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType d
   return FBP_OK;
 }
 
+int make_tensor_map_2d_bf16_sw128(fbp_context* ctx, CUtensorMap* map, void* base, uint64_t inner, uint64_t outer,
+                                  uint64_t pitch_bytes, uint32_t box_inner, uint32_t box_outer) {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t gdim[2] = {inner, outer};
+  cuuint64_t gstr[1] = {pitch_bytes};
+  cuuint32_t bdim[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, gdim, gstr, bdim, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return FBP_OK;
+}
+
 }  // namespace fbp
 
 extern "C" {
@@ -459,6 +480,7 @@ int fbp_destroy(fbp_context* ctx) {
     cudaFree(ctx->ftab.twiddle);
     cudaFree(ctx->ftab.hbr);
     cudaFree(ctx->ftab.kernel);
+    cudaFree(ctx->ttab.th);
     cudaFree(ctx->d_scratch);
     cudaFreeHost(ctx->h_pinned);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);

@@ -68,6 +68,13 @@ struct FilterTables {
   float* kernel = nullptr;    // n entries: spatial kernel g = IDFT(H) (circular)
 };
 
+// Toeplitz operands of the tensor-core filter: Bt[i][k] = g[(i - k) mod n]
+// for i < m, k < kp (zero for k >= m), as BF16 hi rows then BF16 lo rows.
+struct ToeplitzTables {
+  int m = 0, n = 0, filter = -1;
+  void* th = nullptr;  // 2 * m * kp BF16 values
+};
+
 }  // namespace fbp
 
 struct fbp_context {
@@ -98,6 +105,7 @@ struct fbp_context {
   float* d_stage2d = nullptr;    // 2D sinograms restaged with 16-byte row pitch
   size_t stage2d_bytes = 0;
   fbp::FilterTables ftab;
+  fbp::ToeplitzTables ttab;
   void* d_scratch = nullptr;     // generic scratch (row shifts, Toeplitz operands)
   size_t scratch_bytes = 0;
   void* h_pinned = nullptr;      // small pinned staging for per-call tables
@@ -179,5 +187,8 @@ int launch_project_ellipsoids(fbp_context* ctx, const double* d_ell, int count, 
 // ---- TMA helpers ----
 int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
                        const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]);
+// 2D BF16 rows (inner x outer, row pitch in bytes) with 128-byte swizzle.
+int make_tensor_map_2d_bf16_sw128(fbp_context* ctx, CUtensorMap* map, void* base, uint64_t inner, uint64_t outer,
+                                  uint64_t pitch_bytes, uint32_t box_inner, uint32_t box_outer);
 
 }  // namespace fbp

@@ -1,13 +1,325 @@
-// Toeplitz-GEMM row filter (tensor cores). Placeholder until the tcgen05
-// kernel lands: reports unsupported so the FFT filter is used.
+// Row filtering as a dense product on the tensor cores (tcgen05).
+//
+// Filtering every detector row with the circular kernel g of the padded
+// length n is Y = X T with T[k][i] = g[(i - k) mod n] (k, i < m): a dense,
+// symmetric Toeplitz matrix (g is even). It replaces the per-view FFT chain of
+// FBP3D::apply_filter_to_projections (Source/FilteredBackProjection/
+// FBP3D.cpp:389-414) for the MIXED form. Precision: X and T are split into
+// BF16 hi + lo parts (hi = bf16(x), lo = bf16(x - hi)), and
+// Y = Xh Th + Xh Tl + Xl Th is accumulated in FP32 in tensor memory (the
+// dropped Xl Tl term and the split residuals are ~2^-16 relative).
+//
+// Kernel: one CTA per 128 x 256 output tile. Warp 0 streams 64-wide K blocks
+// of Xh, Xl, Th, Tl into a two-stage shared-memory ring with TMA (128-byte
+// swizzle), warp 1 allocates 256 TMEM columns and issues
+// tcgen05.mma.cta_group::1.kind::f16 (M 128, N 256, K 16: 12 per K block), and
+// frees stages with tcgen05.commit; warps 4..7 (one warpgroup, each reading its
+// 32 TMEM lanes) load the FP32 accumulators with tcgen05.ld, stage them
+// through shared memory and write the backprojector's pair layout (FP16 with
+// the per-view scale) with row-contiguous stores. All waits are bounded and
+// TMEM is always released.
+
 #include "fbp_internal.h"
+#include "fbp_rows.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
 
 namespace fbp {
+namespace {
 
-bool toeplitz_supported(int) { return false; }
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int A_BYTES = BM * BK * 2;                     // 16 KB
+constexpr int B_BYTES = BN * BK * 2;                     // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
+constexpr int TMEM_COLS = 256;
+constexpr uint32_t kWait = 1u << 22;
+constexpr int kEpiStride = 33;  // floats per staged row (bank-conflict-free)
 
-int launch_filter_toeplitz(fbp_context* ctx, const RowSet&, int, int) {
-  return set_error(ctx, FBP_ERR_UNSUPPORTED, "Toeplitz filter not available in this build");
+__device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, int* err) {
+  for (uint32_t i = 0; i < kWait; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  atomicCAS(err, 0, kDevTimeout);
+  return false;
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* m, int x, int y, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(su32(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(su32(b))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major operand with 128-byte swizzle:
+// start address >> 4 (bits 0-13), stride between 8-row groups 1024 B >> 4
+// (bits 32-45), descriptor version 1 (bits 46-47), swizzle mode 2 = 128B
+// (bits 61-63). The leading-dimension offset is unused for swizzled K-major.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 in bits 17-22, M >> 4 in
+// bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* b) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b)) : "memory");
+}
+
+struct GemmArgs {
+  RowSet rs;        // output mapping (pair layout) of the whole stack
+  long long row0;   // first stack row of this chunk
+  int nrows;        // rows in this chunk
+  int m;            // samples per row (N and K extent)
+  int ntile_n;      // tiles along N
+  int* err;
+};
+
+__global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_constant__ CUtensorMap mah,
+                                                              const __grid_constant__ CUtensorMap mal,
+                                                              const __grid_constant__ CUtensorMap mbh,
+                                                              const __grid_constant__ CUtensorMap mbl,
+                                                              const GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 128-byte swizzled operand tiles need 1024-byte aligned stages
+  unsigned char* smem = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_holder + 1);
+  const int nt = blockIdx.x % g.ntile_n, mt = blockIdx.x / g.ntile_n;
+  const int rowt = mt * BM, col0 = nt * BN;
+  const int KB = (g.m + BK - 1) / BK;
+
+  if (tid == 0) {
+    *s_abort = 0;
+    for (int s = 0; s < STAGES; ++s) {
+      bar_init(&full[s], 1);
+      bar_init(&empty[s], 1);
+    }
+    bar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_holder)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_holder;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      int issued = 0;
+      for (int kb = 0; kb < KB; ++kb) {
+        const int s = kb % STAGES;
+        if (kb >= STAGES && !bar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1, g.err)) {
+          *s_abort = 1;
+          break;
+        }
+        unsigned char* st = smem + s * STAGE_BYTES;
+        bar_expect_tx(&full[s], STAGE_BYTES);
+        tma_2d(st, &mah, kb * BK, rowt, &full[s]);
+        tma_2d(st + A_BYTES, &mal, kb * BK, rowt, &full[s]);
+        tma_2d(st + 2 * A_BYTES, &mbh, kb * BK, col0, &full[s]);
+        tma_2d(st + 2 * A_BYTES + B_BYTES, &mbl, kb * BK, col0, &full[s]);
+        ++issued;
+      }
+      if (*s_abort) {
+        // drain: the last copy into each stage must land before the CTA exits
+        for (int s = 0; s < STAGES && s < issued; ++s) {
+          const int uses = (issued - s + STAGES - 1) / STAGES;
+          bar_wait(&full[s], (uses - 1) & 1, g.err);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer: D += Ah Bh + Ah Bl + Al Bh per K block
+      bool ok = true;
+      for (int kb = 0; kb < KB && ok; ++kb) {
+        const int s = kb % STAGES;
+        if (!bar_wait(&full[s], (kb / STAGES) & 1, g.err)) {
+          *s_abort = 1;
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = su32(smem + s * STAGE_BYTES);
+        const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
+#pragma unroll
+        for (int term = 0; term < 3; ++term) {
+          const uint32_t a = term == 2 ? al : ah;
+          const uint32_t b = term == 1 ? bl : bh;
+#pragma unroll
+          for (int ks = 0; ks < BK / 16; ++ks)  // 16 BF16 = 32 bytes along K inside the swizzled row
+            mma(tmem, smem_desc(a + ks * 32), smem_desc(b + ks * 32), (kb | term | ks) ? 1u : 0u);
+        }
+        mma_commit(&empty[s]);  // stage free once these MMAs have read it
+      }
+      mma_commit(done);  // accumulator complete (or abandoned after an abort)
+    }
+  } else if (warp >= 4) {
+    // epilogue warpgroup: warp 4 + w reads TMEM lanes 32w .. 32w + 31
+    const int w = warp - 4;
+    const bool ok = bar_wait(done, 0, g.err);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float* stage = reinterpret_cast<float*>(smem);  // ring is idle once `done` completed
+    const int lrow = 32 * w + lane;                 // tile row of this thread
+    for (int c = 0; c < BN / 32; ++c) {
+      uint32_t v[32];
+      const uint32_t addr = tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(c * 32);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%"
+          "19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stage[lrow * kEpiStride + j] = __uint_as_float(v[j]);
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      // warp w writes tile rows w, w + 4, ...; lane = column: row-contiguous stores
+      const int col = col0 + c * 32 + lane;
+      if (ok && !*s_abort && col < g.m) {
+        for (int r = w; r < BM; r += 4) {
+          const int lr = rowt + r;
+          if (lr < g.nrows) store_row_sample(g.rs, g.row0 + lr, col, stage[r * kEpiStride + lane]);
+        }
+      }
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+// X rows (fused log / weight) -> BF16 hi and lo rows of kp samples (zero past m).
+__global__ void split_rows_kernel(RowSet rs, long long row0, int nrows, int kp, __nv_bfloat16* xh, __nv_bfloat16* xl) {
+  const long long total = (long long)nrows * kp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / kp;
+    const int i = (int)(e - r * kp);
+    float x = i < rs.m ? load_pre(rs, row0 + r, i) : 0.f;
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    xh[e] = h;
+    xl[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+// Bt[i][k] = T[k][i] = g[(i - k) mod n], split into BF16 hi and lo (k < kp).
+__global__ void build_toeplitz_kernel(const float* g, int n, int m, int kp, __nv_bfloat16* th, __nv_bfloat16* tl) {
+  const long long total = (long long)m * kp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / kp), k = (int)(e - (long long)i * kp);
+    float t = 0.f;
+    if (k < m) t = g[(((i - k) % n) + n) % n];
+    const __nv_bfloat16 h = __float2bfloat16_rn(t);
+    th[e] = h;
+    tl[e] = __float2bfloat16_rn(t - __bfloat162float(h));
+  }
+}
+
+
+}  // namespace
+
+bool toeplitz_supported(int m) { return m >= 64 && m <= 8192; }
+
+int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter) {
+  const int m = rs.m;
+  if (!toeplitz_supported(m)) return set_error(ctx, FBP_ERR_UNSUPPORTED, "Toeplitz filter needs 64 <= width <= 8192");
+  if (rs.rows == 0) return FBP_OK;
+  const int kp = (m + BK - 1) / BK * BK;  // K padded to whole 64-blocks (16-byte pitch too)
+  ToeplitzTables& t = ctx->ttab;
+  if (!(t.m == m && t.n == n && t.filter == filter)) {
+    cudaFree(t.th);
+    t.th = nullptr;
+    t.m = 0;
+    const size_t bytes = sizeof(__nv_bfloat16) * (size_t)m * kp;
+    if (cuda_check(ctx, cudaMalloc(&t.th, 2 * bytes), "cudaMalloc(Toeplitz operands)")) return FBP_ERR_OUT_OF_MEMORY;
+    if (int rc = ensure_filter_tables(ctx, n, filter)) return rc;
+    build_toeplitz_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, kp, (__nv_bfloat16*)t.th,
+                                                                     (__nv_bfloat16*)t.th + (size_t)m * kp);
+    if (int rc = launched(ctx, "build_toeplitz_kernel")) return rc;
+    t.m = m;
+    t.n = n;
+    t.filter = filter;
+  }
+  // rows in chunks so that the split operands stay small
+  const long long chunk = std::min<long long>(rs.rows, 1LL << 16);
+  const size_t sbytes = sizeof(__nv_bfloat16) * (size_t)chunk * kp;
+  unsigned char* sp = static_cast<unsigned char*>(scratch(ctx, 2 * sbytes + 1024));
+  if (!sp) return FBP_ERR_OUT_OF_MEMORY;
+  __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(sp);
+  __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(sp + sbytes);
+  CUtensorMap mah, mal, mbh, mbl;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mah, xh, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mal, xl, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
+  __nv_bfloat16* th = (__nv_bfloat16*)t.th;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbh, th, kp, m, (uint64_t)kp * 2, BK, BN)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbl, th + (size_t)m * kp, kp, m, (uint64_t)kp * 2, BK, BN)) return rc;
+  const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
+  cudaError_t e = cudaFuncSetAttribute(toeplitz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "toeplitz smem attribute");
+  const int ntn = (m + BN - 1) / BN;
+  for (long long r0 = 0; r0 < rs.rows; r0 += chunk) {
+    const int nr = (int)std::min<long long>(chunk, rs.rows - r0);
+    split_rows_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl);
+    if (int rc = launched(ctx, "split_rows_kernel")) return rc;
+    GemmArgs ga;
+    ga.rs = rs;
+    ga.row0 = r0;
+    ga.nrows = nr;
+    ga.m = m;
+    ga.ntile_n = ntn;
+    ga.err = ctx->d_err;
+    const int grid = ((nr + BM - 1) / BM) * ntn;
+    toeplitz_gemm_kernel<<<grid, 256, smem, ctx->stream>>>(mah, mal, mbh, mbl, ga);
+    if (int rc = launched(ctx, "toeplitz_gemm_kernel")) return rc;
+  }
+  return FBP_OK;
 }
 
 }  // namespace fbp

@@ -18,6 +18,9 @@ pytestmark = pytest.mark.gpu
 TOL_FP32 = 1e-5
 TOL_ROWS = 1e-6
 TOL_MIXED = 1e-4
+# tensor-core filter: split-BF16 operands (hi + lo) with FP32 accumulation;
+# a numpy emulation of the same split gives 0.7e-5 .. 1.3e-5 on these rows
+TOL_TOEPLITZ_ROWS = 5e-5
 
 
 @pytest.fixture(scope="module")
@@ -50,6 +53,47 @@ def test_filter_rows_fp32(solver, oracle, m, filt):
     got = solver.download_projections()
     ref = oracle.filter_rows(proj.astype(np.float64).reshape(-1, m), filt).reshape(proj.shape)
     assert relative_rmse(got, ref) < TOL_ROWS
+
+
+@pytest.mark.parametrize("m,filt", [(64, 0), (367, 0), (384, 1), (1536, 3), (1440, 0), (100, 4)])
+def test_filter_rows_toeplitz(fbp, solver, oracle, m, filt):
+    """tcgen05 Toeplitz-product filter (FP32 output layout) against the oracle."""
+    rng = np.random.default_rng(m + filt)
+    proj = (rng.standard_normal((5, 7, m)) + 2.0).astype(np.float32)
+    solver.set_filter_impl(fbp.FilterImpl.TOEPLITZ)
+    solver.upload_projections(proj)
+    solver.apply_filter_to_projections(filt)
+    got = solver.download_projections()
+    ref = oracle.filter_rows(proj.astype(np.float64).reshape(-1, m), filt).reshape(proj.shape)
+    err = relative_rmse(got, ref)
+    print(f"toeplitz m={m} filter={filt} rel RMSE {err:.3e}")
+    assert err < TOL_TOEPLITZ_ROWS
+
+
+def test_filter_toeplitz_many_rows_and_sinograms(fbp, solver, oracle):
+    """More rows than one operand chunk (65536), sinogram row order, fused weights."""
+    rng = np.random.default_rng(11)
+    sino = rng.random((700, 100, 96)).astype(np.float32)  # [v][view][u]: 70000 rows
+    sod, odd, w = 300.0, 200.0, 96.0
+    solver.set_filter_impl(fbp.FilterImpl.TOEPLITZ)
+    solver.upload_sinograms(sino)
+    solver.apply_fdk_weights_to_sinograms(sod, odd, w)
+    solver.apply_filter_to_sinograms(1)
+    got = solver.download_sinograms(np.empty_like(sino))
+    proj = sino.transpose(1, 0, 2)
+    pw = oracle.fdk_weight(proj, sod + odd, w / 96, w / 96)
+    ref = oracle.filter_rows(pw.reshape(-1, 96), 1).reshape(proj.shape).transpose(1, 0, 2)
+    err = relative_rmse(got, ref)
+    print(f"toeplitz 70000 rows rel RMSE {err:.3e}")
+    assert err < TOL_TOEPLITZ_ROWS
+
+
+def test_filter_toeplitz_rejects_narrow_rows(fbp, solver):
+    solver.set_filter_impl(fbp.FilterImpl.TOEPLITZ)
+    solver.upload_projections(np.ones((2, 3, 32), np.float32))
+    with pytest.raises(fbp.FBPError) as e:
+        solver.apply_filter_to_projections(0)
+    assert e.value.status == -6
 
 
 def test_fdk_weight_fused_into_filter(solver, oracle):
@@ -235,6 +279,21 @@ def test_mixed_precision_cone(fbp, oracle, phantoms):
     ref = oracle.fdk(proj, c, 0)
     err = relative_rmse(got, ref)
     print(f"mixed cone128 rel RMSE {err:.3e}")
+    assert err < TOL_MIXED
+
+
+@pytest.mark.parametrize("impl", ["FFT", "TOEPLITZ"])
+def test_mixed_precision_cone_filter_impls(fbp, oracle, phantoms, impl):
+    """The MIXED form with either filter implementation stays within 1e-4."""
+    c, proj = _cone_case(phantoms, oracle, 2)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED)
+    s.set_filter_impl(getattr(fbp.FilterImpl, impl))
+    got = _gpu_fdk(s, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    err = relative_rmse(got, ref)
+    print(f"mixed cone128 filter {impl} rel RMSE {err:.3e}")
     assert err < TOL_MIXED
 
 
