@@ -242,41 +242,36 @@ int filter_stack(fbp_context* ctx, Stack& s, int filter_type) {
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length must be a power of two >= the row width");
   FBP_TRY(fbp::ensure_filter_tables(ctx, n, filter_type));
   const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
-  const int layout = mixed ? fbp::kLayoutPair16 : fbp::kLayoutPair32;
-  const int fpitch = round_up(s.u, 4);
-  const size_t need = (size_t)fpitch * s.filt_rows() * Stack::elem_bytes(layout);
-  if (!s.filt || s.filt_bytes < need) {
-    cudaFree(s.filt);
-    s.filt = nullptr;
-    s.filt_bytes = 0;
-    if (fbp::cuda_check(ctx, cudaMalloc(&s.filt, need), "cudaMalloc(filtered views)")) return FBP_ERR_OUT_OF_MEMORY;
-    s.filt_bytes = need;
-  }
-  s.filt_layout = layout;
-  s.filt_pitch = fpitch;
-  fbp::RowSet rs = rowset_of(s);
-  rs.out = s.filt;
-  rs.out_layout = layout;
-  rs.out_pitch = fpitch;
   int impl = ctx->filter_impl;
   if (impl == FBP_FILTER_IMPL_AUTO)
     impl = (mixed && fbp::toeplitz_supported(s.u)) ? FBP_FILTER_IMPL_TOEPLITZ : FBP_FILTER_IMPL_FFT;
-  if (mixed) {
-    if (!s.inv_scale &&
-        fbp::cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
-      s.inv_scale = nullptr;
-      return FBP_ERR_OUT_OF_MEMORY;
+  fbp::RowSet rs = rowset_of(s);
+  if (!mixed) {
+    // FP32 form: straight into the backprojector's float2 pair layout
+    const int layout = fbp::kLayoutPair32;
+    const int fpitch = round_up(s.u, 4);
+    const size_t need = (size_t)fpitch * s.filt_rows() * Stack::elem_bytes(layout);
+    if (!s.filt || s.filt_bytes < need) {
+      cudaFree(s.filt);
+      s.filt = nullptr;
+      s.filt_bytes = 0;
+      if (fbp::cuda_check(ctx, cudaMalloc(&s.filt, need), "cudaMalloc(filtered views)")) return FBP_ERR_OUT_OF_MEMORY;
+      s.filt_bytes = need;
     }
-    float* scale = s.inv_scale + s.n;
-    FBP_TRY(fbp::launch_view_absmax(ctx, rs, scale, s.inv_scale));
-    rs.view_scale = scale;
+    s.filt_layout = layout;
+    s.filt_pitch = fpitch;
+    rs.out = s.filt;
+    rs.out_layout = layout;
+    rs.out_pitch = fpitch;
   }
+  // MIXED form: FP32 rows in place; the backprojector packs them to FP16
+  // with per-view scales in the layout of the kernel it selects
   if (impl == FBP_FILTER_IMPL_TOEPLITZ)
     FBP_TRY(fbp::launch_filter_toeplitz(ctx, rs, n, filter_type));
   else
     FBP_TRY(fbp::launch_filter_fft(ctx, rs, n));
   s.log_pending = s.weights_pending = false;
-  s.filtered = true;
+  s.filtered = !mixed;
   return FBP_OK;
 }
 
@@ -376,8 +371,9 @@ void* scratch(fbp_context* ctx, size_t bytes) {
   return ctx->d_scratch;
 }
 
-int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
-                       const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]) {
+static int encode_tiled(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, int rank, void* base,
+                        const uint64_t* dims, const uint64_t* strides_bytes, const uint32_t* box,
+                        CUtensorMapSwizzle swizzle, CUtensorMapL2promotion l2) {
   std::call_once(g_encode_once, [] {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -386,35 +382,63 @@ int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType d
       g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   });
   if (!g_encode) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
-  cuuint64_t gstr[2] = {strides_bytes[0], strides_bytes[1]};
-  cuuint32_t bdim[3] = {box[0], box[1], box[2]};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = g_encode(map, dtype, 3, base, gdim, gstr, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  cuuint64_t gdim[5], gstr[4];
+  cuuint32_t bdim[5], estr[5];
+  for (int i = 0; i < rank; ++i) {
+    gdim[i] = dims[i];
+    bdim[i] = box[i];
+    estr[i] = 1;
+    if (i + 1 < rank) gstr[i] = strides_bytes[i];
+  }
+  CUresult r = g_encode(map, dtype, rank, base, gdim, gstr, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, l2,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return FBP_OK;
 }
 
+int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
+                       const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]) {
+  return encode_tiled(ctx, map, dtype, 3, base, dims, strides_bytes, box, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B);
+}
+
+int make_tensor_map_4d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
+                       const uint64_t dims[4], const uint64_t strides_bytes[3], const uint32_t box[4]) {
+  return encode_tiled(ctx, map, dtype, 4, base, dims, strides_bytes, box, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B);
+}
+
 int make_tensor_map_2d_bf16_sw128(fbp_context* ctx, CUtensorMap* map, void* base, uint64_t inner, uint64_t outer,
                                   uint64_t pitch_bytes, uint32_t box_inner, uint32_t box_outer) {
-  std::call_once(g_encode_once, [] {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  });
-  if (!g_encode) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  cuuint64_t gdim[2] = {inner, outer};
-  cuuint64_t gstr[1] = {pitch_bytes};
-  cuuint32_t bdim[2] = {box_inner, box_outer};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, gdim, gstr, bdim, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_error(ctx, FBP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  const uint64_t dims[2] = {inner, outer};
+  const uint64_t strides[1] = {pitch_bytes};
+  const uint32_t box[2] = {box_inner, box_outer};
+  return encode_tiled(ctx, map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box,
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B);
+}
+
+int prepare_packed(fbp_context* ctx, Stack& s, int layout) {
+  const bool quad = layout == kLayoutQuadG16;
+  const int fpitch = quad ? s.u + 1 : round_up(s.u, 4);
+  const size_t need = quad ? (size_t)(s.n / 4) * (s.v + 1) * (size_t)(s.u + 1) * 32
+                           : (size_t)fpitch * s.filt_rows() * Stack::elem_bytes(layout);
+  if (!s.filt || s.filt_bytes < need) {
+    cudaFree(s.filt);
+    s.filt = nullptr;
+    s.filt_bytes = 0;
+    if (cuda_check(ctx, cudaMalloc(&s.filt, need), "cudaMalloc(packed views)")) return FBP_ERR_OUT_OF_MEMORY;
+    s.filt_bytes = need;
+  }
+  if (!s.inv_scale && cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
+    s.inv_scale = nullptr;
+    return FBP_ERR_OUT_OF_MEMORY;
+  }
+  float* scale = s.inv_scale + s.n;
+  // the four-term difference of the gradient layout is at most 4 max|value|
+  if (int rc = launch_view_scales(ctx, rowset_of(s), quad ? 8192.f : 32768.f, scale, s.inv_scale)) return rc;
+  if (int rc = launch_pack(ctx, s, layout, s.filt, fpitch, scale)) return rc;
+  s.filt_layout = layout;
+  s.filt_pitch = fpitch;
   return FBP_OK;
 }
 

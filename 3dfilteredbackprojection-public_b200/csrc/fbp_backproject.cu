@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 namespace fbp {
@@ -124,6 +125,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
       "[%5];" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -247,6 +257,19 @@ __device__ __forceinline__ __half2 lds_h2(uint32_t addr) {
   uint32_t v;
   asm("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
   return *reinterpret_cast<__half2*>(&v);
+}
+
+__device__ __forceinline__ uint4 lds_u4(uint32_t addr) {
+  uint4 v;
+  asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+  return v;
+}
+
+// FP16 x FP16 + FP32 with one rounding to FP32.
+__device__ __forceinline__ float fma_f16_f32(__half a, __half b, float c) {
+  float d;
+  asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(__half_as_ushort(a)), "h"(__half_as_ushort(b)), "f"(c));
+  return d;
 }
 
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
@@ -487,6 +510,7 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
 
 constexpr int kQuadEntries = 8;  // outstanding view-quads per CTA
 constexpr int kKahanQuads = 4;   // quads (16 views) per Kahan fold
+constexpr int kFoldQG = 32;      // quads per Kahan fold when the running sums live in shared memory
 
 struct QuadCoef {
   float Dx, Dz, D0, Nx, Nz, N0, Vx, Vz, V0;
@@ -498,10 +522,16 @@ struct QuadCoef {
   int pad[3];
 };
 
+// 288 threads, two CTAs per SM: 112 registers per thread.
 template <int LAYOUT, int NY, bool KAHAN>
-__global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
+__global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
   constexpr int TX = 16, TZ = 16, NCW = 8, E = kQuadEntries;
-  constexpr int ESZ = LAYOUT == kLayoutPair32 ? 8 : 4;
+  // QG: the four views of a quad come interleaved in one window (one copy,
+  // two 16-byte loads per voxel step feed all four taps). The quads are
+  // walked group-major, q = g + m K/4 for m = 0..3, so the slot of rotation
+  // r, (m + r) mod 4, is a compile-time index in each of the four unrolled steps.
+  constexpr bool QG = LAYOUT == kLayoutQuadG16;
+  constexpr int ESZ = QG ? 32 : LAYOUT == kLayoutPair32 ? 8 : 4;
   constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -534,12 +564,14 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
     // ---------------------------------------------------------------- producer
     int head = 0, tail = 0, oldest = 0, issued = 0;
     for (int kb = 0; kb < K && !*s_abort; kb += 32) {
-      const int k = kb + lane;  // view of the representative tile; rotation r uses view (k + r Q) mod K
+      const int it = kb + lane;  // iteration (ring entry order)
+      // view of the representative tile; rotation r uses view (k + r Q) mod K
+      const int k = QG ? (it >> 2) + (it & 3) * Q : it;
       QuadCoef qc;
       int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
       bool skip = true;
       qc.skip = 1;
-      if (k < K) {
+      if (it < K) {
         ViewCoef vc;
         bool overflow = false, behind = false;
         int need_u = 0, need_v = 0;
@@ -555,7 +587,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         mi = wi * kNH + hi;
         tx_bytes = maps.w[wi] * maps.h[hi] * ESZ;
         sub = (tx_bytes + 127) & ~127;
-        need = skip ? 0 : 4 * sub;
+        need = skip ? 0 : (QG ? sub : 4 * sub);
         qc.Dx = vc.Dx; qc.Dz = vc.Dz; qc.D0 = vc.D0;
         qc.Nx = vc.Nx; qc.Nz = vc.Nz; qc.N0 = vc.N0;
         qc.Vx = vc.Vx; qc.Vz = vc.Vz; qc.V0 = vc.V0;
@@ -602,6 +634,10 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         if (lane == 0) {
           if (sk) {
             mbar_arrive(&full[e]);
+          } else if (QG) {
+            // group q >> 2, slots = views (q >> 2) + s Q; element column u0 + 1 holds columns u0, u0 + 1
+            mbar_arrive_expect_tx(&full[e], (uint32_t)ctx);
+            tma_load_4d(smem + off, &maps.map[cmi], 0, cu0 + 1, cv0 + a.pair_rows, q >> 2, &full[e]);
           } else {
             mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
             const CUtensorMap* m = &maps.map[cmi];
@@ -631,6 +667,11 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   const int tx = (warp & 1) * 8 + (lane & 7);
   const int tz = (warp >> 1) * 4 + (lane >> 3);
   const float fx = (float)tx, fz = (float)tz;
+  // SMACC (interleaved layout with Kahan sums): the running sums live in
+  // shared memory beside their compensations and only the 4 x NY partial
+  // sums stay in registers, folded every kFoldQG quads.
+  constexpr bool SMACC = QG && KAHAN;
+  float* accs = comp + 4 * NY * 256;
   float acc[4][NY], part[KAHAN ? 4 : 1][KAHAN ? NY : 1];
 #pragma unroll
   for (int r = 0; r < 4; ++r)
@@ -643,17 +684,20 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       for (int j = 0; j < NY; ++j) {
         part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
         comp[(r * NY + j) * 256 + tid] = 0.f;
+        if (SMACC) accs[(r * NY + j) * 256 + tid] = 0.f;
       }
   }
   const uint32_t ring = smem_u32(smem);
   int e = 0;
   uint32_t ph = 0;
-  int kq = 0;
-  bool bad = false;
-  for (int q = 0; q < K; ++q) {
+  bool bad = false, stop = false;
+  // one quad: wait for its window, apply it to the 4 x NY voxels, release it
+  auto step = [&](auto mc) {
+    constexpr int M = decltype(mc)::value;
     if (!mbar_wait(&full[e], ph, a.err)) {
       *s_abort = 1;
-      break;
+      stop = true;
+      return;
     }
     const QuadCoef g = coef[e];
     if (!g.skip) {
@@ -673,20 +717,47 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
         const uint32_t sub = (uint32_t)g.sub;
         const uint32_t c0 = ring + (uint32_t)g.off + (uint32_t)(iu * ESZ) - kMagicBits * RB;
-        float wa[4], wb[4], Wr[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          Wr[r] = W * g.ws[r];
-          wa[r] = Wr[r] - Wr[r] * fu;
-          wb[r] = Wr[r] * fu;
-        }
         const __half2 fu2 = __float2half2_rn(fu);
+        if constexpr (QG) {
+          float Wr[4];
 #pragma unroll
-        for (int j = 0; j < NY; ++j) {
-          const float v = fmaf((float)j, dvv, vl);
+          for (int r = 0; r < 4; ++r) Wr[r] = W * g.ws[r];
 #pragma unroll
-          for (int r = 0; r < 4; ++r)
-            tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu2, Wr[r], KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j]);
+          for (int j = 0; j < NY; ++j) {
+            const float v = fmaf((float)j, dvv, vl);
+            const float t = __fadd_rz(v, kMagic);
+            const float fv = v - (t - kMagic);
+            const uint32_t addr = __float_as_uint(t) * RB + c0;
+            const uint4 L0 = lds_u4(addr), L1 = lds_u4(addr + 16);
+            const uint32_t wv[8] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w};
+            const __half fvh = __float2half_rn(fv);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int sl = (M + r) & 3;
+              const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);
+              const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);
+              const __half2 h = __hfma2(fu2, X2, X1);  // (row e - 1 lerped in u, its v difference)
+              const float tap = fma_f16_f32(fvh, __high2half(h), __low2float(h));
+              float& dst = KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j];
+              dst = fmaf(Wr[r], tap, dst);
+            }
+          }
+        } else {
+          float wa[4], wb[4], Wr[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            Wr[r] = W * g.ws[r];
+            wa[r] = Wr[r] - Wr[r] * fu;
+            wb[r] = Wr[r] * fu;
+          }
+#pragma unroll
+          for (int j = 0; j < NY; ++j) {
+            const float v = fmaf((float)j, dvv, vl);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+              tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu2, Wr[r],
+                          KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j]);
+          }
         }
       } else {
         bad = true;
@@ -698,19 +769,52 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       e = 0;
       ph ^= 1;
     }
-    if (KAHAN && ++kq == kKahanQuads) {
-      kq = 0;
+  };
+  // fold the partial sums into the running sums (Kahan)
+  auto fold = [&]() {
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+    for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int j = 0; j < NY; ++j) {
-          float& c = comp[(r * NY + j) * 256 + tid];
-          const float y = part[KAHAN ? r : 0][KAHAN ? j : 0] - c;
-          const float t = acc[r][j] + y;
-          c = (t - acc[r][j]) - y;
+      for (int j = 0; j < NY; ++j) {
+        const int i = (r * NY + j) * 256 + tid;
+        float& c = comp[i];
+        const float sum = SMACC ? accs[i] : acc[r][j];
+        const float y = part[KAHAN ? r : 0][KAHAN ? j : 0] - c;
+        const float t = sum + y;
+        c = (t - sum) - y;
+        if (SMACC)
+          accs[i] = t;
+        else
           acc[r][j] = t;
-          part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
-        }
+        part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
+      }
+  };
+  static_assert(kKahanQuads == 4 && kFoldQG % 4 == 0, "folds on whole groups of four quads");
+  if constexpr (QG) {
+    int kq = 0;
+    for (int q = 0; q < K; q += 4) {
+      step(std::integral_constant<int, 0>{});
+      if (stop) break;
+      step(std::integral_constant<int, 1>{});
+      if (stop) break;
+      step(std::integral_constant<int, 2>{});
+      if (stop) break;
+      step(std::integral_constant<int, 3>{});
+      if (stop) break;
+      if (KAHAN && (kq += 4) == kFoldQG) {
+        kq = 0;
+        fold();
+      }
+    }
+  } else {
+    int kq = 0;
+    for (int q = 0; q < K; ++q) {
+      step(std::integral_constant<int, 0>{});
+      if (stop) break;
+      if (KAHAN && ++kq == kKahanQuads) {
+        kq = 0;
+        fold();
+      }
     }
   }
   if (bad) atomicCAS(a.err, 0, kDevFootprint);
@@ -718,7 +822,11 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int j = 0; j < NY; ++j) acc[r][j] += part[KAHAN ? r : 0][KAHAN ? j : 0] - comp[(r * NY + j) * 256 + tid];
+      for (int j = 0; j < NY; ++j) {
+        const int i = (r * NY + j) * 256 + tid;
+        const float sum = SMACC ? accs[i] : acc[r][j];
+        acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - comp[i]);
+      }
   }
   if (*s_abort) return;
 
@@ -848,6 +956,8 @@ cudaError_t launch_quad(int layout, const BoxMaps& maps, const BPArgs& a, size_t
       return launch_quad_cfg<kLayoutPair32>(maps, a, smem, kahan, stream);
     case kLayoutPair16:
       return launch_quad_cfg<kLayoutPair16>(maps, a, smem, kahan, stream);
+    case kLayoutQuadG16:
+      return launch_quad_cfg<kLayoutQuadG16>(maps, a, smem, kahan, stream);
     default:
       return launch_quad_cfg<kLayoutRaw32>(maps, a, smem, kahan, stream);
   }
@@ -868,8 +978,26 @@ cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size
 
 }  // namespace
 
-int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit, bool kahan) {
-  const int layout = st.filtered ? st.filt_layout : kLayoutRaw32;
+int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed) {
+  const double pi = 3.14159265358979323846;
+  const bool kahan = mixed;
+  // Four-fold symmetric path: square volume, views over one turn (or
+  // 4m + 1 turns) with K % 4 == 0, an even number of 16-wide tiles per axis.
+  const bool is2d = g.ny == 1;
+  const double turns = g.span / (2.0 * pi);
+  const long long iturns = llround(turns);
+  const bool symmetric = !is2d && g.nx == g.nz && g.nx % 32 == 0 && g.nviews % 4 == 0 &&
+                         fabs(turns - (double)iturns) < 1e-9 && iturns % 4 == 1;
+  const bool quad = symmetric && ctx->bp_variant != FBP_BACKPROJECTOR_GENERIC;
+  if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC && !symmetric)
+    return set_error(ctx, FBP_ERR_UNSUPPORTED,
+                     "the four-fold symmetric backprojector needs nx == nz (a multiple of 32), views % 4 == 0 and "
+                     "views over one full turn");
+  // MIXED form over f32 rows: packed to FP16 for the selected kernel below
+  const bool packed = mixed && !st.filtered;
+  const int layout = st.filtered ? st.filt_layout
+                     : packed    ? (quad ? kLayoutQuadG16 : kLayoutPair16)
+                                 : kLayoutRaw32;
   const int esize = Stack::elem_bytes(layout);
   BPArgs a{};
   a.vol = vol;
@@ -887,7 +1015,6 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   a.vox = g.vox;
   a.cu = 0.5 * g.nu - 0.5;
   a.cv = 0.5 * g.nv - 0.5;
-  const double pi = 3.14159265358979323846;
   if (g.kind == FBP_GEOMETRY_CONE) {
     a.dvn = (float)(g.sdd / (g.sod * g.dv) * g.vox);
     a.scale = (float)(pi / g.nviews * g.sdd / (g.sod * g.du));
@@ -895,8 +1022,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
     a.dvn = (float)(g.vox / g.dv);
     a.scale = (float)(pi / g.nviews / g.du);
   }
-  a.inv_scale = layout == kLayoutPair16 ? st.inv_scale : nullptr;
-  a.align = layout == kLayoutPair32 ? 2 : 4;  // TMA: x * element size must be a multiple of 16 bytes
+  a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;
+  // TMA: x * element size must be a multiple of 16 bytes (the interleaved
+  // layout's x is the 8-byte word inside a 32-byte element: always 0)
+  a.align = layout == kLayoutQuadG16 ? 1 : layout == kLayoutPair32 ? 2 : 4;
   a.sino_layout = st.sinogram ? 1 : 0;
   a.pair_rows = layout == kLayoutRaw32 ? 0 : 1;
   a.clip_ylimit = clip_ylimit;
@@ -938,18 +1067,6 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   }
   a.trig = ctx->d_trig;
 
-  // Four-fold symmetric path: square volume, views over one turn (or
-  // 4m + 1 turns) with K % 4 == 0, an even number of 16-wide tiles per axis.
-  const bool is2d = g.ny == 1;
-  const double turns = g.span / (2.0 * pi);
-  const long long iturns = llround(turns);
-  const bool symmetric = !is2d && g.nx == g.nz && g.nx % 32 == 0 && g.nviews % 4 == 0 &&
-                         fabs(turns - (double)iturns) < 1e-9 && iturns % 4 == 1;
-  const bool quad = symmetric && ctx->bp_variant != FBP_BACKPROJECTOR_GENERIC;
-  if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC && !symmetric)
-    return set_error(ctx, FBP_ERR_UNSUPPORTED,
-                     "the four-fold symmetric backprojector needs nx == nz (a multiple of 32), views % 4 == 0 and "
-                     "views over one full turn");
   // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
   const int TX = 16, TZ = 16, NY = is2d ? 1 : (quad ? 8 : 16);
   a.ntx = (g.nx + TX - 1) / TX;
@@ -1009,9 +1126,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   if (use_quad) {
     // byte ring for the windows + entry records (+ Kahan compensations)
     const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(int)) + 64;
-    const size_t comp = kahan ? (size_t)4 * 8 * 256 * sizeof(float) : 0;
+    // Kahan compensations (+ the running sums for the interleaved layout)
+    const size_t comp = kahan ? (size_t)(layout == kLayoutQuadG16 ? 2 : 1) * 4 * 8 * 256 * sizeof(float) : 0;
     const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
-    if (4 * max_box > ring) {
+    if ((layout == kLayoutQuadG16 ? 1 : 4) * max_box > ring) {
       use_quad = false;  // the largest quad does not fit: generic path
       if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC)
         return set_error(ctx, FBP_ERR_UNSUPPORTED, "detector windows too large for the symmetric backprojector");
@@ -1026,7 +1144,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
       ctx->plan.valid = false;
       const int saved = ctx->bp_variant;
       ctx->bp_variant = FBP_BACKPROJECTOR_GENERIC;
-      const int rc = launch_backproject(ctx, g, st, vol, clip_ylimit, kahan);
+      const int rc = launch_backproject(ctx, g, st, vol, clip_ylimit, mixed);
       ctx->bp_variant = saved;
       return rc;
     }
@@ -1039,9 +1157,12 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
     smem = (size_t)stages * per_stage + 64;
   }
 
+  if (packed)
+    if (int rc = prepare_packed(ctx, st, layout)) return rc;
   // the grid of boxes over the filtered stack (4-byte elements; float2 as two floats)
-  const void* base = st.filtered ? st.filt : (const void*)st.f32;
-  const int pitch_el = st.filtered ? st.filt_pitch : st.pitch;
+  const bool from_filt = st.filtered || packed;
+  const void* base = from_filt ? st.filt : (const void*)st.f32;
+  const int pitch_el = from_filt ? st.filt_pitch : st.pitch;
   const uint64_t pitch_bytes = (uint64_t)pitch_el * esize;
   const uint64_t ux = layout == kLayoutPair32 ? 2ull * st.u : (uint64_t)st.u;
   const uint64_t rows_v = layout == kLayoutRaw32 ? (uint64_t)st.v : (uint64_t)st.v + 1;  // element rows per view
@@ -1055,6 +1176,15 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float
   maps.h[kNH - 1] = bv;
   for (int i = 0; i < kNW; ++i)
     for (int j = 0; j < kNH; ++j) {
+      if (layout == kLayoutQuadG16) {  // [group][element row][element column][4 x 8 bytes]
+        const uint64_t d4[4] = {4, (uint64_t)pitch_el, rows_v, (uint64_t)st.n / 4};
+        const uint64_t s4[3] = {32, 32ull * pitch_el, 32ull * pitch_el * rows_v};
+        const uint32_t b4[4] = {4, (uint32_t)maps.w[i], (uint32_t)maps.h[j], 1};
+        if (int rc = make_tensor_map_4d(ctx, &maps.map[i * kNH + j], CU_TENSOR_MAP_DATA_TYPE_UINT64,
+                                        const_cast<void*>(base), d4, s4, b4))
+          return rc;
+        continue;
+      }
       const uint32_t box_x = layout == kLayoutPair32 ? 2 * maps.w[i] : maps.w[i];  // in 4-byte elements
       uint64_t dims[3], strides[2];
       uint32_t box[3];

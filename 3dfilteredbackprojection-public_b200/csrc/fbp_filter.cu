@@ -219,16 +219,15 @@ __global__ void view_absmax_kernel(RowSet rs, unsigned* vmax) {
     if (smax[i]) atomicMax(vmax + i, smax[i]);
 }
 
-// scale = largest power of two with scale * bound <= 2^15, bound = L1 norm of
-// the filter kernel times the view's max |input|; that bounds every filtered
-// value, so FP16 (max 65504) cannot overflow.
-__global__ void view_scale_kernel(const unsigned* vmax, int nviews, const float* l1, float* scale, float* inv) {
+// scale = largest power of two with scale * max|value| <= limit (so FP16,
+// max 65504, holds every stored value and its neighbour differences).
+__global__ void view_scale_kernel(const unsigned* vmax, int nviews, float limit, float* scale, float* inv) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nviews) return;
-  float bound = __uint_as_float(vmax[k]) * (*l1);
+  const float bound = __uint_as_float(vmax[k]);
   float s = 1.f;
   if (bound > 0.f && isfinite(bound)) {
-    int e = (int)floorf(log2f(32768.f / bound));
+    int e = (int)floorf(log2f(limit / bound));
     e = max(-100, min(100, e));
     s = ldexpf(1.f, e);
   }
@@ -236,17 +235,55 @@ __global__ void view_scale_kernel(const unsigned* vmax, int nviews, const float*
   inv[k] = 1.f / s;
 }
 
-__global__ void l1_kernel(const float* g, int n, float* out) {
-  __shared__ float red[256];
-  float s = 0.f;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += fabsf(g[i]);
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
+// f32 rows -> pair16: element (view, e, c) = (row e - 1, row e) * scale.
+__global__ void pack_pair16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
+                                   const float* scale, __half2* out, long long opitch) {
+  const long long total = (long long)n_views * (n_v + 1) * m;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long er = t / m;  // element row in output order
+    const int c = (int)(t - er * m);
+    const int view = sinogram ? (int)(er % n_views) : (int)(er / (n_v + 1));
+    const int e = sinogram ? (int)(er / n_views) : (int)(er % (n_v + 1));
+    auto row = [&](int iv) -> long long { return sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv; };
+    const float lo = e >= 1 ? src[row(e - 1) * spitch + c] : 0.f;
+    const float hi = e < n_v ? src[row(e) * spitch + c] : 0.f;
+    const float sc = scale[view];
+    out[er * opitch + c] = __floats2half2_rn(lo * sc, hi * sc);
   }
-  if (threadIdx.x == 0) *out = red[0];
+}
+
+// f32 rows -> quad-interleaved gradient layout: one thread per (group g,
+// element row e, element column s), writing the 32 bytes of the four slots.
+__global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
+                                    const float* scale, uint4* out) {
+  const int Q = n_views >> 2, P = m + 1;
+  const long long total = (long long)Q * (n_v + 1) * P;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long ge = t / P;
+    const int sc = (int)(t - ge * P);
+    const int g = (int)(ge / (n_v + 1)), e = (int)(ge - (long long)g * (n_v + 1));
+    const int c = sc - 1;  // element column sc covers columns c, c + 1
+    uint32_t w[8];
+#pragma unroll
+    for (int slot = 0; slot < 4; ++slot) {
+      const int view = g + slot * Q;
+      auto at = [&](int iv, int iu) -> float {
+        if (iv < 0 || iv >= n_v || iu < 0 || iu >= m) return 0.f;
+        const long long r = sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv;
+        return src[r * spitch + iu];
+      };
+      const float k = scale[view];
+      const float pa = at(e - 1, c), pb = at(e, c), pc = at(e - 1, c + 1), pd = at(e, c + 1);
+      const __half2 x1 = __floats2half2_rn(pa * k, (pb - pa) * k);
+      const __half2 x2 = __floats2half2_rn((pc - pa) * k, ((pd - pc) - (pb - pa)) * k);
+      w[2 * slot] = *reinterpret_cast<const uint32_t*>(&x1);
+      w[2 * slot + 1] = *reinterpret_cast<const uint32_t*>(&x2);
+    }
+    out[2 * t] = make_uint4(w[0], w[1], w[2], w[3]);
+    out[2 * t + 1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
 }
 
 // Natural-order complex FFT of rows (FFFT::fft_radix2 / inverse_fft_radix2,
@@ -402,23 +439,36 @@ int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs) {
   return launched(ctx, "elementwise_pre_kernel");
 }
 
-int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale) {
+int launch_view_scales(fbp_context* ctx, const RowSet& rs, float limit, float* view_scale, float* inv_scale) {
+  if (rs.n_views > 16384) return set_error(ctx, FBP_ERR_UNSUPPORTED, "at most 16384 views in MIXED precision");
   unsigned* vmax = static_cast<unsigned*>(scratch(ctx, sizeof(unsigned) * rs.n_views + 64));
   if (!vmax) return FBP_ERR_OUT_OF_MEMORY;
-  float* l1 = reinterpret_cast<float*>(vmax + rs.n_views);
   if (int rc = cuda_check(ctx, cudaMemsetAsync(vmax, 0, sizeof(unsigned) * rs.n_views, ctx->stream), "memset"))
     return rc;
-  if (rs.n_views > 16384) return set_error(ctx, FBP_ERR_UNSUPPORTED, "at most 16384 views in MIXED precision");
-  {
-    const int blocks = (int)std::max(1LL, std::min<long long>((rs.rows + 7) / 8, (long long)ctx->num_sms * 4));
-    const size_t sm = sizeof(unsigned) * rs.n_views;
-    cudaFuncSetAttribute(view_absmax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    view_absmax_kernel<<<blocks, 256, sm, ctx->stream>>>(rs, vmax);
-  }
-  l1_kernel<<<1, 256, 0, ctx->stream>>>(ctx->ftab.kernel, ctx->ftab.n, l1);
-  view_scale_kernel<<<(rs.n_views + 127) / 128, 128, 0, ctx->stream>>>(vmax, rs.n_views, l1, view_scale, inv_scale);
-  ctx->launches += 2;  // three launches above
+  const int blocks = (int)std::max(1LL, std::min<long long>((rs.rows + 7) / 8, (long long)ctx->num_sms * 4));
+  const size_t sm = sizeof(unsigned) * rs.n_views;
+  cudaFuncSetAttribute(view_absmax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  view_absmax_kernel<<<blocks, 256, sm, ctx->stream>>>(rs, vmax);
+  view_scale_kernel<<<(rs.n_views + 127) / 128, 128, 0, ctx->stream>>>(vmax, rs.n_views, limit, view_scale, inv_scale);
+  ctx->launches += 1;  // two launches above
   return launched(ctx, "view scale kernels");
+}
+
+int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long long pitch, const float* view_scale) {
+  if (layout == kLayoutPair16) {
+    const long long total = (long long)s.n * (s.v + 1) * s.u;
+    pack_pair16_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(
+        s.f32, s.pitch, s.u, s.n, s.v, s.sinogram, view_scale, static_cast<__half2*>(out), pitch);
+    return launched(ctx, "pack_pair16_kernel");
+  }
+  if (layout == kLayoutQuadG16) {
+    if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
+    const long long total = (long long)(s.n / 4) * (s.v + 1) * (s.u + 1);
+    pack_quadg16_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
+                                                                            view_scale, static_cast<uint4*>(out));
+    return launched(ctx, "pack_quadg16_kernel");
+  }
+  return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown packed layout");
 }
 
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse) {

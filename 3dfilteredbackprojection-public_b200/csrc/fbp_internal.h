@@ -29,6 +29,14 @@ enum FiltLayout : int {
   kLayoutRaw32 = 0,   // plain FP32 rows (unfiltered data, 2D staging)
   kLayoutPair32 = 1,  // float2 (8 bytes / sample), FP32 form
   kLayoutPair16 = 2,  // half2 (4 bytes / sample) with a per-view scale, MIXED form
+  // Four views interleaved per detector element, for the four-fold symmetric
+  // backprojector (MIXED form). Views k = g + s K/4 (s = 0..3) form group g;
+  // element (g, e, c + 1) holds, for each slot s, the 2 x 2 neighbourhood of
+  // rows e - 1, e and columns c, c + 1 as four FP16 values with the view's
+  // scale: a, b - a, c' - a, d - c' - b + a (a = (e-1, c), b = (e, c),
+  // c' = (e-1, c+1), d = (e, c+1); zero outside the detector). 32 bytes per
+  // element; a bilinear tap is a + fu (c' - a) + fv ((b - a) + fu (...)).
+  kLayoutQuadG16 = 3,
 };
 
 // A stack of detector rows. Projections are [view][v][u] (rows ordered view
@@ -56,7 +64,9 @@ struct Stack {
   double w_sdd = 0, w_du = 0, w_dv = 0;
   size_t rows() const { return (size_t)v * n; }
   size_t bytes32() const { return (size_t)pitch * rows() * sizeof(float); }
-  static int elem_bytes(int layout) { return layout == kLayoutPair32 ? 8 : 4; }
+  static int elem_bytes(int layout) {
+    return layout == kLayoutQuadG16 ? 32 : layout == kLayoutPair32 ? 8 : 4;
+  }
   // element rows of the filtered buffer (pair layouts carry one extra row per view)
   size_t filt_rows() const { return (size_t)(v + 1) * n; }
 };
@@ -157,7 +167,12 @@ int ensure_filter_tables(fbp_context* ctx, int n, int filter);
 int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n);
 int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter);
 int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs);  // weight / log-norm only
-int launch_view_absmax(fbp_context* ctx, const RowSet& rs, float* view_scale, float* inv_scale);
+// Per-view scales for FP16 storage: scale = largest power of two with
+// scale * max|row value of the view| <= limit; inv = 1 / scale.
+int launch_view_scales(fbp_context* ctx, const RowSet& rs, float limit, float* view_scale, float* inv_scale);
+// Pack the stack's f32 rows into an FP16 backprojector layout (kLayoutPair16
+// with row pitch `pitch` elements, or kLayoutQuadG16) using per-view scales.
+int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long long pitch, const float* view_scale);
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse);
 int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift);
 // Copy filtered rows [row0, row0 + nrows) of a pair layout back to FP32 rows.
@@ -173,9 +188,13 @@ struct BPGeom {
   int nu, nv, nviews;
   int nx, ny, nz;
 };
-// Backproject the stack's content (filt when filtered, else f32 rows).
-int launch_backproject(fbp_context* ctx, const BPGeom& g, const Stack& st, float* vol, int clip_ylimit,
-                       bool kahan);
+// Backproject the stack's content (filt when filtered, else f32 rows). In
+// the MIXED form (`mixed`) f32 content is first packed into the FP16 layout
+// the selected kernel reads (prepare_packed), with Kahan-compensated sums.
+int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed);
+// (fbp_api.cu) size the stack's packed buffer for `layout`, compute the
+// per-view scales and pack the f32 rows into it.
+int prepare_packed(fbp_context* ctx, Stack& s, int layout);
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit);
 int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g,
                      float* par, int out_bins, double du_out);
@@ -187,6 +206,8 @@ int launch_project_ellipsoids(fbp_context* ctx, const double* d_ell, int count, 
 // ---- TMA helpers ----
 int make_tensor_map_3d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
                        const uint64_t dims[3], const uint64_t strides_bytes[2], const uint32_t box[3]);
+int make_tensor_map_4d(fbp_context* ctx, CUtensorMap* map, CUtensorMapDataType dtype, void* base,
+                       const uint64_t dims[4], const uint64_t strides_bytes[3], const uint32_t box[4]);
 // 2D BF16 rows (inner x outer, row pitch in bytes) with 128-byte swizzle.
 int make_tensor_map_2d_bf16_sw128(fbp_context* ctx, CUtensorMap* map, void* base, uint64_t inner, uint64_t outer,
                                   uint64_t pitch_bytes, uint32_t box_inner, uint32_t box_outer);
