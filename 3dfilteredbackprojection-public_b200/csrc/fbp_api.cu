@@ -576,6 +576,16 @@ int fbp_set_backprojector(fbp_context* ctx, int variant) {
   return FBP_OK;
 }
 
+int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v) {
+  if (!ctx) return FBP_ERR_INVALID_ARGUMENT;
+  if (ctx->last_bp[0] < 0) return FBP_ERR_STATE;
+  if (variant) *variant = ctx->last_bp[0];
+  if (layout) *layout = ctx->last_bp[1];
+  if (box_u) *box_u = ctx->last_bp[2];
+  if (box_v) *box_v = ctx->last_bp[3];
+  return FBP_OK;
+}
+
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes) {
   if (!ctx || !bytes) return FBP_ERR_INVALID_ARGUMENT;
   size_t b = 0;

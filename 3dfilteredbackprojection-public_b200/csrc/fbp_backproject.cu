@@ -34,6 +34,8 @@
 
 #include "fbp_internal.h"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -85,6 +87,10 @@ struct BPArgs {
   int pair_rows;          // 1: an element carries rows v and v + 1 (pair layouts)
   int clip_ylimit;        // clip negatives where iy < clip_ylimit
   int* err;
+  // interleaved layout in global memory, for windows too large to stage:
+  // 16-byte entries, [group][element row][plane][element column]
+  const uint4* qg;
+  int qg_pitch, qg_rows;  // element columns per plane row, element rows per group
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -519,12 +525,14 @@ struct QuadCoef {
   int box;      // staged window: width (elements) | rows << 16
   int off;      // byte offset of the entry's first window in the ring
   int sub;      // bytes between the entry's four windows
-  int pad[3];
+  int direct;   // interleaved layout: window not staged, consumers gather it from global memory
+  int u0, e0;   // direct: element column / element row of the window origin
 };
 
-// 288 threads, two CTAs per SM: 112 registers per thread.
+// 288 threads, two CTAs per SM: 9 warps each put 5 warps on some SM
+// sub-partitions (16K registers each), so at most 96 registers per thread.
 template <int LAYOUT, int NY, bool KAHAN>
-__global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
+__global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
   constexpr int TX = 16, TZ = 16, NCW = 8, E = kQuadEntries;
   // QG: the four views of a quad come interleaved in one window (one copy,
   // two 16-byte loads per voxel step feed all four taps). The quads are
@@ -569,7 +577,7 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
       const int k = QG ? (it >> 2) + (it & 3) * Q : it;
       QuadCoef qc;
       int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
-      bool skip = true;
+      bool skip = true, direct = false;
       qc.skip = 1;
       if (it < K) {
         ViewCoef vc;
@@ -587,15 +595,21 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
         mi = wi * kNH + hi;
         tx_bytes = maps.w[wi] * maps.h[hi] * ESZ;
         sub = (tx_bytes + 127) & ~127;
-        need = skip ? 0 : (QG ? sub : 4 * sub);
+        // interleaved layout: a window wider than the widest box or larger than
+        // the ring (rare near-source tiles) is read from global memory instead
+        direct = QG && !skip && (need_u > maps.w[kNW - 1] || rows > maps.h[kNH - 1] || sub > R);
+        need = (skip || direct) ? 0 : (QG ? sub : 4 * sub);
         qc.Dx = vc.Dx; qc.Dz = vc.Dz; qc.D0 = vc.D0;
         qc.Nx = vc.Nx; qc.Nz = vc.Nz; qc.N0 = vc.N0;
         qc.Vx = vc.Vx; qc.Vz = vc.Vz; qc.V0 = vc.V0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) qc.ws[r] = a.inv_scale ? a.inv_scale[(k + r * Q) % K] : 1.0f;
         qc.skip = skip;
-        qc.box = maps.w[wi] | (maps.h[hi] << 16);
+        qc.box = direct ? (need_u | (rows << 16)) : (maps.w[wi] | (maps.h[hi] << 16));
         qc.sub = sub;
+        qc.direct = direct;
+        qc.u0 = u0 + 1;
+        qc.e0 = v0 + a.pair_rows;
       }
       const int nb = min(32, K - kb);
       for (int i = 0; i < nb; ++i) {
@@ -626,7 +640,7 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
         }
         if (lane == 0) end_pos[e] = start + qneed;
         head = start + qneed;
-        const int sk = __shfl_sync(0xffffffffu, (int)skip, i);
+        const int sk = __shfl_sync(0xffffffffu, (int)(skip || direct), i);
         const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
         const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
         const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
@@ -637,7 +651,7 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
           } else if (QG) {
             // group q >> 2, slots = views (q >> 2) + s Q; element column u0 + 1 holds columns u0, u0 + 1
             mbar_arrive_expect_tx(&full[e], (uint32_t)ctx);
-            tma_load_4d(smem + off, &maps.map[cmi], 0, cu0 + 1, cv0 + a.pair_rows, q >> 2, &full[e]);
+            tma_load_4d(smem + off, &maps.map[cmi], 2 * (cu0 + 1), 0, cv0 + a.pair_rows, q >> 2, &full[e]);
           } else {
             mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
             const CUtensorMap* m = &maps.map[cmi];
@@ -664,14 +678,18 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
   }
 
   // ------------------------------------------------------------------ consumers
-  const int tx = (warp & 1) * 8 + (lane & 7);
-  const int tz = (warp >> 1) * 4 + (lane >> 3);
+  // a warp owns 8 x 4 columns; for the interleaved layout each quarter-warp
+  // (one shared-memory phase of 16-byte loads) is a compact 4 x 2 patch, whose
+  // detector columns stay within 8 elements (no bank conflicts)
+  const int tx = QG ? (warp & 1) * 8 + ((lane >> 3) & 1) * 4 + (lane & 3) : (warp & 1) * 8 + (lane & 7);
+  const int tz = QG ? (warp >> 1) * 4 + (lane >> 4) * 2 + ((lane >> 2) & 1) : (warp >> 1) * 4 + (lane >> 3);
   const float fx = (float)tx, fz = (float)tz;
   // SMACC (interleaved layout with Kahan sums): the running sums live in
   // shared memory beside their compensations and only the 4 x NY partial
   // sums stay in registers, folded every kFoldQG quads.
   constexpr bool SMACC = QG && KAHAN;
-  float* accs = comp + 4 * NY * 256;
+  float* accs = comp;  // SMACC: FP32 running sums, then BF16 compensations
+  __nv_bfloat16* compb = reinterpret_cast<__nv_bfloat16*>(comp + 4 * NY * 256);
   float acc[4][NY], part[KAHAN ? 4 : 1][KAHAN ? NY : 1];
 #pragma unroll
   for (int r = 0; r < 4; ++r)
@@ -683,14 +701,19 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
 #pragma unroll
       for (int j = 0; j < NY; ++j) {
         part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
-        comp[(r * NY + j) * 256 + tid] = 0.f;
-        if (SMACC) accs[(r * NY + j) * 256 + tid] = 0.f;
+        if (SMACC) {
+          accs[(r * NY + j) * 256 + tid] = 0.f;
+          compb[(r * NY + j) * 256 + tid] = __float2bfloat16_rn(0.f);
+        } else {
+          comp[(r * NY + j) * 256 + tid] = 0.f;
+        }
       }
   }
   const uint32_t ring = smem_u32(smem);
   int e = 0;
   uint32_t ph = 0;
   bool bad = false, stop = false;
+  int grp = 0;  // interleaved layout: view group of the current four quads
   // one quad: wait for its window, apply it to the 4 x NY voxels, release it
   auto step = [&](auto mc) {
     constexpr int M = decltype(mc)::value;
@@ -716,30 +739,57 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
       const float vmax_ok = (float)(BV - kRowTail) - (float)(kSlack / 2);
       if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
         const uint32_t sub = (uint32_t)g.sub;
-        const uint32_t c0 = ring + (uint32_t)g.off + (uint32_t)(iu * ESZ) - kMagicBits * RB;
+        const uint32_t c0 = ring + (uint32_t)g.off + (uint32_t)(iu * (QG ? 16 : ESZ)) - kMagicBits * RB;
         const __half2 fu2 = __float2half2_rn(fu);
         if constexpr (QG) {
           float Wr[4];
 #pragma unroll
           for (int r = 0; r < 4; ++r) Wr[r] = W * g.ws[r];
-#pragma unroll
-          for (int j = 0; j < NY; ++j) {
-            const float v = fmaf((float)j, dvv, vl);
-            const float t = __fadd_rz(v, kMagic);
-            const float fv = v - (t - kMagic);
-            const uint32_t addr = __float_as_uint(t) * RB + c0;
-            const uint4 L0 = lds_u4(addr), L1 = lds_u4(addr + 16);
+          // four bilinear taps from the 2 x 16 bytes of one element (slot of rotation r: (M + r) mod 4)
+          auto taps = [&](const uint4& L0, const uint4& L1, float fv, int j) {
             const uint32_t wv[8] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w};
-            const __half fvh = __float2half_rn(fv);
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               const int sl = (M + r) & 3;
-              const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);
-              const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);
-              const __half2 h = __hfma2(fu2, X2, X1);  // (row e - 1 lerped in u, its v difference)
-              const float tap = fma_f16_f32(fvh, __high2half(h), __low2float(h));
+              const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);      // (a, b - a)
+              const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);  // (c' - a, d - c' - b + a)
+              const float2 P = __half22float2(X1);
+              // u lerps in FP32 (one rounding each): row e - 1 and its v difference
+              const float A = fma_f16_f32(__low2half(fu2), __low2half(X2), P.x);
+              const float G = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
               float& dst = KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j];
-              dst = fmaf(Wr[r], tap, dst);
+              dst = fmaf(Wr[r], fmaf(fv, G, A), dst);
+            }
+          };
+          if (!g.direct) {
+            const uint32_t plane = (uint32_t)BU * 16;
+#pragma unroll
+            for (int j = 0; j < NY; ++j) {
+              const float v = fmaf((float)j, dvv, vl);
+              const float t = __fadd_rz(v, kMagic);
+              const float fv = v - (t - kMagic);
+              const uint32_t addr = __float_as_uint(t) * RB + c0;
+              taps(lds_u4(addr), lds_u4(addr + plane), fv, j);  // slots 0, 1 | slots 2, 3
+            }
+          } else {
+            // window not staged: read the elements from global memory (zero
+            // outside the stored extent, as the TMA fill would give)
+            const int col = g.u0 + iu;
+            const bool col_ok = col >= 0 && col < a.qg_pitch;
+            const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int j = 0; j < NY; ++j) {
+              const float v = fmaf((float)j, dvv, vl);
+              const float t = __fadd_rz(v, kMagic);
+              const float fv = v - (t - kMagic);
+              const int row = g.e0 + (int)(__float_as_uint(t) - kMagicBits);
+              uint4 L0 = zero, L1 = zero;
+              if (col_ok && row >= 0 && row < a.qg_rows) {
+                const uint4* p = a.qg + ((size_t)grp * a.qg_rows + row) * 2 * a.qg_pitch + col;
+                L0 = __ldg(p);
+                L1 = __ldg(p + a.qg_pitch);
+              }
+              taps(L0, L1, fv, j);
             }
           }
         } else {
@@ -777,15 +827,17 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
 #pragma unroll
       for (int j = 0; j < NY; ++j) {
         const int i = (r * NY + j) * 256 + tid;
-        float& c = comp[i];
+        const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
         const float sum = SMACC ? accs[i] : acc[r][j];
         const float y = part[KAHAN ? r : 0][KAHAN ? j : 0] - c;
         const float t = sum + y;
-        c = (t - sum) - y;
-        if (SMACC)
+        if (SMACC) {
+          compb[i] = __float2bfloat16_rn((t - sum) - y);  // an error term: 8 bits suffice
           accs[i] = t;
-        else
+        } else {
+          comp[i] = (t - sum) - y;
           acc[r][j] = t;
+        }
         part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
       }
   };
@@ -793,6 +845,7 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
   if constexpr (QG) {
     int kq = 0;
     for (int q = 0; q < K; q += 4) {
+      grp = q >> 2;
       step(std::integral_constant<int, 0>{});
       if (stop) break;
       step(std::integral_constant<int, 1>{});
@@ -825,7 +878,8 @@ __global__ void __maxnreg__(112) bp_quad_kernel(const __grid_constant__ BoxMaps 
       for (int j = 0; j < NY; ++j) {
         const int i = (r * NY + j) * 256 + tid;
         const float sum = SMACC ? accs[i] : acc[r][j];
-        acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - comp[i]);
+        const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
+        acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - c);
       }
   }
   if (*s_abort) return;
@@ -934,6 +988,8 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
   auto kern = kahan ? bp_kernel<LAYOUT, TX, TZ, NY, true> : bp_kernel<LAYOUT, TX, TZ, NY, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
   dim3 grid(a.ntx * a.ntz, (a.ny + NY - 1) / NY);
   kern<<<grid, TX * TZ + 32, smem, stream>>>(maps, a);
   return cudaGetLastError();
@@ -943,6 +999,9 @@ template <int LAYOUT>
 cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
   auto kern = kahan ? bp_quad_kernel<LAYOUT, 8, true> : bp_quad_kernel<LAYOUT, 8, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // all of L1 as shared memory, so that two CTAs of up to 113 KB share an SM
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   dim3 grid((a.ntx / 2) * (a.ntz / 2), (a.ny + 7) / 8);
   kern<<<grid, 256 + 32, smem, stream>>>(maps, a);
@@ -1024,7 +1083,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   }
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;
   // TMA: x * element size must be a multiple of 16 bytes (the interleaved
-  // layout's x is the 8-byte word inside a 32-byte element: always 0)
+  // layout's x counts 8-byte words, two per 16-byte plane element: always even)
   a.align = layout == kLayoutQuadG16 ? 1 : layout == kLayoutPair32 ? 2 : 4;
   a.sino_layout = st.sinogram ? 1 : 0;
   a.pair_rows = layout == kLayoutRaw32 ? 0 : 1;
@@ -1112,7 +1171,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   const int bu = (plan.box_u + a.align - 1) / a.align * a.align;
   // a pair element carries row v + 1 with it: one row less to stage
   const int bv = layout == kLayoutRaw32 ? plan.box_v : std::max(1, plan.box_v - 1);
-  if ((layout == kLayoutPair32 ? 2 * bu : bu) > 256 || bv > 256)
+  if (layout != kLayoutQuadG16 && ((layout == kLayoutPair32 ? 2 * bu : bu) > 256 || bv > 256))
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
                      "detector footprint of a voxel tile exceeds the 256-element TMA box; geometry magnification "
                      "too large for the staged backprojector");
@@ -1126,10 +1185,13 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   if (use_quad) {
     // byte ring for the windows + entry records (+ Kahan compensations)
     const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(int)) + 64;
-    // Kahan compensations (+ the running sums for the interleaved layout)
-    const size_t comp = kahan ? (size_t)(layout == kLayoutQuadG16 ? 2 : 1) * 4 * 8 * 256 * sizeof(float) : 0;
+    // Kahan compensations (interleaved layout: FP32 running sums + BF16 compensations)
+    const size_t comp = !kahan ? 0 : layout == kLayoutQuadG16 ? (size_t)4 * 8 * 256 * (4 + 2)
+                                                              : (size_t)4 * 8 * 256 * sizeof(float);
     const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
-    if ((layout == kLayoutQuadG16 ? 1 : 4) * max_box > ring) {
+    // the interleaved layout gathers windows that do not fit from global memory
+    const size_t entry = layout == kLayoutQuadG16 ? 0 : 4 * max_box;
+    if (entry > ring) {
       use_quad = false;  // the largest quad does not fit: generic path
       if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC)
         return set_error(ctx, FBP_ERR_UNSUPPORTED, "detector windows too large for the symmetric backprojector");
@@ -1159,6 +1221,12 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
 
   if (packed)
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
+  a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
+  if (layout == kLayoutQuadG16) {
+    a.qg = static_cast<const uint4*>(st.filt);
+    a.qg_pitch = st.filt_pitch;
+    a.qg_rows = st.v + 1;
+  }
   // the grid of boxes over the filtered stack (4-byte elements; float2 as two floats)
   const bool from_filt = st.filtered || packed;
   const void* base = from_filt ? st.filt : (const void*)st.f32;
@@ -1167,19 +1235,23 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   const uint64_t ux = layout == kLayoutPair32 ? 2ull * st.u : (uint64_t)st.u;
   const uint64_t rows_v = layout == kLayoutRaw32 ? (uint64_t)st.v : (uint64_t)st.v + 1;  // element rows per view
   BoxMaps maps;
+  // interleaved layout: boxes of at most 128 x 256 elements (TMA: 256 words per
+  // box row) and at most the ring; larger windows are gathered directly
+  const int mbu = layout == kLayoutQuadG16 ? std::min(bu, 128) : bu;
+  const int mbv = layout == kLayoutQuadG16 ? std::min(bv, std::max(1, (int)(a.box_bytes / (32 * mbu)))) : bv;
   for (int i = 0; i < kNW; ++i) {
-    const int w = (bu * (i + 1) + kNW - 1) / kNW;
+    const int w = (mbu * (i + 1) + kNW - 1) / kNW;
     maps.w[i] = std::max(a.align, (w + a.align - 1) / a.align * a.align);
   }
-  for (int j = 0; j < kNH; ++j) maps.h[j] = std::max(1, (bv * (j + 1) + kNH - 1) / kNH);
-  maps.w[kNW - 1] = bu;
-  maps.h[kNH - 1] = bv;
+  for (int j = 0; j < kNH; ++j) maps.h[j] = std::max(1, (mbv * (j + 1) + kNH - 1) / kNH);
+  maps.w[kNW - 1] = mbu;
+  maps.h[kNH - 1] = mbv;
   for (int i = 0; i < kNW; ++i)
     for (int j = 0; j < kNH; ++j) {
-      if (layout == kLayoutQuadG16) {  // [group][element row][element column][4 x 8 bytes]
-        const uint64_t d4[4] = {4, (uint64_t)pitch_el, rows_v, (uint64_t)st.n / 4};
-        const uint64_t s4[3] = {32, 32ull * pitch_el, 32ull * pitch_el * rows_v};
-        const uint32_t b4[4] = {4, (uint32_t)maps.w[i], (uint32_t)maps.h[j], 1};
+      if (layout == kLayoutQuadG16) {  // [group][element row][plane][element column][2 x 8 bytes]
+        const uint64_t d4[4] = {2ull * pitch_el, 2, rows_v, (uint64_t)st.n / 4};
+        const uint64_t s4[3] = {16ull * pitch_el, 32ull * pitch_el, 32ull * pitch_el * rows_v};
+        const uint32_t b4[4] = {2u * maps.w[i], 2, (uint32_t)maps.h[j], 1};
         if (int rc = make_tensor_map_4d(ctx, &maps.map[i * kNH + j], CU_TENSOR_MAP_DATA_TYPE_UINT64,
                                         const_cast<void*>(base), d4, s4, b4))
           return rc;
@@ -1211,6 +1283,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                                       const_cast<void*>(base), dims, strides, box))
         return rc;
     }
+  ctx->last_bp[0] = use_quad ? FBP_BACKPROJECTOR_SYMMETRIC : FBP_BACKPROJECTOR_GENERIC;
+  ctx->last_bp[1] = layout;
+  ctx->last_bp[2] = bu;
+  ctx->last_bp[3] = bv;
   cudaError_t e = use_quad ? launch_quad(layout, maps, a, smem, kahan, ctx->stream)
                  : is2d   ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
                           : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);

@@ -254,7 +254,8 @@ __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, in
 }
 
 // f32 rows -> quad-interleaved gradient layout: one thread per (group g,
-// element row e, element column s), writing the 32 bytes of the four slots.
+// element row e, element column s), writing the 32 bytes of the four slots
+// as two 16-byte plane entries.
 __global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                     const float* scale, uint4* out) {
   const int Q = n_views >> 2, P = m + 1;
@@ -281,8 +282,9 @@ __global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, i
       w[2 * slot] = *reinterpret_cast<const uint32_t*>(&x1);
       w[2 * slot + 1] = *reinterpret_cast<const uint32_t*>(&x2);
     }
-    out[2 * t] = make_uint4(w[0], w[1], w[2], w[3]);
-    out[2 * t + 1] = make_uint4(w[4], w[5], w[6], w[7]);
+    // two planes per element row: slots 0, 1 then slots 2, 3, 16 bytes per column each
+    out[(2 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
+    out[(2 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
   }
 }
 

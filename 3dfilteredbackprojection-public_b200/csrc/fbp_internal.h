@@ -35,7 +35,9 @@ enum FiltLayout : int {
   // rows e - 1, e and columns c, c + 1 as four FP16 values with the view's
   // scale: a, b - a, c' - a, d - c' - b + a (a = (e-1, c), b = (e, c),
   // c' = (e-1, c+1), d = (e, c+1); zero outside the detector). 32 bytes per
-  // element; a bilinear tap is a + fu (c' - a) + fv ((b - a) + fu (...)).
+  // element, stored as two planes per element row (slots 0, 1 | slots 2, 3,
+  // 16 bytes per column), so neighbouring columns are 16 bytes apart; a
+  // bilinear tap is a + fu (c' - a) + fv ((b - a) + fu (...)).
   kLayoutQuadG16 = 3,
 };
 
@@ -97,6 +99,7 @@ struct fbp_context {
   int pad_len = 0;
   int clip_after_bp = 1;
   int bp_variant = FBP_BACKPROJECTOR_AUTO;
+  int last_bp[4] = {-1, -1, 0, 0};  // variant, layout, box_u, box_v of the last backprojection
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched by this context
 

@@ -102,6 +102,7 @@ SIGNATURES = {
     "fbp_set_clip_after_backprojection": [_P, _I],
     "fbp_set_backprojector": [_P, _I],
     "fbp_memory_in_use": [_P, C.POINTER(C.c_size_t)],
+    "fbp_last_backprojection": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "fbp_generate_blank_volume": [_P, _I, _I, _I],
     "fbp_generate_blank_projections": [_P, _I, _I, _I],
     "fbp_generate_blank_sinograms": [_P, _I, _I, _I],
@@ -259,6 +260,14 @@ class FBP3D:
         b = C.c_double()
         self.ctx.call("fbp_measure_smem_bandwidth", C.byref(b))
         return b.value
+
+    def last_backprojection(self) -> dict:
+        """Kernel, staged layout and window box of the last backprojection."""
+        v, l, bu, bv = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.ctx.call("fbp_last_backprojection", C.byref(v), C.byref(l), C.byref(bu), C.byref(bv))
+        names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16"}
+        return {"kernel": "symmetric" if v.value == Backprojector.SYMMETRIC else "generic",
+                "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value)}
 
     def memory_in_use(self) -> int:
         b = C.c_size_t()

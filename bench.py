@@ -347,6 +347,7 @@ def main() -> None:
     for form in forms:
         s = make_solver(form)
         res[form] = timed(s, pristine)
+        res[form]["kernel"] = s.last_backprojection()
         vols[form] = torch.empty((c["nz"], c["ny"], c["nx"]), dtype=torch.float32, device=dev)
         s.read_volume(vols[form])
         if form == "chosen":
@@ -420,7 +421,7 @@ def main() -> None:
     for form, r in res.items():
         line[f"form_{form}"] = {"value": world * U / (r["ms"] * 1e-3) / 1e9, "ms_per_step": r["ms"],
                                 "filter_ms": r["filter_ms"], "backprojection_ms": r["bp_ms"],
-                                "gpu_launches": r["launches"], "clocks": r["clocks"]}
+                                "gpu_launches": r["launches"], "clocks": r["clocks"], "backprojector": r["kernel"]}
     if "chosen" in res and "plain" in res:
         line["chosen_over_plain"] = res["plain"]["ms"] / res["chosen"]["ms"]
     if e2e is not None:

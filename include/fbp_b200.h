@@ -112,6 +112,13 @@ int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable);
 int fbp_set_backprojector(fbp_context* ctx, int variant);
 /* Device bytes held by ctx's buffers. */
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
+/* What the last backprojection ran (no counterpart in the reference, whose
+ * backprojection is one fixed shader): *variant = FBP_BACKPROJECTOR_GENERIC or
+ * FBP_BACKPROJECTOR_SYMMETRIC; *layout = staged view layout (0 FP32 rows,
+ * 1 FP32 row pairs, 2 FP16 row pairs, 3 FP16 four-view gradient quads);
+ * *box_u x *box_v = largest staged detector window in elements. Any output
+ * pointer may be NULL. FBP_ERR_STATE before the first backprojection. */
+int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v);
 
 /* ---- buffers (FBP3D.cpp:16-56, 197-210) ----------------------------------- */
 int fbp_generate_blank_volume(fbp_context* ctx, int x_size, int y_size, int z_size);
