@@ -91,6 +91,7 @@ struct BPArgs {
   // 16-byte entries, [group][element row][plane][element column]
   const uint4* qg;
   int qg_pitch, qg_rows;  // element columns per plane row, element rows per group
+  int resident;           // CTAs resident on the GPU at once (view-group skew of the interleaved walk)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -547,6 +548,14 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   const int K = a.nviews, Q = K >> 2;
   const int nbh = a.ntx >> 1;  // representative tiles per axis (lower-left quadrant)
   const int bx = blockIdx.x % nbh, bz = blockIdx.x / nbh;
+  // interleaved layout: the CTA starts its walk at view group g0, advanced by
+  // about K/4 groups per `resident` CTAs in launch order. A CTA that starts
+  // after others have progressed then reads the same groups at the same time
+  // (their windows share L2) instead of restarting at group 0; the offset
+  // depends only on the block index, so results stay deterministic.
+  const int g0 = QG ? (int)(((long long)(blockIdx.y * gridDim.x + blockIdx.x) * (K >> 2) / max(1, a.resident)) %
+                            (K >> 2))
+                    : 0;
   const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
 
   QuadCoef* coef = reinterpret_cast<QuadCoef*>(smem + R);
@@ -574,7 +583,8 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
     for (int kb = 0; kb < K && !*s_abort; kb += 32) {
       const int it = kb + lane;  // iteration (ring entry order)
       // view of the representative tile; rotation r uses view (k + r Q) mod K
-      const int k = QG ? (it >> 2) + (it & 3) * Q : it;
+      const int gq = QG ? ((it >> 2) + g0) % Q : 0;  // view group of iteration it
+      const int k = QG ? gq + (it & 3) * Q : it;
       QuadCoef qc;
       int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
       bool skip = true, direct = false;
@@ -649,9 +659,10 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
           if (sk) {
             mbar_arrive(&full[e]);
           } else if (QG) {
-            // group q >> 2, slots = views (q >> 2) + s Q; element column u0 + 1 holds columns u0, u0 + 1
+            // group gq, slots = views gq + s Q; element column u0 + 1 holds columns u0, u0 + 1
             mbar_arrive_expect_tx(&full[e], (uint32_t)ctx);
-            tma_load_4d(smem + off, &maps.map[cmi], 2 * (cu0 + 1), 0, cv0 + a.pair_rows, q >> 2, &full[e]);
+            tma_load_4d(smem + off, &maps.map[cmi], 2 * (cu0 + 1), 0, cv0 + a.pair_rows, ((q >> 2) + g0) % Q,
+                        &full[e]);
           } else {
             mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
             const CUtensorMap* m = &maps.map[cmi];
@@ -845,7 +856,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   if constexpr (QG) {
     int kq = 0;
     for (int q = 0; q < K; q += 4) {
-      grp = q >> 2;
+      grp = ((q >> 2) + g0) % (K >> 2);
       step(std::integral_constant<int, 0>{});
       if (stop) break;
       step(std::integral_constant<int, 1>{});
@@ -1223,6 +1234,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
   if (layout == kLayoutQuadG16) {
+    a.resident = 2 * ctx->num_sms;
     a.qg = static_cast<const uint4*>(st.filt);
     a.qg_pitch = st.filt_pitch;
     a.qg_rows = st.v + 1;
