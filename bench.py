@@ -40,6 +40,7 @@ PKG = ROOT / "3dfilteredbackprojection-public_b200"
 sys.path.insert(0, str(PKG))
 
 METRIC = "FDK Gvox·view/s"
+FILTER_NAMES = {0: "ram_lak", 1: "shepp_logan", 2: "cosine", 3: "hann", 4: "ramp_sampled"}
 UNIT = "Gvox·view/s"
 
 
@@ -51,6 +52,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--scale", type=int, default=1,
                    help="divide volume, detector and views by this factor (profiling runs); 1 = full workload")
+    p.add_argument("--workload", choices=["cone1440", "cone256"], default="cone1440",
+                   help="cone1440: the headline 1440x1470x1440 case; cone256: 256^3, 360 views (profiling)")
     p.add_argument("--forms", default="chosen,plain", help="comma list of chosen,plain")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -58,10 +61,15 @@ def parse_args():
     return p.parse_args()
 
 
-def workload(scale: int) -> dict:
+def workload(scale: int, name: str = "cone1440") -> dict:
     import phantoms as P
-    c = P.config_cone1440()
+    c = P.config_cone1440() if name == "cone1440" else P.config_cone256()
     return c if scale == 1 else P.scaled_cone(c, scale)
+
+
+def data_note(c: dict) -> str:
+    noise = f", Poisson noise I0={c['i0']:g}" if c.get("i0") else ""
+    return f"synthetic: {c.get('n_ellipsoids', 20)} seeded random ellipsoids, analytic FP64 line integrals{noise}"
 
 
 def updates_of(c: dict) -> int:
@@ -138,14 +146,15 @@ def cpu_inputs(c: dict, nviews_sample: int):
     views = np.linspace(0, c["nviews"] - 1, nviews_sample).round().astype(np.int32)
     proj = O.project_ellipsoids_cone(E, c, views)
     if "i0" in c:
-        proj = P.poisson_log(proj, c["i0"], np.random.default_rng(c["seed"]))
+        if c.get("i0"):
+            proj = P.poisson_log(proj, c["i0"], np.random.default_rng(c["seed"]))
     return proj, views
 
 
 def reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    c = workload(args.scale)
+    c = workload(args.scale, args.workload)
     nsv = 8 if args.scale == 1 else 4
     proj, views = cpu_inputs(c, nsv)
     results = []
@@ -165,9 +174,9 @@ def reference_arm(args, rank: int, world: int) -> None:
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 filter / f32 backprojection",
-        "data": "synthetic: seeded random ellipsoids, analytic FP64 line integrals, Poisson noise",
+        "data": data_note(c),
         "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "views": c["nviews"],
-                   "detector": [c["nu"], c["nv"]], "filter": "hann", "parallelism": "host cores"},
+                   "detector": [c["nu"], c["nv"]], "filter": FILTER_NAMES[c["filter"]], "parallelism": "host cores"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": r0["cores"], "kind": kind, "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -250,7 +259,7 @@ def main() -> None:
     import fbp_b200 as F
     import phantoms as P
 
-    c = workload(args.scale)
+    c = workload(args.scale, args.workload)
     U = updates_of(c)
     ga = P.geometry_args(c)
     geom = F.Geometry.cone(ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"],
@@ -281,7 +290,7 @@ def main() -> None:
     with torch.cuda.stream(stream):
         g = torch.Generator(device=dev)
         g.manual_seed(c["seed"] + 7919 * rank)
-        for k0 in range(0, c["nviews"], 64):
+        for k0 in range(0, c["nviews"] if c.get("i0") else 0, 64):
             blk = pristine[k0:k0 + 64]
             counts = torch.poisson(c["i0"] * torch.exp(-blk), generator=g)
             blk.copy_(-torch.log(torch.clamp(counts, min=1.0) / c["i0"]))
@@ -398,10 +407,10 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "storage_dtype": "f16 filtered views" if head == "chosen" else "f32",
-        "data": "synthetic: 40 seeded random ellipsoids, analytic FP64 line integrals, Poisson noise I0=5e4",
+        "data": data_note(c),
         "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "voxel_mm": c["vox"],
                    "views": c["nviews"], "detector": [c["nu"], c["nv"]], "pitch_mm": c["du"],
-                   "sod_mm": c["sod"], "sdd_mm": c["sdd"], "filter": "hann", "form": head,
+                   "sod_mm": c["sod"], "sdd_mm": c["sdd"], "filter": FILTER_NAMES[c["filter"]], "form": head,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (projections %.1f GB)" % (c["nviews"] * c["nv"] * c["nu"] * 4 / 1e9),
                    "step": "D2D restore of raw projections + weights + filter + backprojection + clip"},
