@@ -165,6 +165,7 @@ int require_stack(fbp_context* ctx, const Stack& s, const char* what) {
 }
 
 int ensure_volume(fbp_context* ctx, int x, int y, int z, bool clear) {
+  ctx->minmax_valid = false;
   if (x <= 0 || y <= 0 || z <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume sizes must be positive");
   if (!(ctx->vol && ctx->vx == x && ctx->vy == y && ctx->vz == z)) {
     cudaFree(ctx->vol);
@@ -475,10 +476,12 @@ int fbp_create(fbp_context** out, int device) {
   ctx->num_sms = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
-      cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) {
+      cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_minmax, 2 * sizeof(int)) != cudaSuccess) {
     g_thread_error = std::string("context setup failed: ") + cudaGetErrorString(cudaGetLastError());
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaFree(ctx->d_err);
+    cudaFree(ctx->d_minmax);
     delete ctx;
     return FBP_ERR_CUDA;
   }
@@ -498,6 +501,7 @@ int fbp_destroy(fbp_context* ctx) {
     free_stack(ctx->sino);
     cudaFree(ctx->vol);
     cudaFree(ctx->d_err);
+    cudaFree(ctx->d_minmax);
     cudaFree(ctx->d_trig);
     cudaFree(ctx->d_span);
     cudaFree(ctx->d_stage2d);
@@ -708,6 +712,7 @@ int fbp_load_sinogram(fbp_context* ctx, int y, float* dst, int on_dev) {
 
 static int volume_slice(fbp_context* ctx, int axis, int index, float* host_or_dev, int on_dev, bool load) {
   if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "volume is not allocated");
+  if (!load) ctx->minmax_valid = false;
   if (!host_or_dev) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
   const int nx = ctx->vx, ny = ctx->vy, nz = ctx->vz;
   const int lim = axis == 0 ? nx : axis == 1 ? ny : nz;
@@ -755,6 +760,7 @@ int fbp_read_volume(fbp_context* ctx, float* dst, int on_dev) {
 int fbp_write_volume_data(fbp_context* ctx, const float* src, int on_dev) {
   FBP_CTX(ctx);
   if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "write_volume_data but the volume is not allocated");
+  ctx->minmax_valid = false;
   if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
   size_t bytes = sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
   FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(ctx->vol, src, bytes, kind_of(on_dev, true), ctx->stream), "volume upload"));
@@ -765,6 +771,7 @@ int fbp_volume_device_ptr(fbp_context* ctx, float** ptr) {
   FBP_CTX(ctx);
   if (!ptr) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
   *ptr = ctx->vol;
+  ctx->minmax_valid = false;  // the caller may write through the pointer
   return ctx->vol ? FBP_OK : fbp::set_error(ctx, FBP_ERR_STATE, "volume is not allocated");
 }
 
@@ -814,7 +821,92 @@ int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type) {
 int fbp_clip_negatives_of_volume(fbp_context* ctx) {
   FBP_CTX(ctx);
   if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "clip_negatives_of_volume but the volume is not allocated");
+  ctx->minmax_valid = false;
   return fbp::launch_clip(ctx, ctx->vol, ctx->vx, ctx->vy, ctx->vz, ctx->vz);
+}
+
+// ---------------------------------------------------------- file I/O (f2)
+int fbp_projection_file_index(const char* path) { return path ? fbp::projection_file_index(path) : -1; }
+
+static int read_files(fbp_context* ctx, Stack& s, const char* directory, int fw, int fh, int ch, int bpc, int tw,
+                      int th, int count) {
+  FBP_TRY(alloc_stack(ctx, s, tw, th, count));  // generate_blank_projections / _sinograms
+  s.filtered = false;
+  s.log_pending = s.weights_pending = false;
+  FBP_TRY(fbp::read_projection_files(ctx, directory, fw, fh, ch, bpc, tw, th, count, s.f32, s.pitch, s.sinogram));
+  return sync_host(ctx, true);
+}
+
+int fbp_read_projections(fbp_context* ctx, const char* directory, int file_width, int file_height,
+                         int file_channel_count, int byte_per_channel, int target_width, int target_height,
+                         int projection_count) {
+  FBP_CTX(ctx);
+  return read_files(ctx, ctx->proj, directory, file_width, file_height, file_channel_count, byte_per_channel,
+                    target_width, target_height, projection_count);
+}
+
+int fbp_read_projections_as_sinograms(fbp_context* ctx, const char* directory, int file_width, int file_height,
+                                      int file_channel_count, int byte_per_channel, int target_width,
+                                      int target_height, int projection_count) {
+  FBP_CTX(ctx);
+  return read_files(ctx, ctx->sino, directory, file_width, file_height, file_channel_count, byte_per_channel,
+                    target_width, target_height, projection_count);
+}
+
+int fbp_write_volume(fbp_context* ctx, const char* directory) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "write_volume but the volume is not allocated");
+  FBP_TRY(fbp::write_volume_files(ctx, directory));
+  return sync_host(ctx, true);
+}
+
+// -------------------------------------------------- histogram normalisation
+static int volume_extremes_on_device(fbp_context* ctx) {
+  if (ctx->minmax_valid) return FBP_OK;  // folded in by the last backprojection
+  FBP_TRY(fbp::launch_volume_minmax(ctx, ctx->vol, (long long)ctx->vx * ctx->vy * ctx->vz, ctx->d_minmax));
+  ctx->minmax_valid = true;
+  return FBP_OK;
+}
+
+int fbp_volume_min_max(fbp_context* ctx, float* min_value, float* max_value) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "volume_min_max but the volume is not allocated");
+  if (!min_value || !max_value) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
+  FBP_TRY(volume_extremes_on_device(ctx));
+  int keys[2];
+  FBP_TRY(fbp::cuda_check(ctx, cudaMemcpyAsync(keys, ctx->d_minmax, sizeof(keys), cudaMemcpyDeviceToHost, ctx->stream),
+                          "min/max readback"));
+  FBP_TRY(sync_host(ctx, true));
+  auto value = [](int k) {
+    const int b = k >= 0 ? k : k ^ 0x7fffffff;
+    float f;
+    std::memcpy(&f, &b, sizeof(f));
+    return f;
+  };
+  if (keys[0] > keys[1]) {  // no finite value
+    *min_value = *max_value = 0.f;
+    return FBP_OK;
+  }
+  *min_value = value(keys[0]);
+  *max_value = value(keys[1]);
+  return FBP_OK;
+}
+
+int fbp_normalize_histogram(fbp_context* ctx) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "normalize_histogram but the volume is not allocated");
+  FBP_TRY(volume_extremes_on_device(ctx));
+  FBP_TRY(fbp::launch_normalize(ctx, ctx->vol, (long long)ctx->vx * ctx->vy * ctx->vz, ctx->d_minmax, 0.f, 0.f));
+  ctx->minmax_valid = false;
+  return FBP_OK;
+}
+
+int fbp_normalize_histogram_range(fbp_context* ctx, float min_value, float max_value) {
+  FBP_CTX(ctx);
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "normalize_histogram but the volume is not allocated");
+  FBP_TRY(fbp::launch_normalize(ctx, ctx->vol, (long long)ctx->vx * ctx->vy * ctx->vz, nullptr, min_value, max_value));
+  ctx->minmax_valid = false;
+  return FBP_OK;
 }
 
 int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,

@@ -92,6 +92,7 @@ struct BPArgs {
   const uint4* qg;
   int qg_pitch, qg_rows;  // element columns per plane row, element rows per group
   int resident;           // CTAs resident on the GPU at once (view-group skew of the interleaved walk)
+  int* minmax;            // fold the stored values' min / max into this pair (or nullptr)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -484,6 +485,7 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   if (*s_abort) return;
 
   const int ix = ix0 + tx, iz = iz0 + tz;
+  float lo = __int_as_float(0x7f800000), hi = -lo;
   if (ix < a.nx && iz < a.nz) {
     float* out = a.vol + ((size_t)iz * a.ny) * a.nx + ix;
 #pragma unroll
@@ -493,9 +495,12 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
         float r = acc[j] * a.scale;
         if (iy < a.clip_ylimit) r = fmaxf(r, 0.f);
         out[(size_t)iy * a.nx] = r;
+        lo = fminf(lo, r);
+        hi = fmaxf(hi, r);
       }
     }
   }
+  if (a.minmax) fold_minmax(a.minmax, lo, hi);
 }
 
 // ---------------------------------------------------------------------------
@@ -900,6 +905,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   const int ix = ix0 + tx, iz = iz0 + tz;
   const int cx[4] = {ix, n - 1 - iz, n - 1 - ix, iz};
   const int cz[4] = {iz, ix, n - 1 - iz, n - 1 - ix};
+  float lo = __int_as_float(0x7f800000), hi = -lo;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     float* out = a.vol + ((size_t)cz[r] * a.ny) * a.nx + cx[r];
@@ -910,9 +916,12 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         float val = acc[r][j] * a.scale;
         if (iy < a.clip_ylimit) val = fmaxf(val, 0.f);
         out[(size_t)iy * a.nx] = val;
+        lo = fminf(lo, val);
+        hi = fmaxf(hi, val);
       }
     }
   }
+  if (a.minmax) fold_minmax(a.minmax, lo, hi);
 }
 
 // Footprint pre-pass: one warp per tile (lanes over views) finds the
@@ -1295,6 +1304,11 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                                       const_cast<void*>(base), dims, strides, box))
         return rc;
     }
+  // the stored values' extremes feed histogram normalisation of the context's volume
+  if (vol == ctx->vol && ctx->d_minmax) {
+    if (int rc = launch_minmax_init(ctx, ctx->d_minmax)) return rc;
+    a.minmax = ctx->d_minmax;
+  }
   ctx->last_bp[0] = use_quad ? FBP_BACKPROJECTOR_SYMMETRIC : FBP_BACKPROJECTOR_GENERIC;
   ctx->last_bp[1] = layout;
   ctx->last_bp[2] = bu;
@@ -1303,6 +1317,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                  : is2d   ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
                           : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
+  ctx->minmax_valid = e == cudaSuccess && a.minmax != nullptr;
   return cuda_check(ctx, e, "bp_kernel");
 }
 

@@ -110,6 +110,8 @@ struct fbp_context {
   fbp::Stack sino;
 
   int* d_err = nullptr;          // device error word
+  int* d_minmax = nullptr;       // volume min / max as order-preserving int keys
+  bool minmax_valid = false;     // d_minmax describes the current volume
   double2* d_trig = nullptr;     // per-view (cos, sin) in FP64
   int trig_cap = 0;
   double trig_key[3] = {-1, 0, 0};  // (views, span, offset) of the table in d_trig
@@ -201,6 +203,37 @@ int prepare_packed(fbp_context* ctx, Stack& s, int layout);
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit);
 int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g,
                      float* par, int out_bins, double du_out);
+
+// ---- volume post-processing (fbp_volume.cu) ----
+// Order-preserving key of a float (int comparison == float comparison).
+__device__ __forceinline__ int minmax_key(float f) {
+  const int b = __float_as_int(f);
+  return b >= 0 ? b : b ^ 0x7fffffff;
+}
+__device__ __forceinline__ float minmax_value(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); }
+// Warp-reduce (lo, hi) and fold it into the device pair mm (all 32 lanes call;
+// a lane without values passes +inf / -inf; NaN is ignored).
+__device__ __forceinline__ void fold_minmax(int* mm, float lo, float hi) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0 && lo <= hi) {
+    atomicMin(mm, minmax_key(lo));
+    atomicMax(mm + 1, minmax_key(hi));
+  }
+}
+int launch_minmax_init(fbp_context* ctx, int* mm);
+int launch_volume_minmax(fbp_context* ctx, const float* vol, long long n, int* mm);
+// Rescale in place with the range from the device pair mm, or (mm == nullptr) from mn, mx.
+int launch_normalize(fbp_context* ctx, float* vol, long long n, const int* mm, float mn, float mx);
+
+// ---- file ingest / slice output (fbp_io.cu) ----
+int projection_file_index(const std::string& path);  // -1 when the name carries no index
+int read_projection_files(fbp_context* ctx, const char* directory, int fw, int fh, int channels, int bpc, int tw,
+                          int th, int count, float* dst, long long pitch, bool sinogram);
+int write_volume_files(fbp_context* ctx, const char* directory);
 
 // ---- phantoms (fbp_phantom.cu) ----
 int launch_project_ellipsoids(fbp_context* ctx, const double* d_ell, int count, const BPGeom& g,

@@ -137,6 +137,22 @@ class FBP3D {
     check(c(), fbp_generate_blank_sinograms(c(), x_size, y_size, projection_amount));
   }
   void free_volume() { check(c(), fbp_free_volume(c())); }
+  // FBP3D.h: read_projections / read_projections_as_sinograms / write_volume (FBP3D.cpp:74-195)
+  void read_projections(const std::string& upper_directory, int file_width, int file_height, int file_channel_count,
+                        int byte_per_channel, int target_projection_width, int target_projection_height,
+                        int projection_count) {
+    check(c(), fbp_read_projections(c(), upper_directory.c_str(), file_width, file_height, file_channel_count,
+                                    byte_per_channel, target_projection_width, target_projection_height,
+                                    projection_count));
+  }
+  void read_projections_as_sinograms(const std::string& upper_directory, int file_width, int file_height,
+                                     int file_channel_count, int byte_per_channel, int target_projection_width,
+                                     int target_projection_height, int projection_count) {
+    check(c(), fbp_read_projections_as_sinograms(c(), upper_directory.c_str(), file_width, file_height,
+                                                 file_channel_count, byte_per_channel, target_projection_width,
+                                                 target_projection_height, projection_count));
+  }
+  void write_volume(const std::string& upper_directory) { check(c(), fbp_write_volume(c(), upper_directory.c_str())); }
   void free_projections() { check(c(), fbp_free_projections(c())); }
   void free_sinograms() { check(c(), fbp_free_sinograms(c())); }
 
@@ -168,6 +184,10 @@ class FBP3D {
     check(c(), fbp_apply_filter_to_sinograms(c(), filter_type));
   }
   void clip_negatives_of_volume() { check(c(), fbp_clip_negatives_of_volume(c())); }
+  void normalize_histogram() { check(c(), fbp_normalize_histogram(c())); }                       // FBP3D.h:81
+  void normalize_histogram(float min_value, float max_value) {                                  // FBP3D.h:82
+    check(c(), fbp_normalize_histogram_range(c(), min_value, max_value));
+  }
 
   void project_backward_parallel_from_projections(float full_rotation_count, int volume_resolution_horizontal,
                                                   int volume_resolution_vertical, float rotation_offset_radian = 0.0f) {

@@ -136,6 +136,13 @@ SIGNATURES = {
     "fbp_apply_filter_to_projections": [_P, _I],
     "fbp_apply_filter_to_sinograms": [_P, _I],
     "fbp_clip_negatives_of_volume": [_P],
+    "fbp_volume_min_max": [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+    "fbp_read_projections": [_P, C.c_char_p, _I, _I, _I, _I, _I, _I, _I],
+    "fbp_read_projections_as_sinograms": [_P, C.c_char_p, _I, _I, _I, _I, _I, _I, _I],
+    "fbp_write_volume": [_P, C.c_char_p],
+    "fbp_projection_file_index": [C.c_char_p],
+    "fbp_normalize_histogram": [_P],
+    "fbp_normalize_histogram_range": [_P, C.c_float, C.c_float],
     "fbp_project_backward_cone_fdk_from_projections": [_P, _F, _F, _F, _F, _F, _I, _I, _F],
     "fbp_project_backward_cone_fdk_from_sinograms": [_P, _F, _F, _F, _F, _F, _I, _I, _F],
     "fbp_project_backward_parallel_from_projections": [_P, _F, _I, _I, _F],
@@ -151,6 +158,11 @@ SIGNATURES = {
     "fbp_kernel_launch_count": [_P, C.POINTER(C.c_uint64)],
     "fbp_measure_smem_bandwidth": [_P, C.POINTER(C.c_double)],
 }
+
+
+def projection_file_index(path: str) -> int:
+    """Projection index that read_projections takes from a file name, or -1."""
+    return library().fbp_projection_file_index(str(path).encode())
 
 
 def library() -> C.CDLL:
@@ -286,6 +298,24 @@ class FBP3D:
 
     def free_volume(self) -> None:
         self.ctx.call("fbp_free_volume")
+
+    # -- file I/O (FBP3D.cpp:74-195)
+    def read_projections(self, upper_directory: str, file_width: int, file_height: int, file_channel_count: int,
+                         byte_per_channel: int, target_projection_width: int, target_projection_height: int,
+                         projection_count: int) -> None:
+        self.ctx.call("fbp_read_projections", str(upper_directory).encode(), file_width, file_height,
+                      file_channel_count, byte_per_channel, target_projection_width, target_projection_height,
+                      projection_count)
+
+    def read_projections_as_sinograms(self, upper_directory: str, file_width: int, file_height: int,
+                                      file_channel_count: int, byte_per_channel: int, target_projection_width: int,
+                                      target_projection_height: int, projection_count: int) -> None:
+        self.ctx.call("fbp_read_projections_as_sinograms", str(upper_directory).encode(), file_width, file_height,
+                      file_channel_count, byte_per_channel, target_projection_width, target_projection_height,
+                      projection_count)
+
+    def write_volume(self, upper_directory: str) -> None:
+        self.ctx.call("fbp_write_volume", str(upper_directory).encode())
 
     def free_projections(self) -> None:
         self.ctx.call("fbp_free_projections")
@@ -423,6 +453,19 @@ class FBP3D:
 
     def clip_negatives_of_volume(self) -> None:
         self.ctx.call("fbp_clip_negatives_of_volume")
+
+    def volume_min_max(self) -> tuple[float, float]:
+        """compute_min_value_of_volume / compute_max_value_of_volume (FBP3D.cpp:780-800)."""
+        lo, hi = C.c_float(), C.c_float()
+        self.ctx.call("fbp_volume_min_max", C.byref(lo), C.byref(hi))
+        return lo.value, hi.value
+
+    def normalize_histogram(self, min_value=None, max_value=None) -> None:
+        """FBP3D::normalize_histogram (FBP3D.cpp:802-826): the volume's own range, or a given one."""
+        if min_value is None:
+            self.ctx.call("fbp_normalize_histogram")
+        else:
+            self.ctx.call("fbp_normalize_histogram_range", float(min_value), float(max_value))
 
     def project_backward_cone_fdk_from_projections(self, xray_source_distance, detector_panel_distance,
                                                    detector_width, volume_width, full_rotation_count,

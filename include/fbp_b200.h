@@ -173,6 +173,37 @@ int fbp_apply_fdk_weights_to_sinograms(fbp_context* ctx, float xray_source_dista
 int fbp_apply_filter_to_projections(fbp_context* ctx, int filter_type);                               /* :389-414 */
 int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type);                                 /* :417-442 */
 int fbp_clip_negatives_of_volume(fbp_context* ctx);                                                    /* :444-458 */
+/* ---- file I/O (FBP3D.cpp:74-195) -------------------------------------------------------
+ * FBP3D::read_projections / read_projections_as_sinograms (FBP3D.cpp:74-176): allocate the
+ * stack (target_width x target_height x projection_count) and fill it from the files of
+ * `directory`. A file's projection index is the 4 characters before a 4-character extension
+ * (FBP3D.cpp:97-104); other files are ignored; a missing index is an error. Each file is raw
+ * file_width x file_height pixels of file_channel_count channels of byte_per_channel (1 or 2,
+ * little endian) bytes; channel 0 is used, normalised by 255 / 65535, and resampled
+ * bilinearly (pixel centres aligned, edges clamped) when the sizes differ. Host threads read
+ * into pinned buffers overlapped with the device conversion. */
+int fbp_read_projections(fbp_context* ctx, const char* directory, int file_width, int file_height,
+                         int file_channel_count, int byte_per_channel, int target_width, int target_height,
+                         int projection_count);
+int fbp_read_projections_as_sinograms(fbp_context* ctx, const char* directory, int file_width, int file_height,
+                                      int file_channel_count, int byte_per_channel, int target_width,
+                                      int target_height, int projection_count);
+/* FBP3D::write_volume (FBP3D.cpp:178-195): one raw uint16 file per y-slice (x fastest, then z),
+ * round(clamp(v, 0, 1) * 65535), named directory + "/CTAnalyzer_Slice#" + 6-digit index + ".raw"
+ * (the reference always appends the separator). */
+int fbp_write_volume(fbp_context* ctx, const char* directory);
+/* The projection index a file name carries under the read_projections rule, or -1 (host only). */
+int fbp_projection_file_index(const char* path);
+
+/* Volume extremes, FBP3D::compute_min_value_of_volume / compute_max_value_of_volume
+ * (FBP3D.cpp:780-800): NaN ignored; 0, 0 for a volume without finite values. */
+int fbp_volume_min_max(fbp_context* ctx, float* min_value, float* max_value);
+/* FBP3D::normalize_histogram() (FBP3D.cpp:802-815): v' = (v - min) / (max - min) over the
+ * volume's extremes, in FP32 (0 everywhere when max <= min). The range stays on the device;
+ * right after a backprojection it comes from the backprojector's store epilogue. */
+int fbp_normalize_histogram(fbp_context* ctx);
+/* FBP3D::normalize_histogram(min texture, max texture) (FBP3D.cpp:817-826): given range. */
+int fbp_normalize_histogram_range(fbp_context* ctx, float min_value, float max_value);
 int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float xray_source_distance,
     float detector_panel_distance, float detector_width, float volume_width, float full_rotation_count,
     int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :524-559 */

@@ -224,6 +224,59 @@ def rebin_fan_to_parallel(fan: np.ndarray, g: dict, n_out: int, du_out: float) -
     return out
 
 
+def decode_projection_file(raw: bytes, width: int, height: int, channels: int, byte_per_channel: int) -> np.ndarray:
+    """One raw projection file as FBP3D::read_projections loads it
+    (Source/FilteredBackProjection/FBP3D.cpp:110-117): channel 0, normalised
+    like an UNSIGNED_SHORT / UNSIGNED_BYTE texture upload (v / 65535, v / 255)."""
+    dt = np.dtype("<u2") if byte_per_channel == 2 else np.dtype("u1")
+    a = np.frombuffer(raw, dtype=dt, count=width * height * channels).reshape(height, width, channels)[:, :, 0]
+    return (a.astype(np.float32) / np.float32(65535 if byte_per_channel == 2 else 255)).astype(np.float32)
+
+
+def resample_bilinear(img: np.ndarray, tw: int, th: int) -> np.ndarray:
+    """The library's resize for read_projections (the reference's Image::resize
+    lives in its absent GraphicsCortex library): pixel centres aligned, edges
+    clamped, FP32 in the library's operation order."""
+    img = np.asarray(img, dtype=np.float32)
+    fh, fw = img.shape
+    if (fw, fh) == (tw, th):
+        return img.copy()
+    f32 = np.float32
+    rx, ry = f32(fw) / f32(tw), f32(fh) / f32(th)
+    sx = np.clip((np.arange(tw, dtype=f32) + f32(0.5)) * rx - f32(0.5), f32(0), f32(fw - 1)).astype(f32)
+    sy = np.clip((np.arange(th, dtype=f32) + f32(0.5)) * ry - f32(0.5), f32(0), f32(fh - 1)).astype(f32)
+    x0 = sx.astype(np.int64); y0 = sy.astype(np.int64)
+    x1 = np.minimum(x0 + 1, fw - 1); y1 = np.minimum(y0 + 1, fh - 1)
+    ax = (sx - x0.astype(f32)).astype(f32)[None, :]; ay = (sy - y0.astype(f32)).astype(f32)[:, None]
+    one = f32(1)
+    top = ((one - ax) * img[y0][:, x0] + ax * img[y0][:, x1]).astype(f32)
+    bot = ((one - ax) * img[y1][:, x0] + ax * img[y1][:, x1]).astype(f32)
+    return ((one - ay) * top + ay * bot).astype(f32)
+
+
+def volume_slices_u16(vol: np.ndarray) -> np.ndarray:
+    """FBP3D::write_volume's slice conversion (FBP3D.cpp:178-195): y-slices
+    [y][z][x] as round(clamp(v, 0, 1) * 65535), GL's float -> normalised
+    unsigned short rule (round half to even)."""
+    v = np.clip(np.asarray(vol, dtype=np.float32), 0, 1).astype(np.float32)
+    return np.rint(v * np.float32(65535)).astype(np.uint16).transpose(1, 0, 2).copy()
+
+
+def normalize_histogram(vol: np.ndarray, min_value: float | None = None, max_value: float | None = None) -> np.ndarray:
+    """FBP3D::normalize_histogram (Source/FilteredBackProjection/FBP3D.cpp:780-826)
+    restated in FP32 with the library's operation order: d = v - min, r = max - min,
+    d / r (IEEE division), 0 everywhere when max <= min; the extremes ignore NaN."""
+    v = np.asarray(vol, dtype=np.float32)
+    if min_value is None:
+        finite = v[~np.isnan(v)]
+        min_value, max_value = (float(finite.min()), float(finite.max())) if finite.size else (0.0, 0.0)
+    mn, mx = np.float32(min_value), np.float32(max_value)
+    r = np.float32(mx - mn)
+    if not r > 0:
+        return np.zeros_like(v)
+    return ((v - mn) / r).astype(np.float32)
+
+
 def clip_negatives(vol: np.ndarray, y_limit: int | None = None) -> np.ndarray:
     vol = np.array(vol, dtype=np.float64, order="C", copy=True)
     nz, ny, nx = vol.shape

@@ -89,3 +89,14 @@ def test_cpp_dropin_links_against_library(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{PKG}", str(src), "-o", str(exe),
                         f"-L{PKG}", "-lfbp_b200", f"-Wl,-rpath,{PKG}"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_projection_file_index_rule():
+    """read_projections takes a file's projection index from the 4 characters
+    before a 4-character extension (FBP3D.cpp:97-104); names without one are
+    ignored. Host-only: no device is touched."""
+    import fbp_b200 as F
+    cases = {"dir/proj_0012.raw": 12, "a/b/0007.tif": 7, "scan1234.raw": 1234, "ab12cd.raw": 12,
+             "img-001.raw": -1, "x.raw": -1, "abc": -1, "readme.txt": -1}
+    for name, idx in cases.items():
+        assert F.projection_file_index(name) == idx, name

@@ -459,3 +459,98 @@ def test_symmetric_backprojector_rejects_other_geometries(fbp, oracle):
     with pytest.raises(fbp.FBPError) as e:
         _gpu_fdk(s, c, proj, 0)
     assert e.value.status == -6
+
+
+# ------------------------------------------------- histogram normalisation (f4)
+def test_normalize_histogram_after_backprojection(fbp, oracle, phantoms):
+    """Extremes folded in by the backprojector's store epilogue; result
+    bit-identical to the FP32 restatement (FBP3D.cpp:780-826)."""
+    c, proj = _cone_case(phantoms, oracle, 4)
+    s = fbp.FBP3D(0)  # clip after backprojection on, as in the reference
+    _gpu_fdk(s, c, proj, 0)
+    vol = s.read_volume()
+    lo, hi = s.volume_min_max()
+    assert (lo, hi) == (float(vol.min()), float(vol.max()))
+    s.normalize_histogram()
+    got = s.read_volume()
+    np.testing.assert_array_equal(got, oracle.normalize_histogram(vol))
+    assert got.min() == 0.0 and got.max() == 1.0
+
+
+def test_normalize_histogram_reduction_and_range(fbp, oracle):
+    """Volume written by the caller (ragged size, negatives): the extremes come
+    from the reduction kernel; the given-range overload; a flat volume."""
+    rng = np.random.default_rng(5)
+    vol = (rng.standard_normal((9, 7, 5)) * 3.0 - 1.0).astype(np.float32)
+    s = fbp.FBP3D(0)
+    s.generate_blank_volume(5, 7, 9)
+    s.write_volume_data(vol)
+    assert s.volume_min_max() == (float(vol.min()), float(vol.max()))
+    s.normalize_histogram()
+    np.testing.assert_array_equal(s.read_volume(), oracle.normalize_histogram(vol))
+    s.write_volume_data(vol)
+    s.normalize_histogram(-1.0, 2.5)
+    np.testing.assert_array_equal(s.read_volume(), oracle.normalize_histogram(vol, -1.0, 2.5))
+    s.write_volume_data(np.full_like(vol, 0.75))
+    s.normalize_histogram()
+    assert not s.read_volume().any()
+
+
+# ----------------------------------------------------------------- file I/O (f2)
+def _write_projection_files(d, arrays, stem="scan_", ext=".raw"):
+    for i, a in enumerate(arrays):
+        (d / f"{stem}{i:04d}{ext}").write_bytes(np.ascontiguousarray(a).tobytes())
+
+
+def test_read_projections_uint16(fbp, oracle, tmp_path):
+    rng = np.random.default_rng(21)
+    raw = [rng.integers(0, 65536, size=(12, 20), dtype=np.uint16).astype("<u2") for _ in range(5)]
+    _write_projection_files(tmp_path, raw)
+    (tmp_path / "readme.txt").write_text("not a projection")
+    (tmp_path / "scan_0099.raw").write_bytes(raw[0].tobytes())  # index out of range: ignored
+    s = fbp.FBP3D(0)
+    s.read_projections(str(tmp_path), 20, 12, 1, 2, 20, 12, 5)
+    got = s.download_projections()
+    ref = np.stack([oracle.decode_projection_file(r.tobytes(), 20, 12, 1, 2) for r in raw])
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_read_projections_rgb8_resampled_and_as_sinograms(fbp, oracle, tmp_path):
+    rng = np.random.default_rng(22)
+    raw = [rng.integers(0, 256, size=(12, 20, 3), dtype=np.uint8) for _ in range(4)]
+    _write_projection_files(tmp_path, raw, stem="p", ext=".bin")
+    ref = np.stack([oracle.resample_bilinear(oracle.decode_projection_file(r.tobytes(), 20, 12, 3, 1), 15, 9)
+                    for r in raw])
+    s = fbp.FBP3D(0)
+    s.read_projections(str(tmp_path), 20, 12, 3, 1, 15, 9, 4)
+    np.testing.assert_allclose(s.download_projections(), ref, rtol=0, atol=2e-7)
+    s.read_projections_as_sinograms(str(tmp_path), 20, 12, 3, 1, 15, 9, 4)
+    sino = s.download_sinograms(np.empty((9, 4, 15), np.float32))
+    np.testing.assert_allclose(sino, ref.transpose(1, 0, 2), rtol=0, atol=2e-7)
+
+
+def test_read_projections_errors(fbp, tmp_path):
+    s = fbp.FBP3D(0)
+    with pytest.raises(fbp.FBPError) as e:
+        s.read_projections(str(tmp_path / "missing"), 4, 4, 1, 2, 4, 4, 2)
+    assert e.value.status == -1
+    _write_projection_files(tmp_path, [np.zeros((4, 4), "<u2")])  # index 1 missing
+    with pytest.raises(fbp.FBPError) as e:
+        s.read_projections(str(tmp_path), 4, 4, 1, 2, 4, 4, 2)
+    assert "index 1" in str(e.value)
+    (tmp_path / "scan_0001.raw").write_bytes(b"\x00" * 8)  # short file
+    with pytest.raises(fbp.FBPError):
+        s.read_projections(str(tmp_path), 4, 4, 1, 2, 4, 4, 2)
+
+
+def test_write_volume_slices(fbp, oracle, tmp_path):
+    rng = np.random.default_rng(23)
+    vol = (rng.random((6, 5, 7)) * 2.0 - 0.5).astype(np.float32)  # [z][y][x], outside [0, 1] too
+    s = fbp.FBP3D(0)
+    s.generate_blank_volume(7, 5, 6)
+    s.write_volume_data(vol)
+    s.write_volume(str(tmp_path))
+    ref = oracle.volume_slices_u16(vol)
+    for y in range(5):
+        got = np.fromfile(tmp_path / f"CTAnalyzer_Slice#{y:06d}.raw", dtype="<u2").reshape(6, 7)
+        np.testing.assert_array_equal(got, ref[y])
