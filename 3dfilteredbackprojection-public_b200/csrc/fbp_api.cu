@@ -138,6 +138,7 @@ fbp::RowSet rowset_of(Stack& s) {
   rs.w_sdd = (float)s.w_sdd;
   rs.w_du = (float)s.w_du;
   rs.w_dv = (float)s.w_dv;
+  rs.w_voff = (float)s.w_voff;
   return rs;
 }
 
@@ -286,6 +287,8 @@ int record_weights(fbp_context* ctx, Stack& s, float sod, float odd, float det_w
   s.w_sdd = (double)sod + (double)odd;
   s.w_du = (double)det_w / s.u;
   s.w_dv = s.w_du;  // square detector pixels
+  // a row band of a taller detector: the weight needs the global row index
+  s.w_voff = ctx->det_rows_total > 0 ? ctx->det_row_off + 0.5 * ((double)s.v - ctx->det_rows_total) : 0.0;
   return FBP_OK;
 }
 
@@ -324,13 +327,29 @@ fbp::BPGeom cone_geom(const Stack& s, float sod, float odd, float det_w, float v
 int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
   if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
+  // sharding: detector row band and volume y-slab set on the context
+  if (ctx->det_rows_total > 0) {
+    if (ctx->det_row_off + s.v > ctx->det_rows_total)
+      return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector row band exceeds the detector");
+    g.row_off = ctx->det_row_off;
+    g.nv_total = ctx->det_rows_total;
+  }
+  int clip_limit = g.nz;  // the reference clips y-slices below z_size (FBP3D.cpp:448)
+  if (ctx->slab_ny > 0) {
+    if (ctx->slab_y0 + ctx->slab_ny > g.ny)
+      return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume slab exceeds the volume");
+    g.ny_total = g.ny;
+    g.y_off = ctx->slab_y0;
+    g.ny = ctx->slab_ny;
+    clip_limit = std::max(0, std::min(g.ny, g.nz - g.y_off));
+  }
   if (g.kind == FBP_GEOMETRY_CONE && !(g.sod > 0.0 && g.sdd >= g.sod))
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "source distance must be positive");
   if (!(g.du > 0.0) || !(g.vox > 0.0))
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
   FBP_TRY(flush_pending(ctx, s));
   FBP_TRY(ensure_volume(ctx, g.nx, g.ny, g.nz, false));
-  const int ylim = ctx->clip_after_bp ? g.nz : 0;  // the reference clips y-slices below z_size
+  const int ylim = ctx->clip_after_bp ? clip_limit : 0;
   return fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, ctx->precision == FBP_PRECISION_MIXED);
 }
 
@@ -823,6 +842,68 @@ int fbp_clip_negatives_of_volume(fbp_context* ctx) {
   if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "clip_negatives_of_volume but the volume is not allocated");
   ctx->minmax_valid = false;
   return fbp::launch_clip(ctx, ctx->vol, ctx->vx, ctx->vy, ctx->vz, ctx->vz);
+}
+
+// ---------------------------------------------------------- sharding (e)
+int fbp_set_detector_rows(fbp_context* ctx, int row_offset, int total_rows) {
+  FBP_CTX(ctx);
+  if (total_rows < 0 || row_offset < 0 || (total_rows == 0 && row_offset != 0) ||
+      (total_rows > 0 && row_offset >= total_rows))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad detector row band");
+  ctx->det_row_off = row_offset;
+  ctx->det_rows_total = total_rows;
+  return FBP_OK;
+}
+
+int fbp_set_volume_slab(fbp_context* ctx, int y_offset, int y_count) {
+  FBP_CTX(ctx);
+  if (y_offset < 0 || y_count < 0 || (y_count == 0 && y_offset != 0))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad volume slab");
+  ctx->slab_y0 = y_offset;
+  ctx->slab_ny = y_count;
+  return FBP_OK;
+}
+
+int fbp_plan_slabs(const fbp_geometry* g, int detector_cols, int detector_rows, int volume_h, int volume_v,
+                   int slabs, int* out) {
+  if (!g || !out || detector_cols <= 0 || detector_rows <= 0 || volume_h <= 0 || volume_v <= 0 || slabs <= 0 ||
+      slabs > volume_v)
+    return FBP_ERR_INVALID_ARGUMENT;
+  const bool cone = g->kind == FBP_GEOMETRY_CONE;
+  const double du = (double)g->detector_width / detector_cols, dv = du;  // square detector pixels
+  const double vox = (double)g->volume_width / volume_h;
+  const double sod = g->source_distance, sdd = (double)g->source_distance + g->detector_distance;
+  if (!(du > 0.0) || !(vox > 0.0) || (cone && !(sod > 0.0))) return FBP_ERR_INVALID_ARGUMENT;
+  const double cv = 0.5 * detector_rows - 0.5;
+  // farthest voxel centre from the rotation axis bounds the source distance over every view
+  const double rad = std::sqrt(2.0) * (0.5 * volume_h - 0.5) * vox;
+  const double dmin = cone ? (sod - rad) / sod : 1.0, dmax = cone ? (sod + rad) / sod : 1.0;
+  const double G = cone ? sdd / (sod * dv) : 1.0 / dv;
+  for (int k = 0; k < slabs; ++k) {
+    const int y0 = (int)((long long)volume_v * k / slabs), y1 = (int)((long long)volume_v * (k + 1) / slabs);
+    int r0 = 0, r1 = detector_rows;  // whole detector when a voxel may lie at or behind the source
+    if (dmin > 0.0) {
+      double vmin = 1e300, vmax = -1e300;
+      for (int y : {y0, y1 - 1})
+        for (double d : {dmin, dmax}) {
+          const double v = G * (y + 0.5 - 0.5 * volume_v) * vox / d + cv;
+          vmin = std::min(vmin, v);
+          vmax = std::max(vmax, v);
+        }
+      // bilinear taps use rows floor(v) and floor(v) + 1; one row of margin each side
+      r0 = (int)std::max(0.0, std::floor(vmin) - 1.0);
+      r1 = (int)std::min((double)detector_rows, std::floor(vmax) + 3.0);
+      if (r1 <= r0) {  // slab projects off the detector: keep one (all-zero-weight) row
+        r0 = std::min(std::max(r0, 0), detector_rows - 1);
+        r1 = r0 + 1;
+      }
+    }
+    out[4 * k] = y0;
+    out[4 * k + 1] = y1;
+    out[4 * k + 2] = r0;
+    out[4 * k + 3] = r1;
+  }
+  return FBP_OK;
 }
 
 // ---------------------------------------------------------- file I/O (f2)

@@ -93,6 +93,7 @@ struct BPArgs {
   int qg_pitch, qg_rows;  // element columns per plane row, element rows per group
   int resident;           // CTAs resident on the GPU at once (view-group skew of the interleaved walk)
   int* minmax;            // fold the stored values' min / max into this pair (or nullptr)
+  int y_off, ny_total;    // the volume is y-slices [y_off, y_off + ny) of ny_total
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -163,7 +164,7 @@ __device__ void tile_geo(const BPArgs& a, int k, int ix0, int iy0, int iz0, int 
   const double c = a.trig[k].x, s = a.trig[k].y;
   const double Xc = (ix0 + 0.5 - 0.5 * a.nx) * a.vox;
   const double Zc = (iz0 + 0.5 - 0.5 * a.nz) * a.vox;
-  t.Yc = (iy0 + 0.5 - 0.5 * a.ny) * a.vox;
+  t.Yc = (a.y_off + iy0 + 0.5 - 0.5 * a.ny_total) * a.vox;
   if (a.kind == FBP_GEOMETRY_CONE) {
     const double K = a.sdd / (a.sod * a.du);
     t.Dx = a.vox * c / a.sod;
@@ -1093,7 +1094,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   a.dv = g.dv;
   a.vox = g.vox;
   a.cu = 0.5 * g.nu - 0.5;
-  a.cv = 0.5 * g.nv - 0.5;
+  // row band of a taller detector / y-slab of a taller volume (sharding)
+  a.cv = 0.5 * (g.nv_total > 0 ? g.nv_total : g.nv) - 0.5 - g.row_off;
+  a.y_off = g.y_off;
+  a.ny_total = g.ny_total > 0 ? g.ny_total : g.ny;
   if (g.kind == FBP_GEOMETRY_CONE) {
     a.dvn = (float)(g.sdd / (g.sod * g.dv) * g.vox);
     a.scale = (float)(pi / g.nviews * g.sdd / (g.sod * g.du));
@@ -1153,12 +1157,13 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   const int nty = (g.ny + NY - 1) / NY;
 
   // footprint pre-pass (cached per geometry and layout)
-  double key[16] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
+  double key[20] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
                     (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz,
-                    (double)a.align, (double)NY};
+                    (double)a.align, (double)NY, (double)g.row_off, (double)g.nv_total, (double)g.y_off,
+                    (double)g.ny_total};
   fbp_context::BPPlan& plan = ctx->plan;
   bool hit = plan.valid;
-  for (int i = 0; i < 16 && hit; ++i) hit = plan.key[i] == key[i];
+  for (int i = 0; i < 20 && hit; ++i) hit = plan.key[i] == key[i];
   if (!hit) {
     plan.valid = false;
     if (ctx->span_cap < 4) {
@@ -1186,7 +1191,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     plan.box_u = std::max(hs[0], 2);
     plan.box_v = std::max(hs[1], 2);
     plan.valid = true;
-    for (int i = 0; i < 16; ++i) plan.key[i] = key[i];
+    for (int i = 0; i < 20; ++i) plan.key[i] = key[i];
   }
   const int bu = (plan.box_u + a.align - 1) / a.align * a.align;
   // a pair element carries row v + 1 with it: one row less to stage

@@ -64,6 +64,7 @@ struct Stack {
   double log_base = 1.0;
   bool weights_pending = false;
   double w_sdd = 0, w_du = 0, w_dv = 0;
+  double w_voff = 0;  // rows held are a band of a taller detector: centre offset in rows
   size_t rows() const { return (size_t)v * n; }
   size_t bytes32() const { return (size_t)pitch * rows() * sizeof(float); }
   static int elem_bytes(int layout) {
@@ -99,6 +100,8 @@ struct fbp_context {
   int pad_len = 0;
   int clip_after_bp = 1;
   int bp_variant = FBP_BACKPROJECTOR_AUTO;
+  int det_row_off = 0, det_rows_total = 0;  // fbp_set_detector_rows (0 rows: the whole detector)
+  int slab_y0 = 0, slab_ny = 0;             // fbp_set_volume_slab (0 slices: the whole volume)
   int last_bp[4] = {-1, -1, 0, 0};  // variant, layout, box_u, box_v of the last backprojection
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched by this context
@@ -131,7 +134,7 @@ struct fbp_context {
   // (tile, view) for the geometry (samples, rows including row v + 1)
   struct BPPlan {
     bool valid = false;
-    double key[16] = {0};
+    double key[20] = {0};
     int box_u = 0, box_v = 0;
   } plan;
 };
@@ -162,6 +165,7 @@ struct RowSet {
   float log_base = 1.f;
   bool weight = false;
   float w_sdd = 0, w_du = 0, w_dv = 0;
+  float w_voff = 0;  // detector-centre offset of the rows (row band of a taller detector)
   // output: in place into `data` (out == nullptr) or into a pair layout
   void* out = nullptr;
   int out_layout = kLayoutRaw32;
@@ -192,6 +196,10 @@ struct BPGeom {
   double span, offset;
   int nu, nv, nviews;
   int nx, ny, nz;
+  // sharding: the stack holds detector rows [row_off, row_off + nv) of nv_total
+  // rows, and the volume y-slices [y_off, y_off + ny) of ny_total (0: whole)
+  int row_off = 0, nv_total = 0;
+  int y_off = 0, ny_total = 0;
 };
 // Backproject the stack's content (filt when filtered, else f32 rows). In
 // the MIXED form (`mixed`) f32 content is first packed into the FP16 layout

@@ -15,7 +15,7 @@ __device__ __forceinline__ float load_pre(const RowSet& rs, long long r, int i) 
   if (rs.weight) {
     int iv = rs.sinogram ? (int)(r / rs.n_views) : (int)(r % rs.n_v);
     float u = (i + 0.5f - 0.5f * rs.m) * rs.w_du;
-    float v = (iv + 0.5f - 0.5f * rs.n_v) * rs.w_dv;
+    float v = (iv + 0.5f - 0.5f * rs.n_v + rs.w_voff) * rs.w_dv;
     x *= rs.w_sdd * rsqrtf(rs.w_sdd * rs.w_sdd + u * u + v * v);
   }
   return x;

@@ -141,6 +141,9 @@ SIGNATURES = {
     "fbp_read_projections_as_sinograms": [_P, C.c_char_p, _I, _I, _I, _I, _I, _I, _I],
     "fbp_write_volume": [_P, C.c_char_p],
     "fbp_projection_file_index": [C.c_char_p],
+    "fbp_plan_slabs": [C.POINTER(Geometry), _I, _I, _I, _I, _I, C.POINTER(C.c_int)],
+    "fbp_set_detector_rows": [_P, _I, _I],
+    "fbp_set_volume_slab": [_P, _I, _I],
     "fbp_normalize_histogram": [_P],
     "fbp_normalize_histogram_range": [_P, C.c_float, C.c_float],
     "fbp_project_backward_cone_fdk_from_projections": [_P, _F, _F, _F, _F, _F, _I, _I, _F],
@@ -163,6 +166,16 @@ SIGNATURES = {
 def projection_file_index(path: str) -> int:
     """Projection index that read_projections takes from a file name, or -1."""
     return library().fbp_projection_file_index(str(path).encode())
+
+
+def plan_slabs(geometry: "Geometry", detector_cols: int, detector_rows: int, volume_h: int, volume_v: int,
+               slabs: int) -> list[tuple[int, int, int, int]]:
+    """fbp_plan_slabs: per slab (y0, y1, row0, row1); host only, no device needed."""
+    out = (C.c_int * (4 * slabs))()
+    rc = library().fbp_plan_slabs(C.byref(geometry), detector_cols, detector_rows, volume_h, volume_v, slabs, out)
+    if rc != 0:
+        raise FBPError(rc, "fbp_plan_slabs: invalid arguments")
+    return [tuple(out[4 * k:4 * k + 4]) for k in range(slabs)]
 
 
 def library() -> C.CDLL:
@@ -280,6 +293,14 @@ class FBP3D:
         names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16"}
         return {"kernel": "symmetric" if v.value == Backprojector.SYMMETRIC else "generic",
                 "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value)}
+
+    def set_detector_rows(self, row_offset: int, total_rows: int) -> None:
+        """The stacks hold rows [row_offset, row_offset + v) of a total_rows-row detector (0, 0: whole)."""
+        self.ctx.call("fbp_set_detector_rows", int(row_offset), int(total_rows))
+
+    def set_volume_slab(self, y_offset: int, y_count: int) -> None:
+        """project_backward_* compute only y-slices [y_offset, y_offset + y_count) (0, 0: whole)."""
+        self.ctx.call("fbp_set_volume_slab", int(y_offset), int(y_count))
 
     def memory_in_use(self) -> int:
         b = C.c_size_t()

@@ -173,6 +173,22 @@ int fbp_apply_fdk_weights_to_sinograms(fbp_context* ctx, float xray_source_dista
 int fbp_apply_filter_to_projections(fbp_context* ctx, int filter_type);                               /* :389-414 */
 int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type);                                 /* :417-442 */
 int fbp_clip_negatives_of_volume(fbp_context* ctx);                                                    /* :444-458 */
+/* ---- sharding (no counterpart in the reference, which runs on one GL context) ----------
+ * One volume over several GPUs without a collective on the data path: y-slab k of the
+ * volume needs only the detector rows its voxels project to. fbp_plan_slabs splits
+ * volume_v y-slices into `slabs` balanced slabs and writes, per slab, out[4k..4k+3] =
+ * {y0, y1, row0, row1}: slices [y0, y1) and detector rows [row0, row1) (cone magnification
+ * bound over every view, bilinear neighbour and one row of margin included). Host only.
+ * On the rank of slab k: fbp_set_detector_rows(ctx, row0, detector_rows) declares that the
+ * stacks hold that row band (the FDK weight and the backprojector use the global row), and
+ * fbp_set_volume_slab(ctx, y0, y1 - y0) makes project_backward_* (called with the whole
+ * volume's resolution) compute only those y-slices; the context's volume is the slab.
+ * Offsets 0 and counts 0 restore the whole detector / volume. */
+int fbp_plan_slabs(const fbp_geometry* geometry, int detector_cols, int detector_rows, int volume_h, int volume_v,
+                   int slabs, int* out);
+int fbp_set_detector_rows(fbp_context* ctx, int row_offset, int total_rows);
+int fbp_set_volume_slab(fbp_context* ctx, int y_offset, int y_count);
+
 /* ---- file I/O (FBP3D.cpp:74-195) -------------------------------------------------------
  * FBP3D::read_projections / read_projections_as_sinograms (FBP3D.cpp:74-176): allocate the
  * stack (target_width x target_height x projection_count) and fill it from the files of

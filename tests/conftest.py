@@ -40,3 +40,12 @@ def oracle():
 def phantoms():
     import phantoms as P
     return P
+
+
+@pytest.fixture(scope="session")
+def fbp():
+    """The ctypes mirror over the built library (host-only calls work without a GPU)."""
+    import build as B
+    B.build()
+    import fbp_b200
+    return fbp_b200

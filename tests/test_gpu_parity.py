@@ -554,3 +554,52 @@ def test_write_volume_slices(fbp, oracle, tmp_path):
     for y in range(5):
         got = np.fromfile(tmp_path / f"CTAnalyzer_Slice#{y:06d}.raw", dtype="<u2").reshape(6, 7)
         np.testing.assert_array_equal(got, ref[y])
+
+
+# ------------------------------------------------------- y-slab sharding (e)
+@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+def test_slab_sharding_matches_whole_volume(fbp, oracle, phantoms, precision):
+    """The ranks of a 3-slab plan, run one after another on one GPU: each
+    context holds only its detector row band and its y-slab; the slabs put
+    together equal the whole-volume reconstruction."""
+    import sharding
+    c, proj = _cone_case(phantoms, oracle, 4 if precision == "FP32" else 2)
+    ga = phantoms.geometry_args(c)
+    g = fbp.Geometry.cone(ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"],
+                          ga["full_rotation_count"], ga["offset"])
+    prec = getattr(fbp.Precision, precision)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(prec)
+    whole = _gpu_fdk(s, c, proj, 0)
+    plan = fbp.plan_slabs(g, c["nu"], c["nv"], c["nx"], c["ny"], 3)
+    parts = []
+    for slab in plan:
+        r = fbp.FBP3D(0)
+        r.set_clip_after_backprojection(False)
+        r.set_precision(prec)
+        sharding.reconstruct_slab(r, proj, g, c["nx"], c["ny"], 0, slab)
+        part = r.read_volume()
+        assert part.shape == (c["nz"], slab[1] - slab[0], c["nx"])
+        parts.append(part)
+    vol = np.concatenate(parts, axis=1)
+    ref = oracle.fdk(proj, c, 0)
+    tol = TOL_FP32 if precision == "FP32" else TOL_MIXED
+    print(f"slabs {plan}: vs whole {relative_rmse(vol, whole):.2e}, vs oracle {relative_rmse(vol, ref):.2e}")
+    assert relative_rmse(vol, whole) < tol
+    assert relative_rmse(vol, ref) < tol
+
+
+def test_slab_clip_keeps_the_reference_extent(fbp, oracle):
+    """Clip after backprojection on a slab: only global y-slices < z_size are
+    clipped (FBP3D.cpp:448), as in the whole volume."""
+    import sharding
+    c, proj = _sym_case(oracle, nviews=64, n=32, ny=40, offset=0.0)
+    g = fbp.Geometry.cone(c["sod"], c["sdd"] - c["sod"], c["nu"] * c["du"], c["nx"] * c["vox"], 1.0, 0.0)
+    ref = oracle.clip_negatives(oracle.fdk(proj, c, 2), y_limit=c["nz"])
+    parts = []
+    for slab in fbp.plan_slabs(g, c["nu"], c["nv"], c["nx"], c["ny"], 2):
+        r = fbp.FBP3D(0)
+        sharding.reconstruct_slab(r, proj, g, c["nx"], c["ny"], 2, slab)
+        parts.append(r.read_volume())
+    assert relative_rmse(np.concatenate(parts, axis=1), ref) < TOL_FP32
