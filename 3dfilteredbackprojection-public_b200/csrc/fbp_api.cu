@@ -100,26 +100,32 @@ void free_stack(Stack& s) {
   s.sinogram = sino;
 }
 
-int alloc_stack(fbp_context* ctx, Stack& s, int u, int v, int n) {
+// Size the stack for u x v x n (clearing it, as generate_blank_* do,
+// FBP3D.cpp:30-56). The allocation only grows: a smaller stack reuses it, so
+// a context serving jobs of varying size stops allocating (and cudaFree's
+// device-wide synchronisation) once it has seen its largest job.
+int alloc_stack(fbp_context* ctx, Stack& s, int u, int v, int n, bool clear = true) {
   if (u <= 0 || v <= 0 || n <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "stack sizes must be positive");
-  if (s.f32 && s.u == u && s.v == v && s.n == n) {
-    // same size: keep the allocation and clear it (FBP3D.cpp:30-38)
-    s.filtered = false;
-    s.log_pending = s.weights_pending = false;
-    return fbp::cuda_check(ctx, cudaMemsetAsync(s.f32, 0, s.bytes32(), ctx->stream), "clear stack");
+  const int pitch = round_up(u, 4);
+  const size_t need = (size_t)pitch * v * n * sizeof(float);
+  if (!s.f32 || s.f32_cap < need) {
+    cudaFree(s.f32);
+    s.f32 = nullptr;
+    s.f32_cap = 0;
+    if (cudaMalloc(&s.f32, need) != cudaSuccess) {
+      s.f32 = nullptr;
+      cudaGetLastError();
+      return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the detector stack failed");
+    }
+    s.f32_cap = need;
   }
-  free_stack(s);
   s.u = u;
   s.v = v;
   s.n = n;
-  s.pitch = round_up(u, 4);
-  cudaError_t e = cudaMalloc(&s.f32, s.bytes32());
-  if (e != cudaSuccess) {
-    s.f32 = nullptr;
-    free_stack(s);
-    cudaGetLastError();
-    return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the detector stack failed");
-  }
+  s.pitch = pitch;
+  s.filtered = false;
+  s.log_pending = s.weights_pending = false;
+  if (!clear) return FBP_OK;
   return fbp::cuda_check(ctx, cudaMemsetAsync(s.f32, 0, s.bytes32(), ctx->stream), "clear stack");
 }
 
@@ -168,30 +174,32 @@ int require_stack(fbp_context* ctx, const Stack& s, const char* what) {
 int ensure_volume(fbp_context* ctx, int x, int y, int z, bool clear) {
   ctx->minmax_valid = false;
   if (x <= 0 || y <= 0 || z <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume sizes must be positive");
+  const size_t need = sizeof(float) * (size_t)x * y * z;
   if (!(ctx->vol && ctx->vx == x && ctx->vy == y && ctx->vz == z)) {
-    cudaFree(ctx->vol);
-    ctx->vol = nullptr;
-    ctx->vx = ctx->vy = ctx->vz = 0;
-    cudaError_t e = cudaMalloc(&ctx->vol, sizeof(float) * (size_t)x * y * z);
-    if (e != cudaSuccess) {
+    if (!ctx->vol || ctx->vol_cap < need) {  // grow only, like the stacks
+      cudaFree(ctx->vol);
       ctx->vol = nullptr;
-      cudaGetLastError();
-      return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the volume failed");
+      ctx->vol_cap = 0;
+      if (cudaMalloc(&ctx->vol, need) != cudaSuccess) {
+        ctx->vol = nullptr;
+        ctx->vx = ctx->vy = ctx->vz = 0;
+        cudaGetLastError();
+        return fbp::set_error(ctx, FBP_ERR_OUT_OF_MEMORY, "cudaMalloc of the volume failed");
+      }
+      ctx->vol_cap = need;
     }
     ctx->vx = x;
     ctx->vy = y;
     ctx->vz = z;
     clear = true;
   }
-  if (clear)
-    return fbp::cuda_check(ctx, cudaMemsetAsync(ctx->vol, 0, sizeof(float) * (size_t)x * y * z, ctx->stream),
-                           "clear volume");
+  if (clear) return fbp::cuda_check(ctx, cudaMemsetAsync(ctx->vol, 0, need, ctx->stream), "clear volume");
   return FBP_OK;
 }
 
 int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int n, int on_dev) {
   if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
-  if (!(s.f32 && s.u == u && s.v == v && s.n == n)) FBP_TRY(alloc_stack(ctx, s, u, v, n));
+  if (!(s.f32 && s.u == u && s.v == v && s.n == n)) FBP_TRY(alloc_stack(ctx, s, u, v, n, false));
   s.filtered = false;
   s.log_pending = s.weights_pending = false;
   FBP_TRY(fbp::cuda_check(ctx,
@@ -449,9 +457,13 @@ int prepare_packed(fbp_context* ctx, Stack& s, int layout) {
     if (cuda_check(ctx, cudaMalloc(&s.filt, need), "cudaMalloc(packed views)")) return FBP_ERR_OUT_OF_MEMORY;
     s.filt_bytes = need;
   }
-  if (!s.inv_scale && cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)")) {
+  if (!s.inv_scale || s.scale_cap < s.n) {
+    cudaFree(s.inv_scale);
     s.inv_scale = nullptr;
-    return FBP_ERR_OUT_OF_MEMORY;
+    s.scale_cap = 0;
+    if (cuda_check(ctx, cudaMalloc(&s.inv_scale, sizeof(float) * 2 * s.n), "cudaMalloc(view scales)"))
+      return FBP_ERR_OUT_OF_MEMORY;
+    s.scale_cap = s.n;
   }
   float* scale = s.inv_scale + s.n;
   // the four-term difference of the gradient layout is at most 4 max|value|
@@ -612,11 +624,11 @@ int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, i
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes) {
   if (!ctx || !bytes) return FBP_ERR_INVALID_ARGUMENT;
   size_t b = 0;
-  if (ctx->vol) b += sizeof(float) * (size_t)ctx->vx * ctx->vy * ctx->vz;
+  if (ctx->vol) b += ctx->vol_cap;
   for (const Stack* s : {&ctx->proj, &ctx->sino}) {
-    if (s->f32) b += s->bytes32();
+    if (s->f32) b += s->f32_cap;
     if (s->filt) b += s->filt_bytes;
-    if (s->inv_scale) b += sizeof(float) * 2 * s->n;
+    if (s->inv_scale) b += sizeof(float) * 2 * s->scale_cap;
   }
   b += ctx->scratch_bytes;
   *bytes = b;
@@ -644,7 +656,9 @@ int fbp_free_volume(fbp_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->vol);
   ctx->vol = nullptr;
+  ctx->vol_cap = 0;
   ctx->vx = ctx->vy = ctx->vz = 0;
+  ctx->minmax_valid = false;
   return FBP_OK;
 }
 

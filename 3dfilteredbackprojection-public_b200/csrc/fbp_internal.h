@@ -56,7 +56,9 @@ struct Stack {
   size_t filt_bytes = 0;
   int filt_layout = kLayoutPair32;
   int filt_pitch = 0;             // elements per row of filt (multiple of 4)
-  float* inv_scale = nullptr;     // per view (x2: [inv | scale]) for kLayoutPair16
+  float* inv_scale = nullptr;     // per view (x2: [inv | scale]) for the FP16 layouts
+  int scale_cap = 0;              // views inv_scale has room for
+  size_t f32_cap = 0;             // bytes allocated at f32 (buffers only grow: no cudaFree between jobs)
   // Log normalisation and FDK weights recorded by their calls and applied
   // inside the filter kernel's load (log first, then weight), or by a
   // standalone pass when something else reads the rows first.
@@ -108,6 +110,7 @@ struct fbp_context {
 
   float* vol = nullptr;
   int vx = 0, vy = 0, vz = 0;
+  size_t vol_cap = 0;  // bytes allocated at vol
 
   fbp::Stack proj;
   fbp::Stack sino;

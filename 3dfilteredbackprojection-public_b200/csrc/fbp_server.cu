@@ -1,0 +1,293 @@
+// Reconstruction server: continuous batching of independent FBP jobs on one
+// GPU. No counterpart in the reference (one reconstruction per process on a
+// GL context).
+//
+// A server owns `slots` worker threads, each with its own fbp_context (own
+// CUDA stream and buffers). Jobs are queued in arrival order; a free worker
+// takes the first queued job whose working-set estimate fits the HBM budget
+// beside the jobs already running (looking at most kLookahead jobs past the
+// head, so a large job is not starved), or the head job alone when nothing
+// runs. A job's uploads, kernels and readback run on its worker's stream, so
+// jobs admitted together overlap on the device (copies of one beside the
+// kernels of another, small jobs beside large ones). Results are identical to
+// the same job run alone: every job runs the same kernels with the same
+// arguments on its own buffers.
+//
+// Worker buffers only grow (see alloc_stack), so after warm-up a slot stops
+// allocating; the budget covers the working sets of running jobs, and each
+// slot retains at most its largest job's buffers.
+
+#include "fbp_internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+constexpr int kLookahead = 8;    // queued jobs looked at past a head that does not fit
+constexpr int kMaxBypass = 16;   // times a head may be passed over before it blocks the queue
+
+struct Job {
+  fbp_request req;
+  long long ticket = 0;
+  size_t bytes = 0;
+  int bypassed = 0;  // later jobs started while this one headed the queue
+  int status = FBP_OK;
+  bool done = false;
+  double queued = 0, started = 0, finished = 0;  // ms since the server started
+  std::string error;
+};
+
+struct Worker {
+  fbp_context* ctx = nullptr;
+  float* d_in = nullptr;  // 2D jobs: sinogram and image on the device (grow only)
+  float* d_out = nullptr;
+  size_t in_cap = 0, out_cap = 0;
+  std::thread thread;
+};
+
+size_t estimate_bytes(const fbp_request& r) {
+  if (r.reserve_bytes > 0) return (size_t)r.reserve_bytes;
+  const size_t cols4 = (size_t)(r.det_cols + 3) / 4 * 4;
+  if (r.kind == FBP_JOB_CONE) {
+    const size_t stack = cols4 * r.det_rows * r.views * 4;
+    const size_t packed = r.precision == FBP_PRECISION_MIXED ? (size_t)r.views * (r.det_rows + 1) * (r.det_cols + 1) * 8
+                                                             : cols4 * (r.det_rows + 1) * r.views * 8;
+    const size_t vol = (size_t)r.vol_h * r.vol_v * r.vol_h * 4;
+    const size_t split = std::min<size_t>((size_t)r.det_rows * r.views, 65536) * (cols4 + 64) * 4;
+    return stack + packed + vol + split + (64u << 20);
+  }
+  if (r.kind == FBP_JOB_FAN2D || r.kind == FBP_JOB_PARALLEL2D)
+    return cols4 * r.views * 4 * 3 + (size_t)r.vol_h * r.vol_h * 4 + (16u << 20);
+  return 0;
+}
+
+int device_buffer(float** p, size_t* cap, size_t bytes) {
+  if (*p && *cap >= bytes) return FBP_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return FBP_ERR_OUT_OF_MEMORY;
+  }
+  *cap = bytes;
+  return FBP_OK;
+}
+
+}  // namespace
+
+struct fbp_server {
+  int device = -1;
+  size_t budget = 0;
+  Clock::time_point t0;
+  std::vector<Worker> workers;
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv;
+  std::deque<Job*> queue;
+  std::unordered_map<long long, Job*> jobs;
+  size_t reserved = 0;
+  int running = 0;
+  long long next_ticket = 1;
+  bool stop = false;
+
+  double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+
+  // first admissible queued job (caller holds mu)
+  std::deque<Job*>::iterator pick() {
+    int seen = 0;
+    for (auto it = queue.begin(); it != queue.end() && seen <= kLookahead; ++it, ++seen) {
+      if (running == 0 && it == queue.begin()) return it;  // nothing runs: the head goes, whatever its size
+      if (reserved + (*it)->bytes <= budget) {
+        if (it != queue.begin()) ++queue.front()->bypassed;
+        return it;
+      }
+      if (queue.front()->bypassed >= kMaxBypass) break;  // the head waits for memory; nobody passes it
+    }
+    return queue.end();
+  }
+
+  int run(Worker& w, Job& j) {
+    const fbp_request& r = j.req;
+    if (r.kind == FBP_JOB_HOST_WAIT) {  // scheduler tests: holds the slot and the reservation for views us
+      std::this_thread::sleep_for(std::chrono::microseconds(std::max(0, r.views)));
+      return FBP_OK;
+    }
+    fbp_context* c = w.ctx;
+    if (!c) {
+      j.error = "server has no device";
+      return FBP_ERR_STATE;
+    }
+    if (!r.input || !r.output) {
+      j.error = "null input or output";
+      return FBP_ERR_INVALID_ARGUMENT;
+    }
+    const fbp_geometry& g = r.geometry;
+    int rc = fbp_set_precision(c, r.precision);
+    if (r.kind == FBP_JOB_CONE) {
+      if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
+      if (!rc) rc = fbp_upload_projections(c, r.input, r.det_cols, r.det_rows, r.views, 0);
+      if (!rc) rc = fbp_apply_fdk_weights_to_projections(c, g.source_distance, g.detector_distance, g.detector_width);
+      if (!rc) rc = fbp_apply_filter_to_projections(c, r.filter_type);
+      if (!rc)
+        rc = fbp_project_backward_cone_fdk_from_projections(c, g.source_distance, g.detector_distance,
+                                                            g.detector_width, g.volume_width, g.full_rotation_count,
+                                                            r.vol_h, r.vol_v, g.rotation_offset_radian);
+      if (!rc) rc = fbp_read_volume(c, r.output, 0);
+    } else if (r.kind == FBP_JOB_FAN2D || r.kind == FBP_JOB_PARALLEL2D) {
+      const size_t in = (size_t)r.det_cols * r.views * 4, out = (size_t)r.vol_h * r.vol_h * 4;
+      rc = device_buffer(&w.d_in, &w.in_cap, in);
+      if (!rc) rc = device_buffer(&w.d_out, &w.out_cap, out);
+      cudaStream_t st = c->stream;
+      if (!rc && cudaMemcpyAsync(w.d_in, r.input, in, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = FBP_ERR_CUDA;
+      const bool fan = r.kind == FBP_JOB_FAN2D;
+      const float sdd = fan ? g.source_distance + g.detector_distance : 0.f;
+      if (!rc) rc = fbp2d_filter_sinogram(c, w.d_in, r.det_cols, r.views, r.filter_type, sdd, g.detector_width);
+      fbp_geometry gg = g;
+      gg.kind = fan ? FBP_GEOMETRY_CONE : FBP_GEOMETRY_PARALLEL;
+      if (!rc) rc = fbp2d_project_backward(c, w.d_in, r.det_cols, r.views, &gg, w.d_out, r.vol_h, r.vol_h);
+      if (!rc && cudaMemcpyAsync(r.output, w.d_out, out, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = FBP_ERR_CUDA;
+      if (!rc) rc = fbp_synchronize(c);
+    } else {
+      j.error = "unknown job kind";
+      return FBP_ERR_INVALID_ARGUMENT;
+    }
+    if (rc && j.error.empty()) j.error = fbp_last_error(c);
+    return rc;
+  }
+
+  void worker_main(Worker& w) {
+    if (device >= 0) cudaSetDevice(device);
+    for (;;) {
+      Job* j = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        std::deque<Job*>::iterator it = queue.end();
+        // wake for an admissible job; leave once stopped with nothing queued
+        work_cv.wait(lk, [&] { return (it = pick()) != queue.end() || (stop && queue.empty()); });
+        if (it == queue.end()) return;
+        j = *it;
+        queue.erase(it);
+        reserved += j->bytes;
+        ++running;
+        j->started = now_ms();
+      }
+      const int rc = run(w, *j);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        j->status = rc;
+        j->finished = now_ms();
+        j->done = true;
+        reserved -= j->bytes;
+        --running;
+      }
+      done_cv.notify_all();
+      work_cv.notify_all();  // memory and a slot freed up
+    }
+  }
+};
+
+extern "C" {
+
+int fbp_server_create(fbp_server** out, int device, size_t hbm_budget_bytes, int slots) {
+  if (!out || slots <= 0 || slots > 64) return FBP_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  fbp_server* s = new fbp_server();
+  s->device = device;
+  s->t0 = Clock::now();
+  s->workers.resize(slots);
+  if (device >= 0) {
+    if (hbm_budget_bytes == 0) {
+      size_t free_b = 0, total_b = 0;
+      int prev = 0;
+      cudaGetDevice(&prev);
+      cudaSetDevice(device);
+      cudaMemGetInfo(&free_b, &total_b);
+      cudaSetDevice(prev);
+      hbm_budget_bytes = free_b / 10 * 8;  // 80 % of what is free now
+    }
+    for (auto& w : s->workers) {
+      const int rc = fbp_create(&w.ctx, device);
+      if (rc) {
+        for (auto& v : s->workers) fbp_destroy(v.ctx);
+        delete s;
+        return rc;
+      }
+    }
+  }
+  s->budget = hbm_budget_bytes;
+  for (auto& w : s->workers) w.thread = std::thread([s, &w] { s->worker_main(w); });
+  *out = s;
+  return FBP_OK;
+}
+
+int fbp_server_submit(fbp_server* s, const fbp_request* req, long long* ticket) {
+  if (!s || !req || !ticket) return FBP_ERR_INVALID_ARGUMENT;
+  Job* j = new Job();
+  j->req = *req;
+  j->bytes = estimate_bytes(*req);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) {
+      delete j;
+      return FBP_ERR_STATE;
+    }
+    j->ticket = s->next_ticket++;
+    j->queued = s->now_ms();
+    s->jobs[j->ticket] = j;
+    s->queue.push_back(j);
+    *ticket = j->ticket;
+  }
+  s->work_cv.notify_all();
+  return FBP_OK;
+}
+
+int fbp_server_wait(fbp_server* s, long long ticket, fbp_job_result* result) {
+  if (!s) return FBP_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return FBP_ERR_INVALID_ARGUMENT;
+  Job* j = it->second;
+  s->done_cv.wait(lk, [&] { return j->done; });
+  if (result) {
+    result->status = j->status;
+    result->queued_ms = j->queued;
+    result->started_ms = j->started;
+    result->finished_ms = j->finished;
+    std::memset(result->error, 0, sizeof(result->error));
+    std::strncpy(result->error, j->error.c_str(), sizeof(result->error) - 1);
+  }
+  s->jobs.erase(it);
+  delete j;
+  return FBP_OK;
+}
+
+int fbp_server_destroy(fbp_server* s) {
+  if (!s) return FBP_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;  // queued jobs still run; then the workers leave
+  }
+  s->work_cv.notify_all();
+  for (auto& w : s->workers)
+    if (w.thread.joinable()) w.thread.join();
+  for (auto& w : s->workers) {
+    cudaFree(w.d_in);
+    cudaFree(w.d_out);
+    fbp_destroy(w.ctx);
+  }
+  for (auto& kv : s->jobs) delete kv.second;
+  delete s;
+  return FBP_OK;
+}
+
+}  // extern "C"

@@ -61,6 +61,13 @@ class FilterImpl(enum.IntEnum):
     TOEPLITZ = 2
 
 
+class JobKind(enum.IntEnum):
+    CONE = 0
+    FAN2D = 1
+    PARALLEL2D = 2
+    HOST_WAIT = 3
+
+
 class Geometry(C.Structure):
     """fbp_geometry (include/fbp_b200.h)."""
     CONE = 0
@@ -142,6 +149,10 @@ SIGNATURES = {
     "fbp_write_volume": [_P, C.c_char_p],
     "fbp_projection_file_index": [C.c_char_p],
     "fbp_plan_slabs": [C.POINTER(Geometry), _I, _I, _I, _I, _I, C.POINTER(C.c_int)],
+    "fbp_server_create": [C.POINTER(C.c_void_p), _I, C.c_size_t, _I],
+    "fbp_server_submit": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
+    "fbp_server_wait": [C.c_void_p, C.c_longlong, C.c_void_p],
+    "fbp_server_destroy": [C.c_void_p],
     "fbp_set_detector_rows": [_P, _I, _I],
     "fbp_set_volume_slab": [_P, _I, _I],
     "fbp_normalize_histogram": [_P],
@@ -161,6 +172,62 @@ SIGNATURES = {
     "fbp_kernel_launch_count": [_P, C.POINTER(C.c_uint64)],
     "fbp_measure_smem_bandwidth": [_P, C.POINTER(C.c_double)],
 }
+
+
+class Request(C.Structure):
+    """fbp_request (include/fbp_b200.h)."""
+    _fields_ = [("kind", C.c_int), ("precision", C.c_int), ("filter_type", C.c_int), ("clip", C.c_int),
+                ("geometry", Geometry), ("det_cols", C.c_int), ("det_rows", C.c_int), ("views", C.c_int),
+                ("vol_h", C.c_int), ("vol_v", C.c_int), ("reserve_bytes", C.c_longlong),
+                ("input", C.c_void_p), ("output", C.c_void_p)]
+
+
+class JobResult(C.Structure):
+    """fbp_job_result (include/fbp_b200.h)."""
+    _fields_ = [("status", C.c_int), ("queued_ms", C.c_double), ("started_ms", C.c_double),
+                ("finished_ms", C.c_double), ("error", C.c_char * 128)]
+
+
+class Server:
+    """Reconstruction server (fbp_server_*): continuous batching of independent
+    jobs on one GPU over `slots` contexts. device < 0: host-only scheduler for
+    FBP_JOB_HOST_WAIT jobs. Host arrays passed to submit() must stay alive
+    (and should be pinned) until wait() returns."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 3):
+        self.lib = library()
+        self.handle = C.c_void_p()
+        rc = self.lib.fbp_server_create(C.byref(self.handle), int(device), C.c_size_t(hbm_budget_bytes), int(slots))
+        if rc != 0:
+            raise FBPError(rc, self.lib.fbp_last_error(None).decode())
+        self._keep = {}
+
+    def submit(self, request: Request, keep=None) -> int:
+        t = C.c_longlong()
+        rc = self.lib.fbp_server_submit(self.handle, C.byref(request), C.byref(t))
+        if rc != 0:
+            raise FBPError(rc, "fbp_server_submit failed")
+        self._keep[t.value] = keep  # the arrays behind input / output
+        return t.value
+
+    def wait(self, ticket: int) -> JobResult:
+        r = JobResult()
+        rc = self.lib.fbp_server_wait(self.handle, int(ticket), C.byref(r))
+        self._keep.pop(ticket, None)
+        if rc != 0:
+            raise FBPError(rc, "fbp_server_wait: unknown ticket")
+        return r
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.fbp_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def projection_file_index(path: str) -> int:

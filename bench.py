@@ -55,6 +55,9 @@ def parse_args():
     p.add_argument("--workload", choices=["cone1440", "cone256"], default="cone1440",
                    help="cone1440: the headline 1440x1470x1440 case; cone256: 256^3, 360 views (profiling)")
     p.add_argument("--forms", default="chosen,plain", help="comma list of chosen,plain")
+    p.add_argument("--shard", choices=["replicas", "slabs"], default="replicas",
+                   help="N>1: replicas = one independent volume per rank (weak scaling); slabs = one volume "
+                        "split into y-slabs, each rank holding its detector row band (strong scaling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the CPU-baseline sample")
@@ -65,6 +68,19 @@ def workload(scale: int, name: str = "cone1440") -> dict:
     import phantoms as P
     c = P.config_cone1440() if name == "cone1440" else P.config_cone256()
     return c if scale == 1 else P.scaled_cone(c, scale)
+
+
+def measured_traffic(workload_name: str, form: str):
+    """DRAM bytes (read + write) of one backprojector launch for this workload
+    and form, from the ncu capture recorded in profiles/ (None if absent)."""
+    try:
+        for line in (ROOT / "profiles" / "bp_dram_traffic.txt").read_text().splitlines():
+            f = line.split()
+            if len(f) == 4 and not line.startswith("#") and f[0] == workload_name and f[1] == form:
+                return float(f[2]) + float(f[3])
+    except OSError:
+        pass
+    return None
 
 
 def data_note(c: dict) -> str:
@@ -270,6 +286,13 @@ def main() -> None:
         if dist is not None:
             dist.barrier()
 
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
     def max_over_ranks(x: float) -> float:
         if dist is None:
             return x
@@ -297,6 +320,15 @@ def main() -> None:
             del counts
     stream.synchronize()
 
+    # y-slab sharding: this rank keeps only its detector row band and volume slab
+    slab = (0, c["ny"], 0, c["nv"])
+    if args.shard == "slabs":
+        slab = F.plan_slabs(geom, c["nu"], c["nv"], c["nx"], c["ny"], world)[rank]
+        pristine = pristine[:, slab[2]:slab[3], :].contiguous()
+        torch.cuda.empty_cache()
+    slab_ny = slab[1] - slab[0]
+    job_units = U if args.shard == "slabs" else world * U  # voxel-view updates of the whole job
+
     sod, odd, w, vw, rot = ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"], ga["full_rotation_count"]
 
     def make_solver(form: str):
@@ -304,6 +336,9 @@ def main() -> None:
         s.set_stream(stream)
         s.set_precision(F.Precision.MIXED if form == "chosen" else F.Precision.FP32)
         s.set_clip_after_backprojection(True)
+        if args.shard == "slabs":
+            s.set_detector_rows(slab[2], c["nv"])
+            s.set_volume_slab(slab[0], slab_ny)
         return s
 
     def step(s, src, ev=None):
@@ -357,7 +392,7 @@ def main() -> None:
         s = make_solver(form)
         res[form] = timed(s, pristine)
         res[form]["kernel"] = s.last_backprojection()
-        vols[form] = torch.empty((c["nz"], c["ny"], c["nx"]), dtype=torch.float32, device=dev)
+        vols[form] = torch.empty((c["nz"], slab_ny, c["nx"]), dtype=torch.float32, device=dev)
         s.read_volume(vols[form])
         if form == "chosen":
             smem_bw = s.measure_smem_bandwidth()
@@ -378,45 +413,51 @@ def main() -> None:
     e2e = None
     head = "chosen" if "chosen" in res else forms[0]
     if not args.no_e2e:
-        host_proj = torch.empty((c["nviews"], c["nv"], c["nu"]), dtype=torch.float32, pin_memory=True)
+        host_proj = torch.empty(tuple(pristine.shape), dtype=torch.float32, pin_memory=True)
         host_proj.copy_(pristine)
-        host_vol = torch.empty((c["nz"], c["ny"], c["nx"]), dtype=torch.float32, pin_memory=True)
+        host_vol = torch.empty((c["nz"], slab_ny, c["nx"]), dtype=torch.float32, pin_memory=True)
         s = make_solver(head)
         r = timed(s, host_proj, readback=host_vol)
         s.ctx.close()
         del s
-        e2e = {"value": world * U / (r["ms"] * 1e-3) / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": int(host_proj.numel() * 4), "d2h_bytes_per_step": int(host_vol.numel() * 4),
+        e2e = {"value": job_units / (r["ms"] * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(sum_over_ranks(host_proj.numel() * 4)),
+               "d2h_bytes_per_step": int(sum_over_ranks(host_vol.numel() * 4)),
                "ms_per_step": r["ms"]}
         del host_proj, host_vol
 
     h = res[head]
-    value = world * U / (h["ms"] * 1e-3) / 1e9
+    value = job_units / (h["ms"] * 1e-3) / 1e9
     # roofline of the dominant kernel (the backprojector)
     esize = 2 if head == "chosen" else 4
     bp_s = h["bp_ms"] * 1e-3
-    hbm_bytes = c["nviews"] * c["nv"] * c["nu"] * esize + 4 * c["nx"] * c["ny"] * c["nz"]
+    band_rows = slab[3] - slab[2]
+    local_units = c["nx"] * slab_ny * c["nz"] * c["nviews"]  # this rank's updates
+    hbm_bytes = c["nviews"] * band_rows * c["nu"] * esize + 4 * c["nx"] * slab_ny * c["nz"]
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except (OSError, ValueError):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    gather_bytes = 4 * esize * U  # four bilinear taps per update
+    gather_bytes = 4 * esize * local_units  # four bilinear taps per update
+    traffic = measured_traffic(c["name"], head) if slab == (0, c["ny"], 0, c["nv"]) else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True,
+        "scaling": "strong" if args.shard == "slabs" else "weak",
         "vs_baseline": None, "dtype": "f32", "storage_dtype": "f16 filtered views" if head == "chosen" else "f32",
         "data": data_note(c),
         "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "voxel_mm": c["vox"],
                    "views": c["nviews"], "detector": [c["nu"], c["nv"]], "pitch_mm": c["du"],
                    "sod_mm": c["sod"], "sdd_mm": c["sdd"], "filter": FILTER_NAMES[c["filter"]], "form": head,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "parallelism": (f"y-slabs x{world}" if args.shard == "slabs" else f"replicas x{world}")
+                   if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (projections %.1f GB)" % (c["nviews"] * c["nv"] * c["nu"] * 4 / 1e9),
                    "step": "D2D restore of raw projections + weights + filter + backprojection + clip"},
         "stages_ms": {"filter": h["filter_ms"], "backprojection": h["bp_ms"]},
         "roofline": {"bound": "hbm", "achieved": hbm_bytes / bp_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": hbm_bytes / bp_s / 1e9 / hbm_peak, "traffic": None,
+                     "frac": hbm_bytes / bp_s / 1e9 / hbm_peak, "traffic": traffic,
                      "note": "backprojector algorithmic HBM bytes (filtered views read once + volume written "
                              "once); the kernel is bound by shared-memory gathers, see roofline_smem"},
         "roofline_smem": {"bound": "smem", "achieved": gather_bytes / bp_s / 1e12,
@@ -428,7 +469,7 @@ def main() -> None:
         "accuracy": accuracy,
     }
     for form, r in res.items():
-        line[f"form_{form}"] = {"value": world * U / (r["ms"] * 1e-3) / 1e9, "ms_per_step": r["ms"],
+        line[f"form_{form}"] = {"value": job_units / (r["ms"] * 1e-3) / 1e9, "ms_per_step": r["ms"],
                                 "filter_ms": r["filter_ms"], "backprojection_ms": r["bp_ms"],
                                 "gpu_launches": r["launches"], "clocks": r["clocks"], "backprojector": r["kernel"]}
     if "chosen" in res and "plain" in res:

@@ -189,6 +189,41 @@ int fbp_plan_slabs(const fbp_geometry* geometry, int detector_cols, int detector
 int fbp_set_detector_rows(fbp_context* ctx, int row_offset, int total_rows);
 int fbp_set_volume_slab(fbp_context* ctx, int y_offset, int y_count);
 
+/* ---- reconstruction server (no counterpart in the reference) --------------------------
+ * Continuous batching of independent jobs on one GPU: `slots` worker threads, each with its
+ * own context and CUDA stream; queued jobs start in arrival order as a slot and HBM budget
+ * (hbm_budget_bytes, 0 = 80 % of the free memory) free up, looking up to 8 jobs past a head
+ * that does not fit; a job larger than the budget runs alone. Jobs admitted together overlap
+ * on the device, and each result equals the same job run alone. Slots keep their buffers
+ * (grow only). Host buffers should be pinned so that copies overlap other jobs' kernels. */
+#define FBP_JOB_CONE 0        /* FDK: input [views][det_rows][det_cols], output [vol_h][vol_v][vol_h] */
+#define FBP_JOB_FAN2D 1       /* flat-detector fan FBP: input [views][det_cols], output [vol_h][vol_h] */
+#define FBP_JOB_PARALLEL2D 2  /* parallel-beam FBP, same shapes as FAN2D */
+#define FBP_JOB_HOST_WAIT 3   /* holds a slot and reserve_bytes for `views` microseconds (scheduler tests) */
+typedef struct fbp_request {
+  int kind;                /* FBP_JOB_* */
+  int precision;           /* FBP_PRECISION_* */
+  int filter_type;         /* FBP_FILTER_* */
+  int clip;                /* cone: clip negatives after backprojection (the reference's default: 1) */
+  fbp_geometry geometry;   /* cone: reference-API distances; 2D: detector_width, volume_width, turns */
+  int det_cols, det_rows, views;
+  int vol_h, vol_v;
+  long long reserve_bytes; /* HBM working set to reserve; 0 = estimate from the sizes */
+  const float* input;      /* host */
+  float* output;           /* host */
+} fbp_request;
+typedef struct fbp_job_result {
+  int status;                                      /* FBP_OK or the job's error code */
+  double queued_ms, started_ms, finished_ms;       /* since the server was created */
+  char error[128];
+} fbp_job_result;
+typedef struct fbp_server fbp_server;
+int fbp_server_create(fbp_server** server, int device, size_t hbm_budget_bytes, int slots);
+/* device < 0: no GPU, only FBP_JOB_HOST_WAIT jobs (tests of the scheduler). */
+int fbp_server_submit(fbp_server* server, const fbp_request* request, long long* ticket);
+int fbp_server_wait(fbp_server* server, long long ticket, fbp_job_result* result);
+int fbp_server_destroy(fbp_server* server); /* runs the queued jobs, then stops */
+
 /* ---- file I/O (FBP3D.cpp:74-195) -------------------------------------------------------
  * FBP3D::read_projections / read_projections_as_sinograms (FBP3D.cpp:74-176): allocate the
  * stack (target_width x target_height x projection_count) and fill it from the files of

@@ -603,3 +603,78 @@ def test_slab_clip_keeps_the_reference_extent(fbp, oracle):
         sharding.reconstruct_slab(r, proj, g, c["nx"], c["ny"], 2, slab)
         parts.append(r.read_volume())
     assert relative_rmse(np.concatenate(parts, axis=1), ref) < TOL_FP32
+
+
+# ------------------------------------------------------- reconstruction server
+def _server_jobs(fbp, rng):
+    """Mixed jobs (cone FDK of several sizes and both forms, 2D fan and
+    parallel) with seeded inputs; returns (requests, inputs, outputs)."""
+    reqs, keep, outs = [], [], []
+    for h, v, k, prec in [(64, 64, 96, "FP32"), (96, 96, 128, "MIXED"), (64, 40, 64, "MIXED"), (32, 32, 48, "FP32")]:
+        det = h * 3 // 2
+        proj = rng.random((k, det, det), dtype=np.float32)
+        out = np.empty((h, v, h), np.float32)
+        r = fbp.Request()
+        r.kind, r.precision, r.filter_type, r.clip = fbp.JobKind.CONE, getattr(fbp.Precision, prec), 0, 1
+        r.geometry = fbp.Geometry.cone(3.0 * h, 1.5 * h, float(det), float(h), 1.0, 0.0)
+        r.det_cols, r.det_rows, r.views, r.vol_h, r.vol_v = det, det, k, h, v
+        r.input, r.output = proj.ctypes.data, out.ctypes.data
+        reqs.append(r), keep.append(proj), outs.append(out)
+    for kind, h, k, bins in [("FAN2D", 128, 180, 192), ("PARALLEL2D", 96, 120, 136)]:
+        sino = rng.random((k, bins), dtype=np.float32)
+        out = np.empty((h, h), np.float32)
+        r = fbp.Request()
+        r.kind, r.precision, r.filter_type = getattr(fbp.JobKind, kind), fbp.Precision.FP32, 1
+        r.geometry = (fbp.Geometry.cone(2.0 * h, 2.0 * h, float(bins), float(h), 1.0, 0.0) if kind == "FAN2D"
+                      else fbp.Geometry.parallel(float(bins), float(h), 0.5, 0.0))
+        r.det_cols, r.det_rows, r.views, r.vol_h, r.vol_v = bins, 1, k, h, 1
+        r.input, r.output = sino.ctypes.data, out.ctypes.data
+        reqs.append(r), keep.append(sino), outs.append(out)
+    return reqs, keep, outs
+
+
+def test_server_results_alone_equal_results_in_the_mix(fbp):
+    """Every job's output is the same run alone (one slot, one job at a time)
+    and admitted together with the others (three slots, overlapping)."""
+    rng = np.random.default_rng(61)
+    reqs, keep, alone = _server_jobs(fbp, rng)
+    s = fbp.Server(0, 0, 1)
+    for r in reqs:
+        res = s.wait(s.submit(r))
+        assert res.status == 0, res.error
+    s.close()
+    mix = [np.empty_like(o) for o in alone]
+    for r, o in zip(reqs, mix):
+        r.output = o.ctypes.data
+    s = fbp.Server(0, 0, 3)
+    tickets = [s.submit(r) for r in reqs * 1]
+    res = [s.wait(t) for t in tickets]
+    s.close()
+    assert all(r.status == 0 for r in res), [r.error for r in res]
+    starts = sorted(r.started_ms for r in res)
+    assert starts[2] < min(r.finished_ms for r in res)  # three jobs were on the device together
+    for a, m in zip(alone, mix):
+        np.testing.assert_array_equal(a, m)
+
+
+def test_server_cone_job_matches_oracle_and_bad_jobs_fail_alone(fbp, oracle, phantoms):
+    c, proj = _cone_case(phantoms, oracle, 4)
+    sod, odd, w, vw, rot = _cone_args(c)
+    out = np.empty((c["nz"], c["ny"], c["nx"]), np.float32)
+    r = fbp.Request()
+    r.kind, r.precision, r.filter_type, r.clip = fbp.JobKind.CONE, fbp.Precision.FP32, 0, 0
+    r.geometry = fbp.Geometry.cone(sod, odd, w, vw, rot, c["offset"])
+    r.det_cols, r.det_rows, r.views, r.vol_h, r.vol_v = c["nu"], c["nv"], c["nviews"], c["nx"], c["ny"]
+    r.input, r.output = proj.ctypes.data, out.ctypes.data
+    bad = fbp.Request()
+    bad.kind = fbp.JobKind.CONE
+    bad.geometry = fbp.Geometry.cone(sod, odd, w, vw, rot, 0.0)
+    bad.det_cols, bad.det_rows, bad.views, bad.vol_h, bad.vol_v = 0, c["nv"], c["nviews"], c["nx"], c["ny"]
+    bad.input, bad.output = proj.ctypes.data, out.ctypes.data
+    s = fbp.Server(0, 0, 2)
+    tb, tg = s.submit(bad), s.submit(r)
+    rb, rg = s.wait(tb), s.wait(tg)
+    s.close()
+    assert rb.status != 0 and rb.error
+    assert rg.status == 0, rg.error
+    assert relative_rmse(out, oracle.fdk(proj, c, 0)) < TOL_FP32
