@@ -45,7 +45,8 @@
 namespace fbp {
 namespace {
 
-constexpr int kMaxStages = 8;           // shared-memory ring stages (one view each)
+constexpr int kMaxStages = 8;                // shared-memory ring stages (one view each)
+constexpr int kMaxDynamicSmem = 227 * 1024;  // sm_100: largest dynamic shared memory of one CTA
 constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
 
 struct ViewCoef {
@@ -1007,7 +1008,11 @@ __global__ void rebin_fan_kernel(const float* fan, int bins, int views, double s
 template <int LAYOUT, int TX, int TZ, int NY>
 cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
   auto kern = kahan ? bp_kernel<LAYOUT, TX, TZ, NY, true> : bp_kernel<LAYOUT, TX, TZ, NY, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // The attribute is process-wide: contexts on other threads launch this kernel
+  // with other sizes, so it is always raised to the device maximum (a launch
+  // still uses only its own dynamic size).
+  (void)smem;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
@@ -1019,7 +1024,7 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
 template <int LAYOUT>
 cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
   auto kern = kahan ? bp_quad_kernel<LAYOUT, 8, true> : bp_quad_kernel<LAYOUT, 8, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   // all of L1 as shared memory, so that two CTAs of up to 113 KB share an SM
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);

@@ -386,7 +386,7 @@ int ensure_filter_tables(fbp_context* ctx, int n, int filter) {
     return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "filter length must be a power of two in [2, 8192]");
   if (filter < 0 || filter > FBP_FILTER_RAMP_SAMPLED)
     return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown filter type");
-  if (t.n != n) {
+  if (n > t.cap) {  // grow only: a context serving many row lengths stops allocating
     cudaFree(t.twiddle);
     cudaFree(t.hbr);
     cudaFree(t.kernel);
@@ -394,10 +394,12 @@ int ensure_filter_tables(fbp_context* ctx, int n, int filter) {
     t.hbr = nullptr;
     t.kernel = nullptr;
     t.n = 0;
+    t.cap = 0;
     if (cuda_check(ctx, cudaMalloc(&t.twiddle, sizeof(float2) * (n / 2 + 1)), "cudaMalloc(twiddle)") ||
         cuda_check(ctx, cudaMalloc(&t.hbr, sizeof(float) * n), "cudaMalloc(hbr)") ||
         cuda_check(ctx, cudaMalloc(&t.kernel, sizeof(float) * n), "cudaMalloc(kernel)"))
       return FBP_ERR_OUT_OF_MEMORY;
+    t.cap = n;
   }
   double* H = static_cast<double*>(scratch(ctx, sizeof(double) * n));
   if (!H) return FBP_ERR_OUT_OF_MEMORY;

@@ -78,6 +78,7 @@ struct Stack {
 
 struct FilterTables {
   int n = 0, filter = -1;
+  int cap = 0;                // entries allocated (grow only: no cudaFree between jobs)
   float2* twiddle = nullptr;  // n/2 entries exp(-2 pi i k / n)
   float* hbr = nullptr;       // n entries H[bitrev(k)] / n
   float* kernel = nullptr;    // n entries: spatial kernel g = IDFT(H) (circular)
@@ -88,6 +89,7 @@ struct FilterTables {
 struct ToeplitzTables {
   int m = 0, n = 0, filter = -1;
   void* th = nullptr;  // 2 * m * kp BF16 values
+  size_t cap = 0;      // bytes allocated at th (grow only)
 };
 
 }  // namespace fbp

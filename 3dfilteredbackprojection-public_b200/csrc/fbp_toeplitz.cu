@@ -274,11 +274,15 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   const int kp = (m + BK - 1) / BK * BK;  // K padded to whole 64-blocks (16-byte pitch too)
   ToeplitzTables& t = ctx->ttab;
   if (!(t.m == m && t.n == n && t.filter == filter)) {
-    cudaFree(t.th);
-    t.th = nullptr;
     t.m = 0;
     const size_t bytes = sizeof(__nv_bfloat16) * (size_t)m * kp;
-    if (cuda_check(ctx, cudaMalloc(&t.th, 2 * bytes), "cudaMalloc(Toeplitz operands)")) return FBP_ERR_OUT_OF_MEMORY;
+    if (2 * bytes > t.cap) {  // grow only
+      cudaFree(t.th);
+      t.th = nullptr;
+      t.cap = 0;
+      if (cuda_check(ctx, cudaMalloc(&t.th, 2 * bytes), "cudaMalloc(Toeplitz operands)")) return FBP_ERR_OUT_OF_MEMORY;
+      t.cap = 2 * bytes;
+    }
     if (int rc = ensure_filter_tables(ctx, n, filter)) return rc;
     build_toeplitz_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, kp, (__nv_bfloat16*)t.th,
                                                                      (__nv_bfloat16*)t.th + (size_t)m * kp);

@@ -52,8 +52,13 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--scale", type=int, default=1,
                    help="divide volume, detector and views by this factor (profiling runs); 1 = full workload")
-    p.add_argument("--workload", choices=["cone1440", "cone256"], default="cone1440",
-                   help="cone1440: the headline 1440x1470x1440 case; cone256: 256^3, 360 views (profiling)")
+    p.add_argument("--workload", choices=["cone1440", "cone256", "serving"], default="cone1440",
+                   help="cone1440: the headline 1440x1470x1440 case; cone256: 256^3, 360 views (profiling); "
+                        "serving: the mixed request stream (reconstructions/s, p50/p99 latency)")
+    p.add_argument("--requests", type=int, default=2000, help="serving: requests in the stream")
+    p.add_argument("--slots", type=int, default=5, help="serving: concurrent jobs of the chosen form")
+    p.add_argument("--load", type=float, default=0.7,
+                   help="serving: Poisson arrival rate as a fraction of the plain one-at-a-time capacity")
     p.add_argument("--forms", default="chosen,plain", help="comma list of chosen,plain")
     p.add_argument("--shard", choices=["replicas", "slabs"], default="replicas",
                    help="N>1: replicas = one independent volume per rank (weak scaling); slabs = one volume "
@@ -249,6 +254,144 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ our arm
+def serving_requests(n: int, seed: int = 1004) -> list[dict]:
+    """The mixed stream: 40 % 2D fan (512^2 or 1024^2 images, 720-1440 views,
+    768-1536 bins), 40 % cone FDK (edge in {128, 192, 256, 384, 512}, 360-720
+    views, detector 1.5 x edge), 20 % cone 768^3 with 1024 views. View and
+    bin counts are drawn on a grid (multiples of 120 views, 256 bins) so that
+    the inputs come from a pool of distinct shapes."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        u = rng.random()
+        if u < 0.4:
+            out.append(dict(kind="fan", n=int(rng.choice([512, 1024])), views=int(rng.choice([720, 960, 1200, 1440])),
+                            bins=int(rng.choice([768, 1024, 1280, 1536]))))
+        elif u < 0.8:
+            e = int(rng.choice([128, 192, 256, 384, 512]))
+            out.append(dict(kind="cone", n=e, views=int(rng.choice([360, 480, 600, 720])), det=e * 3 // 2))
+        else:
+            out.append(dict(kind="cone", n=768, views=1024, det=1152))
+    return out
+
+
+def serving_main(args) -> None:
+    """Serving on one GPU: the stream's capacity (reconstructions/s, every
+    request submitted at once) for the plain form run one job at a time (FP32,
+    one slot) and for the chosen form under continuous batching (MIXED,
+    `--slots` slots), then p50/p99 latency of both under seeded Poisson
+    arrivals at `--load` x the plain capacity. Inputs: seeded random
+    ellipsoids projected analytically on the GPU (fan jobs: the central
+    detector row), held in pinned host memory as the requests arrive."""
+    import numpy as np
+    import torch
+
+    import build as B
+    B.build()
+    import fbp_b200 as F
+    import phantoms as P
+
+    torch.cuda.set_device(0)
+    reqs = serving_requests(args.requests)
+
+    def shape_key(r):
+        return (r["kind"], r["n"], r["views"], r.get("det", r.get("bins")))
+
+    def geometry(r):
+        if r["kind"] == "cone":  # 1 mm voxels, magnification 1.5, detector 1.5 x the volume's shadow
+            e = r["n"]
+            return F.Geometry.cone(3.0 * e, 1.5 * e, 1.5 * r["det"], float(e), 1.0, 0.0)
+        # fan: SOD 500, SDD 1000, 256 mm field of view, 768 mm detector
+        return F.Geometry.cone(500.0, 500.0, 768.0, 256.0, 1.0, 0.0)
+
+    # ---- input pool (pinned host), one seeded phantom per distinct shape
+    pool, outs = {}, {}
+    gen = F.FBP3D(0)
+    for i, key in enumerate(sorted({shape_key(r) for r in reqs})):
+        kind, n, views, cols = key
+        rows = cols if kind == "cone" else 1
+        g = geometry(dict(kind=kind, n=n, views=views, det=cols, bins=cols))
+        radius = 0.5 * g.volume_width
+        E = P.random_ellipsoids(np.random.default_rng(2000 + i), 20, radius)
+        gen.generate_blank_projections(cols, rows, views)
+        gen.project_ellipsoids(E, g)
+        host = torch.empty((views, rows, cols), dtype=torch.float32, pin_memory=True)
+        gen.download_projections(host)
+        pool[key] = host
+        vol_shape = (n, n, n) if kind == "cone" else (n, n)
+        outs[key] = [torch.empty(vol_shape, dtype=torch.float32, pin_memory=True) for _ in range(args.slots + 1)]
+    gen.ctx.close()
+    del gen
+
+    def request_struct(r, precision, out):
+        key = shape_key(r)
+        q = F.Request()
+        q.kind = F.JobKind.CONE if r["kind"] == "cone" else F.JobKind.FAN2D
+        q.precision = precision
+        q.filter_type = 0 if r["kind"] == "cone" else 1
+        q.clip = 1
+        q.geometry = geometry(r)
+        inp = pool[key]
+        q.views, q.det_rows, q.det_cols = inp.shape
+        q.vol_h = r["n"]
+        q.vol_v = r["n"] if r["kind"] == "cone" else 1
+        q.input, q.output = inp.data_ptr(), out.data_ptr()
+        return q
+
+    def run(precision, slots, arrivals=None):
+        srv = F.Server(0, 0, slots)
+        # warm every slot's buffers with the largest jobs (buffers only grow)
+        big = max(reqs, key=lambda r: r["n"] ** 3 * r["views"] if r["kind"] == "cone" else 0)
+        big2 = max(reqs, key=lambda r: r["n"] ** 2 * r["views"] if r["kind"] == "fan" else 0)
+        warm = [srv.submit(request_struct(w, precision, outs[shape_key(w)][0])) for w in [big] * slots + [big2] * slots]
+        for t in warm:
+            assert srv.wait(t).status == 0
+        rr = {k: 0 for k in outs}
+        tickets = []
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            if arrivals is not None:
+                delay = arrivals[i] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            key = shape_key(r)
+            out = outs[key][rr[key] % len(outs[key])]
+            rr[key] += 1
+            tickets.append(srv.submit(request_struct(r, precision, out)))
+        res = [srv.wait(t) for t in tickets]
+        srv.close()
+        bad = [x.error.decode() for x in res if x.status != 0]
+        assert not bad, bad[:3]
+        lat = np.array([x.finished_ms - x.queued_ms for x in res])
+        span = (max(x.finished_ms for x in res) - min(x.queued_ms for x in res)) * 1e-3
+        return dict(recon_per_s=len(res) / span, p50_ms=float(np.percentile(lat, 50)),
+                    p99_ms=float(np.percentile(lat, 99)), makespan_s=span)
+
+    plain_cap = run(F.Precision.FP32, 1)
+    chosen_cap = run(F.Precision.MIXED, args.slots)
+    rate = args.load * plain_cap["recon_per_s"]
+    arrivals = np.cumsum(np.random.default_rng(1005).exponential(1.0 / rate, size=len(reqs)))
+    plain_lat = run(F.Precision.FP32, 1, arrivals)
+    chosen_lat = run(F.Precision.MIXED, args.slots, arrivals)
+    mix = {"fan2d": sum(r["kind"] == "fan" for r in reqs), "cone_128_512": sum(r["kind"] == "cone" and r["n"] < 768
+                                                                               for r in reqs),
+           "cone_768": sum(r["kind"] == "cone" and r["n"] == 768 for r in reqs)}
+    line = {
+        "metric": "mixed-stream reconstructions/s", "value": chosen_cap["recon_per_s"], "unit": "recon/s",
+        "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 accumulation, f16 filtered views (chosen)", "data": "synthetic: seeded random ellipsoids, "
+        "analytic projections (GPU), pinned host inputs",
+        "config": {"workload": "serving_mixed_stream", "requests": len(reqs), "mix": mix, "slots": args.slots,
+                   "arrival_rate_per_s": rate, "load_vs_plain_capacity": args.load},
+        "chosen": {"capacity": chosen_cap, "poisson": chosen_lat},
+        "plain_one_at_a_time_fp32": {"capacity": plain_cap, "poisson": plain_lat},
+        "chosen_over_plain_recon_per_s": chosen_cap["recon_per_s"] / plain_cap["recon_per_s"],
+        "p99_ms": chosen_lat["p99_ms"], "p50_ms": chosen_lat["p50_ms"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -256,6 +399,9 @@ def main() -> None:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.workload == "serving":
+        serving_main(args)
         return
 
     import numpy as np
