@@ -858,6 +858,63 @@ int fbp_clip_negatives_of_volume(fbp_context* ctx) {
   return fbp::launch_clip(ctx, ctx->vol, ctx->vx, ctx->vy, ctx->vz, ctx->vz);
 }
 
+// ------------------------------------------------ forward projection (f3)
+// The reference sizes the detector like the volume: volume x columns, volume
+// y rows (FBP3D.cpp:219, 274); parallel beam measures in voxels (detector
+// width = volume width = x size, FBP3D.cpp:230-231).
+static int forward(fbp_context* ctx, Stack& s, bool cone, float sod, float odd, float det_w, float vol_w, float rot,
+                   int count, float offset) {
+  if (!ctx->vol) return fbp::set_error(ctx, FBP_ERR_STATE, "project_forward but the volume is not allocated");
+  if (count <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "projection count must be positive");
+  if (cone && (!(sod > 0.f) || !(odd >= 0.f) || !(det_w > 0.f) || !(vol_w > 0.f)))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "distances and widths must be positive");
+  const int nu = ctx->vx, nv = ctx->vy;
+  FBP_TRY(alloc_stack(ctx, s, nu, nv, count, false));  // generate_blank_*: every sample is written
+  const double vox = cone ? (double)vol_w / ctx->vx : 1.0;
+  const double du = cone ? (double)det_w / nu : 1.0;
+  return fbp::launch_forward(ctx, ctx->vol, ctx->vx, ctx->vy, ctx->vz, vox, cone, sod, (double)sod + odd, du, du,
+                             2.0 * kPi * (double)rot, offset, nu, nv, count, s.f32, s.pitch, s.sinogram);
+}
+
+int fbp_project_forward_cone_to_projections(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,
+                                            float rot, int count, float offset) {
+  FBP_CTX(ctx);
+  return forward(ctx, ctx->proj, true, sod, odd, det_w, vol_w, rot, count, offset);
+}
+
+int fbp_project_forward_cone_to_sinograms(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,
+                                          float rot, int count, float offset) {
+  FBP_CTX(ctx);
+  return forward(ctx, ctx->sino, true, sod, odd, det_w, vol_w, rot, count, offset);
+}
+
+int fbp_project_forward_parallel_to_projections(fbp_context* ctx, float rot, int count, float offset) {
+  FBP_CTX(ctx);
+  return forward(ctx, ctx->proj, false, 0.f, 0.f, 0.f, 0.f, rot, count, offset);
+}
+
+int fbp_project_forward_parallel_to_sinograms(fbp_context* ctx, float rot, int count, float offset) {
+  FBP_CTX(ctx);
+  return forward(ctx, ctx->sino, false, 0.f, 0.f, 0.f, 0.f, rot, count, offset);
+}
+
+int fbp2d_project_forward(fbp_context* ctx, const float* image, int nx, int nz, float* sinogram, int bins, int views,
+                          const fbp_geometry* g) {
+  FBP_CTX(ctx);
+  if (!image || !sinogram || !g || nx <= 0 || nz <= 0 || bins <= 0 || views <= 0)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "bad 2D forward projection arguments");
+  if (!(g->detector_width > 0.f) || !(g->volume_width > 0.f))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
+  const bool cone = g->kind == FBP_GEOMETRY_CONE;
+  if (cone && !(g->source_distance > 0.f))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "source distance must be positive");
+  const double vox = (double)g->volume_width / nx, du = (double)g->detector_width / bins;
+  return fbp::launch_forward(ctx, image, nx, 1, nz, vox, cone, g->source_distance,
+                             (double)g->source_distance + g->detector_distance, du, du,
+                             2.0 * kPi * (double)g->full_rotation_count, g->rotation_offset_radian, bins, 1, views,
+                             sinogram, bins, false);
+}
+
 // ---------------------------------------------------------- sharding (e)
 int fbp_set_detector_rows(fbp_context* ctx, int row_offset, int total_rows) {
   FBP_CTX(ctx);

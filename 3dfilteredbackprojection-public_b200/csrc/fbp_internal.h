@@ -242,6 +242,11 @@ int launch_volume_minmax(fbp_context* ctx, const float* vol, long long n, int* m
 // Rescale in place with the range from the device pair mm, or (mm == nullptr) from mn, mx.
 int launch_normalize(fbp_context* ctx, float* vol, long long n, const int* mm, float mn, float mx);
 
+// ---- forward projection (fbp_forward.cu) ----
+int launch_forward(fbp_context* ctx, const float* vol, int nx, int ny, int nz, double vox, bool cone, double sod,
+                   double sdd, double du, double dv, double span, double offset, int nu, int nv, int nviews,
+                   float* out, long long pitch, bool sinogram);
+
 // ---- file ingest / slice output (fbp_io.cu) ----
 int projection_file_index(const std::string& path);  // -1 when the name carries no index
 int read_projection_files(fbp_context* ctx, const char* directory, int fw, int fh, int channels, int bpc, int tw,

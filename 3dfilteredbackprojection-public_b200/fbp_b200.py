@@ -149,6 +149,11 @@ SIGNATURES = {
     "fbp_write_volume": [_P, C.c_char_p],
     "fbp_projection_file_index": [C.c_char_p],
     "fbp_plan_slabs": [C.POINTER(Geometry), _I, _I, _I, _I, _I, C.POINTER(C.c_int)],
+    "fbp_project_forward_cone_to_projections": [_P, _F, _F, _F, _F, _F, _I, _F],
+    "fbp_project_forward_cone_to_sinograms": [_P, _F, _F, _F, _F, _F, _I, _F],
+    "fbp_project_forward_parallel_to_projections": [_P, _F, _I, _F],
+    "fbp_project_forward_parallel_to_sinograms": [_P, _F, _I, _F],
+    "fbp2d_project_forward": [_P, _P, _I, _I, _P, _I, _I, C.POINTER(Geometry)],
     "fbp_server_create": [C.POINTER(C.c_void_p), _I, C.c_size_t, _I],
     "fbp_server_submit": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
     "fbp_server_wait": [C.c_void_p, C.c_longlong, C.c_void_p],
@@ -360,6 +365,31 @@ class FBP3D:
         names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16"}
         return {"kernel": "symmetric" if v.value == Backprojector.SYMMETRIC else "generic",
                 "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value)}
+
+    # -- forward projection (FBP3D.cpp:212-330)
+    def project_forward_cone_to_projections(self, xray_source_distance, detector_panel_distance, detector_width,
+                                            volume_width, full_rotation_count, projection_count,
+                                            rotation_offset_radian=0.0) -> None:
+        self.ctx.call("fbp_project_forward_cone_to_projections", xray_source_distance, detector_panel_distance,
+                      detector_width, volume_width, full_rotation_count, int(projection_count),
+                      rotation_offset_radian)
+
+    def project_forward_cone_to_sinogram(self, xray_source_distance, detector_panel_distance, detector_width,
+                                         volume_width, full_rotation_count, projection_count,
+                                         rotation_offset_radian=0.0) -> None:
+        self.ctx.call("fbp_project_forward_cone_to_sinograms", xray_source_distance, detector_panel_distance,
+                      detector_width, volume_width, full_rotation_count, int(projection_count),
+                      rotation_offset_radian)
+
+    def project_forward_parallel_to_projections(self, full_rotation_count, projection_count,
+                                                rotation_offset_radian=0.0) -> None:
+        self.ctx.call("fbp_project_forward_parallel_to_projections", full_rotation_count, int(projection_count),
+                      rotation_offset_radian)
+
+    def project_forward_parallel_to_sinogram(self, full_rotation_count, projection_count,
+                                             rotation_offset_radian=0.0) -> None:
+        self.ctx.call("fbp_project_forward_parallel_to_sinograms", full_rotation_count, int(projection_count),
+                      rotation_offset_radian)
 
     def set_detector_rows(self, row_offset: int, total_rows: int) -> None:
         """The stacks hold rows [row_offset, row_offset + v) of a total_rows-row detector (0, 0: whole)."""
@@ -632,6 +662,17 @@ class FBP2D:
         self.ctx.call("fbp2d_project_backward", C.c_void_p(d.data_ptr()), bins, views, C.byref(geometry),
                       C.c_void_p(img.data_ptr()), nx, nz)
         return self._ret(img, copied)
+
+    def project_forward(self, image, geometry: Geometry, bins: int, views: int, out=None):
+        """FBP2D::project_forward (FBP2D.cpp:54-94): ray-driven sinogram [views][bins]
+        of image [rows][cols] (parallel beam, or flat-detector fan for a cone geometry)."""
+        d, copied = self._dev(image)
+        nz, nx = d.shape
+        sino = out if out is not None else self.torch.empty((views, bins), dtype=self.torch.float32,
+                                                            device=self.device)
+        self.ctx.call("fbp2d_project_forward", C.c_void_p(d.data_ptr()), nx, nz, C.c_void_p(sino.data_ptr()), bins,
+                      views, C.byref(geometry))
+        return self._ret(sino, copied)
 
     def parallelize_fan_beam_sinogram(self, source_sinogram, geometry: Geometry, out_bins: int,
                                       out_detector_width: float):

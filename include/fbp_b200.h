@@ -173,6 +173,30 @@ int fbp_apply_fdk_weights_to_sinograms(fbp_context* ctx, float xray_source_dista
 int fbp_apply_filter_to_projections(fbp_context* ctx, int filter_type);                               /* :389-414 */
 int fbp_apply_filter_to_sinograms(fbp_context* ctx, int filter_type);                                 /* :417-442 */
 int fbp_clip_negatives_of_volume(fbp_context* ctx);                                                    /* :444-458 */
+/* ---- forward projection (FBP3D.cpp:212-330, FBP2D.cpp:54-94) -----------------------------
+ * Ray-driven: each detector pixel's ray (backprojector conventions) is clipped to the volume
+ * box and cut into n = ceil(length / (voxel / 2)) equal steps; the trilinearly interpolated
+ * volume (zero outside) is summed at the step midpoints times the step. As in the reference
+ * the detector is sized like the volume (x columns, y rows) and the stack is (re)allocated;
+ * parallel beam measures in voxels (detector width = volume width). */
+int fbp_project_forward_cone_to_projections(fbp_context* ctx, float xray_source_distance,
+                                            float detector_panel_distance, float detector_width, float volume_width,
+                                            float full_rotation_count, int projection_count,
+                                            float rotation_offset_radian);                  /* FBP3D.cpp:266-297 */
+int fbp_project_forward_cone_to_sinograms(fbp_context* ctx, float xray_source_distance,
+                                          float detector_panel_distance, float detector_width, float volume_width,
+                                          float full_rotation_count, int projection_count,
+                                          float rotation_offset_radian);                    /* FBP3D.cpp:299-330 */
+int fbp_project_forward_parallel_to_projections(fbp_context* ctx, float full_rotation_count, int projection_count,
+                                                float rotation_offset_radian);              /* FBP3D.cpp:212-238 */
+int fbp_project_forward_parallel_to_sinograms(fbp_context* ctx, float full_rotation_count, int projection_count,
+                                              float rotation_offset_radian);                /* FBP3D.cpp:240-264 */
+/* FBP2D::project_forward (FBP2D.cpp:54-94) on caller device buffers: image [nz][nx] pixels
+ * of volume_width/nx, sinogram [views][bins]; parallel beam, or flat-detector fan beam for
+ * FBP_GEOMETRY_CONE. */
+int fbp2d_project_forward(fbp_context* ctx, const float* image, int nx, int nz, float* sinogram, int bins, int views,
+                          const fbp_geometry* geometry);
+
 /* ---- sharding (no counterpart in the reference, which runs on one GL context) ----------
  * One volume over several GPUs without a collective on the data path: y-slab k of the
  * volume needs only the detector rows its voxels project to. fbp_plan_slabs splits

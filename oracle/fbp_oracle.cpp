@@ -707,3 +707,79 @@ extern "C" int orc_bp_cone_f32(const float* q, const int* views, int nsel, int n
   }
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Forward projection (ray-driven), FBP3D::project_forward_cone_to_projections /
+// project_forward_parallel_to_projections (Source/FilteredBackProjection/
+// FBP3D.cpp:212-330) and FBP2D::project_forward (FBP2D.cpp:54-94). The
+// reference's shaders are absent; the library defines the transform as: in
+// the backprojector's conventions, the ray of detector pixel (iu, iv) at view
+// k (cone: from the source -SOD d through the pixel centre on the flat
+// detector at (SDD - SOD) d + u e_u + v y; parallel: along d through
+// u e_u + v y) is clipped to the volume box; its length L is cut into
+// n = ceil(L / (vox / 2)) equal steps; the volume, trilinearly interpolated
+// between voxel centres (zero outside), is summed at the step midpoints and
+// times the step. Restated here in FP64 with the same n.
+extern "C" int orc_forward_project(const double* vol, int nx, int ny, int nz, double vox, int cone, double sod,
+                                   double sdd, double du, double dv, int nu, int nv, int nviews, double span,
+                                   double offset, double* out /* [view][v][u] */) {
+  const double hx = 0.5 * nx * vox, hy = 0.5 * ny * vox, hz = 0.5 * nz * vox;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+  for (int k = 0; k < nviews; ++k)
+    for (int iv = 0; iv < nv; ++iv) {
+      const double th = offset + span * k / nviews, c = std::cos(th), s = std::sin(th);
+      for (int iu = 0; iu < nu; ++iu) {
+        const double u = (iu + 0.5 - 0.5 * nu) * du, v = (iv + 0.5 - 0.5 * nv) * dv;
+        double S[3], D[3];
+        if (cone) {
+          S[0] = -sod * c; S[1] = 0.0; S[2] = -sod * s;
+          const double P[3] = {(sdd - sod) * c - u * s, v, (sdd - sod) * s + u * c};
+          for (int a = 0; a < 3; ++a) D[a] = P[a] - S[a];
+        } else {
+          const double R = 2.0 * (hx + hy + hz);  // start well outside the box
+          S[0] = -R * c - u * s; S[1] = v; S[2] = -R * s + u * c;
+          D[0] = c; D[1] = 0.0; D[2] = s;
+        }
+        const double len = std::sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
+        for (int a = 0; a < 3; ++a) D[a] /= len;
+        double t0 = -1e300, t1 = 1e300;
+        const double h[3] = {hx, hy, hz};
+        bool miss = false;
+        for (int a = 0; a < 3; ++a) {
+          if (std::fabs(D[a]) < 1e-300) {
+            if (S[a] <= -h[a] || S[a] >= h[a]) miss = true;
+            continue;
+          }
+          double ta = (-h[a] - S[a]) / D[a], tb = (h[a] - S[a]) / D[a];
+          if (ta > tb) std::swap(ta, tb);
+          t0 = std::max(t0, ta);
+          t1 = std::min(t1, tb);
+        }
+        double acc = 0.0;
+        if (!miss && t1 > t0) {
+          const long n = (long)std::ceil((t1 - t0) / (0.5 * vox));
+          const double step = (t1 - t0) / n;
+          for (long q = 0; q < n; ++q) {
+            const double t = t0 + (q + 0.5) * step;
+            const double f[3] = {(S[0] + t * D[0]) / vox + 0.5 * nx - 0.5, (S[1] + t * D[1]) / vox + 0.5 * ny - 0.5,
+                                 (S[2] + t * D[2]) / vox + 0.5 * nz - 0.5};
+            const long i0 = (long)std::floor(f[0]), j0 = (long)std::floor(f[1]), l0 = (long)std::floor(f[2]);
+            const double wx = f[0] - i0, wy = f[1] - j0, wz = f[2] - l0;
+            double val = 0.0;
+            for (int dz = 0; dz < 2; ++dz)
+              for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                  const long i = i0 + dx, j = j0 + dy, l = l0 + dz;
+                  if (i < 0 || i >= nx || j < 0 || j >= ny || l < 0 || l >= nz) continue;
+                  const double w = (dx ? wx : 1 - wx) * (dy ? wy : 1 - wy) * (dz ? wz : 1 - wz);
+                  val += w * vol[(l * ny + j) * nx + i];
+                }
+            acc += val;
+          }
+          acc *= step;
+        }
+        out[((long)k * nv + iv) * nu + iu] = acc;
+      }
+    }
+  return 0;
+}

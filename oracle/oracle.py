@@ -89,6 +89,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_rasterize_ellipses.argtypes = [_D, i, i, i, d, _D]
     L.orc_rasterize_ellipsoids.argtypes = [_D, i, i, i, i, d, _D]
     L.orc_bp_cone_f32.argtypes = [_F, _I, i, i, i, i, d, d, d, d, d, d, i, i, i, d, i, i, _F]
+    L.orc_forward_project.argtypes = [_D, i, i, i, d, i, d, d, d, d, i, i, i, d, d, _D]
     L.orc_num_threads.restype = i
     L.orc_set_num_threads.argtypes = [i]
 
@@ -260,6 +261,19 @@ def volume_slices_u16(vol: np.ndarray) -> np.ndarray:
     unsigned short rule (round half to even)."""
     v = np.clip(np.asarray(vol, dtype=np.float32), 0, 1).astype(np.float32)
     return np.rint(v * np.float32(65535)).astype(np.uint16).transpose(1, 0, 2).copy()
+
+
+def forward_project(vol: np.ndarray, c: dict, cone: bool = True) -> np.ndarray:
+    """Ray-driven forward projection of a [z][y][x] volume in FP64 (see
+    orc_forward_project): c gives vox, nu, nv, nviews, du, dv, span, offset and,
+    for cone beam, sod and sdd. Returns [view][v][u]."""
+    v = np.ascontiguousarray(vol, dtype=np.float64)
+    nz, ny, nx = v.shape
+    out = np.zeros((c["nviews"], c["nv"], c["nu"]), np.float64)
+    _check(lib().orc_forward_project(_d(v), nx, ny, nz, c["vox"], int(cone), c.get("sod", 0.0), c.get("sdd", 0.0),
+                                     c["du"], c["dv"], c["nu"], c["nv"], c["nviews"], c["span"], c["offset"], _d(out)),
+           "forward_project")
+    return out
 
 
 def normalize_histogram(vol: np.ndarray, min_value: float | None = None, max_value: float | None = None) -> np.ndarray:
