@@ -555,14 +555,15 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   const int K = a.nviews, Q = K >> 2;
   const int nbh = a.ntx >> 1;  // representative tiles per axis (lower-left quadrant)
   const int bx = blockIdx.x % nbh, bz = blockIdx.x / nbh;
-  // interleaved layout: the CTA starts its walk at view group g0, advanced by
-  // about K/4 groups per `resident` CTAs in launch order. A CTA that starts
-  // after others have progressed then reads the same groups at the same time
-  // (their windows share L2) instead of restarting at group 0; the offset
-  // depends only on the block index, so results stay deterministic.
-  const int g0 = QG ? (int)(((long long)(blockIdx.y * gridDim.x + blockIdx.x) * (K >> 2) / max(1, a.resident)) %
-                            (K >> 2))
-                    : 0;
+  // The CTA starts its walk over the views at an offset advanced by about K
+  // views per `resident` CTAs in launch order (interleaved layout: by view
+  // groups). A CTA that starts after others have progressed then reads the
+  // same views at the same time (their windows share L2) instead of
+  // restarting at view 0; the offset depends only on the block index, so
+  // results stay deterministic.
+  const long long bid = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+  const int g0 = QG ? (int)((bid * (K >> 2) / max(1, a.resident)) % (K >> 2)) : 0;  // first view group
+  const int k0 = QG ? 0 : (int)((bid * K / max(1, a.resident)) % K);                 // first view (other layouts)
   const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
 
   QuadCoef* coef = reinterpret_cast<QuadCoef*>(smem + R);
@@ -591,7 +592,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       const int it = kb + lane;  // iteration (ring entry order)
       // view of the representative tile; rotation r uses view (k + r Q) mod K
       const int gq = QG ? ((it >> 2) + g0) % Q : 0;  // view group of iteration it
-      const int k = QG ? gq + (it & 3) * Q : it;
+      const int k = QG ? gq + (it & 3) * Q : (it + k0) % K;
       QuadCoef qc;
       int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
       bool skip = true, direct = false;
@@ -661,6 +662,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
         const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
         const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
+        const int ck = __shfl_sync(0xffffffffu, k, i);  // view of the representative tile at iteration q
         __syncwarp();
         if (lane == 0) {
           if (sk) {
@@ -678,7 +680,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               void* dst = smem + off + r * csub;
-              const int kv = (q + r * Q) % K;
+              const int kv = (ck + r * Q) % K;
               if (a.sino_layout)
                 tma_load_3d(dst, m, x, kv, e0, &full[e]);
               else
@@ -1252,8 +1254,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   if (packed)
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
+  a.resident = 2 * ctx->num_sms;  // symmetric kernel: two CTAs per SM
   if (layout == kLayoutQuadG16) {
-    a.resident = 2 * ctx->num_sms;
     a.qg = static_cast<const uint4*>(st.filt);
     a.qg_pitch = st.filt_pitch;
     a.qg_rows = st.v + 1;
