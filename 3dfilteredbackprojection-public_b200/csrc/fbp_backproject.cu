@@ -269,6 +269,18 @@ __device__ __forceinline__ __half2 lds_h2(uint32_t addr) {
   return *reinterpret_cast<__half2*>(&v);
 }
 
+// Two FP32 FMAs in one instruction (sm_100 packed f32x2), d = a * b + c per lane.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long ra, rb, rc, rd;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rc) : "f"(c.x), "f"(c.y));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(rc));
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(rd));
+  return d;
+}
+
 __device__ __forceinline__ uint4 lds_u4(uint32_t addr) {
   uint4 v;
   asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
@@ -662,7 +674,8 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
         const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
         const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
-        const int ck = __shfl_sync(0xffffffffu, k, i);  // view of the representative tile at iteration q
+        // view of the representative tile at iteration q (the interleaved layout addresses its group instead)
+        const int ck = QG ? 0 : __shfl_sync(0xffffffffu, k, i);
         __syncwarp();
         if (lane == 0) {
           if (sk) {
@@ -768,17 +781,25 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
           // four bilinear taps from the 2 x 16 bytes of one element (slot of rotation r: (M + r) mod 4)
           auto taps = [&](const uint4& L0, const uint4& L1, float fv, int j) {
             const uint32_t wv[8] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w};
+            float A[4], G[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               const int sl = (M + r) & 3;
               const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);      // (a, b - a)
               const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);  // (c' - a, d - c' - b + a)
               const float2 P = __half22float2(X1);
-              // u lerps in FP32 (one rounding each): row e - 1 and its v difference
-              const float A = fma_f16_f32(__low2half(fu2), __low2half(X2), P.x);
-              const float G = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
-              float& dst = KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j];
-              dst = fmaf(Wr[r], fmaf(fv, G, A), dst);
+              A[r] = fma_f16_f32(__low2half(fu2), __low2half(X2), P.x);
+              G[r] = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
+            }
+#pragma unroll
+            for (int pr = 0; pr < 2; ++pr) {
+              float& d0 = KAHAN ? part[KAHAN ? 2 * pr : 0][KAHAN ? j : 0] : acc[2 * pr][j];
+              float& d1 = KAHAN ? part[KAHAN ? 2 * pr + 1 : 0][KAHAN ? j : 0] : acc[2 * pr + 1][j];
+              const float2 t = ffma2(make_float2(fv, fv), make_float2(G[2 * pr], G[2 * pr + 1]),
+                                     make_float2(A[2 * pr], A[2 * pr + 1]));
+              const float2 d = ffma2(make_float2(Wr[2 * pr], Wr[2 * pr + 1]), t, make_float2(d0, d1));
+              d0 = d.x;
+              d1 = d.y;
             }
           };
           if (!g.direct) {
