@@ -426,11 +426,8 @@ int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n) {
   a.tw = ctx->ftab.twiddle;
   a.hbr = ctx->ftab.hbr;
   size_t smem = sizeof(float2) * (n / 2) + sizeof(float) * n + sizeof(float2) * n * a.pairs_per_cta;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-    attr_set = true;
-  }
+  // per device and process-wide: set on every launch (same value from every context)
+  cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   long long groups = (a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta;
   int grid = (int)std::min<long long>(groups, (long long)ctx->num_sms * 4);
   filter_fft_kernel<<<grid, 256, smem, ctx->stream>>>(a);
