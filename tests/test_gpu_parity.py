@@ -770,3 +770,72 @@ def test_forward_projection_agrees_with_analytic_line_integrals(fbp, oracle):
     err_r = relative_rmse(recs[0], recs[1])
     print(f"forward vs exact line integrals {err_p:.3e}, their FDKs {err_r:.3e}")
     assert err_p < 0.08 and err_r < 0.13
+
+
+# ------------------------------------------------------------------ edge cases
+def _edge_case(oracle, **kw):
+    c = dict(sod=300.0, sdd=520.0, du=1.25, dv=1.25, span=2 * math.pi, offset=0.1, nu=96, nv=72, nviews=48, nx=64,
+             ny=40, nz=64, vox=2.0)
+    c.update(kw)
+    from phantoms import random_ellipsoids
+    E = random_ellipsoids(np.random.default_rng(81), 12, 0.5 * min(c["nx"], c["nz"]) * c["vox"])
+    return c, oracle.project_ellipsoids_cone(E, c)
+
+
+@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+@pytest.mark.parametrize("case", ["one_view", "one_row", "ragged"])
+def test_edge_geometries(fbp, oracle, precision, case):
+    """A single view, a single-row detector, and ragged sizes (odd detector,
+    149 views, volume not a multiple of the 16 x 16 x 16 tile: generic kernel)."""
+    kw = {"one_view": dict(nviews=1), "one_row": dict(nv=1, ny=3),
+          "ragged": dict(nu=97, nv=61, nviews=149, nx=50, ny=7, nz=50)}[case]
+    c, proj = _edge_case(oracle, **kw)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(getattr(fbp.Precision, precision))
+    got = _gpu_fdk(s, c, proj, 0)
+    ref = oracle.fdk(proj, c, 0)
+    err = relative_rmse(got, ref)
+    print(f"edge {case} {precision}: {s.last_backprojection()} rel RMSE {err:.2e}")
+    # a single view or a single detector row leaves the FP16 storage error (2^-12
+    # relative per sample) almost unaveraged: 2.8e-4 and 1.3e-4 measured
+    tol = TOL_FP32 if precision == "FP32" else (4e-4 if case in ("one_view", "one_row") else TOL_MIXED)
+    assert err < tol
+
+
+def test_edge_rows_wider_than_the_fft(fbp, oracle):
+    """4100-sample rows pad to 8192: beyond the FFT filter (rejected with a
+    status), within the tensor-core Toeplitz filter."""
+    rng = np.random.default_rng(82)
+    proj = (rng.standard_normal((2, 3, 4100)) + 1.0).astype(np.float32)
+    s = fbp.FBP3D(0)
+    s.set_filter_impl(fbp.FilterImpl.FFT)
+    s.upload_projections(proj)
+    with pytest.raises(fbp.FBPError) as e:
+        s.apply_filter_to_projections(0)
+    assert e.value.status == -6
+    s.set_filter_impl(fbp.FilterImpl.TOEPLITZ)
+    s.upload_projections(proj)
+    s.apply_filter_to_projections(0)
+    got = s.download_projections()
+    ref = oracle.filter_rows(proj.astype(np.float64).reshape(-1, 4100), 0).reshape(proj.shape)
+    assert relative_rmse(got, ref) < TOL_TOEPLITZ_ROWS
+
+
+def test_edge_invalid_arguments_leave_the_context_usable(fbp, oracle):
+    s = fbp.FBP3D(0)
+    for bad in (lambda: s.generate_blank_projections(0, 8, 4), lambda: s.generate_blank_volume(4, -1, 4),
+                lambda: s.upload_projections(np.zeros((0, 4, 4), np.float32)),
+                lambda: s.set_precision(7), lambda: s.set_filter_padding(100)):
+        with pytest.raises(fbp.FBPError):
+            bad()
+    s.generate_blank_projections(8, 8, 4)
+    with pytest.raises(fbp.FBPError):
+        s.apply_fdk_weights_to_projections(-1.0, 10.0, 8.0)
+    with pytest.raises(fbp.FBPError):
+        s.project_backward_cone_fdk_from_projections(100.0, 50.0, 8.0, 8.0, 1.0, 0, 8, 0.0)
+    # the context still reconstructs correctly afterwards
+    c, proj = _edge_case(oracle, nviews=16, nu=48, nv=32, nx=32, ny=20, nz=32)
+    got = _gpu_fdk(s, c, proj, 0)
+    assert relative_rmse(s.read_volume() if got is None else got, oracle.clip_negatives(oracle.fdk(proj, c, 0),
+                                                                                        y_limit=c["nz"])) < TOL_FP32
