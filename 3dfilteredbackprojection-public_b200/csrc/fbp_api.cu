@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 using fbp::Stack;
 
@@ -542,6 +543,10 @@ int fbp_destroy(fbp_context* ctx) {
     cudaFree(ctx->ttab.th);
     cudaFree(ctx->d_scratch);
     cudaFreeHost(ctx->h_pinned);
+    if (ctx->copy_stream) {
+      cudaStreamSynchronize(ctx->copy_stream);
+      cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   }
   delete ctx;
@@ -607,7 +612,7 @@ int fbp_set_backprojector(fbp_context* ctx, int variant) {
   if (variant < FBP_BACKPROJECTOR_AUTO || variant > FBP_BACKPROJECTOR_SYMMETRIC)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown backprojector variant");
   ctx->bp_variant = variant;
-  ctx->plan.valid = false;
+  for (auto& p : ctx->plans) p.valid = false;
   return FBP_OK;
 }
 
@@ -1106,6 +1111,81 @@ int fbp_project_backward_parallel_from_sinograms(fbp_context* ctx, float rot, in
   FBP_TRY(require_stack(ctx, ctx->sino, "project_backward_parallel_from_sinograms"));
   if (h <= 0 || v <= 0) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
   return backproject(ctx, ctx->sino, parallel_geom(ctx->sino, rot, h, v, offset));
+}
+
+int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int cols, int rows, int count,
+                                const fbp_geometry* g, int filter_type, int h, int v, float* volume, int slabs) {
+  FBP_CTX(ctx);
+  if (!projections || !volume || !g) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null pointer");
+  if (slabs < 1 || slabs > 64 || v <= 0 || h <= 0 || slabs > v)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "slabs must be in [1, min(64, v)]");
+  if (ctx->det_rows_total > 0 || ctx->slab_ny > 0)
+    return fbp::set_error(ctx, FBP_ERR_STATE, "reconstruct_fdk_to_host with a detector band or volume slab set");
+  Stack& s = ctx->proj;
+  // upload (the host buffer should be pinned), weights, filter
+  if (!(s.f32 && s.u == cols && s.v == rows && s.n == count)) FBP_TRY(alloc_stack(ctx, s, cols, rows, count, false));
+  s.filtered = false;
+  s.log_pending = s.weights_pending = false;
+  FBP_TRY(fbp::cuda_check(ctx,
+                          cudaMemcpy2DAsync(s.f32, (size_t)s.pitch * 4, projections, (size_t)cols * 4, (size_t)cols * 4,
+                                            s.rows(), cudaMemcpyHostToDevice, ctx->stream),
+                          "projection upload"));
+  const bool cone = g->kind == FBP_GEOMETRY_CONE;
+  if (cone)
+    FBP_TRY(record_weights(ctx, s, g->source_distance, g->detector_distance, g->detector_width, "reconstruct_fdk_to_host"));
+  FBP_TRY(filter_stack(ctx, s, filter_type));
+  fbp::BPGeom gg;
+  if (cone) {
+    gg = cone_geom(s, g->source_distance, g->detector_distance, g->detector_width, g->volume_width,
+                   g->full_rotation_count, h, v, g->rotation_offset_radian);
+  } else {
+    gg = parallel_geom(s, g->full_rotation_count, h, v, g->rotation_offset_radian);
+    gg.vox = (double)g->volume_width / h;
+    gg.du = (double)g->detector_width / s.u;
+    gg.dv = gg.du;
+  }
+  if (cone && !(gg.sod > 0.0 && gg.sdd >= gg.sod))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "source distance must be positive");
+  if (!(gg.du > 0.0) || !(gg.vox > 0.0))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
+  FBP_TRY(ensure_volume(ctx, h, v, h, false));
+  if (!ctx->copy_stream) {
+    DeviceGuard guard(ctx->device);
+    FBP_TRY(fbp::cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream"));
+  }
+  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  std::vector<cudaEvent_t> done(slabs, nullptr);
+  int rc = FBP_OK;
+  // y-slab k is backprojected straight into the whole volume, then copied to
+  // the host on the copy stream while slab k + 1 computes
+  for (int k = 0; k < slabs && rc == FBP_OK; ++k) {
+    const int y0 = (int)((long long)v * k / slabs), y1 = (int)((long long)v * (k + 1) / slabs);
+    fbp::BPGeom gs = gg;
+    gs.ny_total = v;
+    gs.y_off = y0;
+    gs.ny = y1 - y0;
+    gs.vol_ystride = v;
+    const int ylim = ctx->clip_after_bp ? std::max(0, std::min(gs.ny, gs.nz - y0)) : 0;
+    rc = fbp::launch_backproject(ctx, gs, s, ctx->vol + (size_t)y0 * h, ylim, mixed);
+    s.pack_ready = mixed && !s.filtered;  // the first slab packed the views: the others reuse them
+    if (rc) break;
+    if ((rc = fbp::cuda_check(ctx, cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming), "event")) ||
+        (rc = fbp::cuda_check(ctx, cudaEventRecord(done[k], ctx->stream), "event")) ||
+        (rc = fbp::cuda_check(ctx, cudaStreamWaitEvent(ctx->copy_stream, done[k], 0), "event wait")))
+      break;
+    rc = fbp::cuda_check(ctx,
+                         cudaMemcpy2DAsync(volume + (size_t)y0 * h, (size_t)v * h * 4, ctx->vol + (size_t)y0 * h,
+                                           (size_t)v * h * 4, (size_t)(y1 - y0) * h * 4, h, cudaMemcpyDeviceToHost,
+                                           ctx->copy_stream),
+                         "slab readback");
+  }
+  s.pack_ready = false;
+  ctx->minmax_valid = false;
+  cudaStreamSynchronize(ctx->copy_stream);
+  for (cudaEvent_t e : done)
+    if (e) cudaEventDestroy(e);
+  if (rc) return rc;
+  return sync_host(ctx, true);
 }
 
 int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* g, int filter_type, int h, int v) {

@@ -95,6 +95,7 @@ struct BPArgs {
   int resident;           // CTAs resident on the GPU at once (view-group skew of the interleaved walk)
   int* minmax;            // fold the stored values' min / max into this pair (or nullptr)
   int y_off, ny_total;    // the volume is y-slices [y_off, y_off + ny) of ny_total
+  int vol_ystride;        // y-slices between z planes of the output buffer
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   const int ix = ix0 + tx, iz = iz0 + tz;
   float lo = __int_as_float(0x7f800000), hi = -lo;
   if (ix < a.nx && iz < a.nz) {
-    float* out = a.vol + ((size_t)iz * a.ny) * a.nx + ix;
+    float* out = a.vol + ((size_t)iz * a.vol_ystride) * a.nx + ix;
 #pragma unroll
     for (int j = 0; j < NY; ++j) {
       const int iy = iy0 + j;
@@ -933,7 +934,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   float lo = __int_as_float(0x7f800000), hi = -lo;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    float* out = a.vol + ((size_t)cz[r] * a.ny) * a.nx + cx[r];
+    float* out = a.vol + ((size_t)cz[r] * a.vol_ystride) * a.nx + cx[r];
 #pragma unroll
     for (int j = 0; j < NY; ++j) {
       const int iy = iy0 + j;
@@ -1125,6 +1126,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   // row band of a taller detector / y-slab of a taller volume (sharding)
   a.cv = 0.5 * (g.nv_total > 0 ? g.nv_total : g.nv) - 0.5 - g.row_off;
   a.y_off = g.y_off;
+  a.vol_ystride = g.vol_ystride > 0 ? g.vol_ystride : g.ny;
   a.ny_total = g.ny_total > 0 ? g.ny_total : g.ny;
   if (g.kind == FBP_GEOMETRY_CONE) {
     a.dvn = (float)(g.sdd / (g.sod * g.dv) * g.vox);
@@ -1189,10 +1191,19 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                     (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz,
                     (double)a.align, (double)NY, (double)g.row_off, (double)g.nv_total, (double)g.y_off,
                     (double)g.ny_total};
-  fbp_context::BPPlan& plan = ctx->plan;
-  bool hit = plan.valid;
-  for (int i = 0; i < 20 && hit; ++i) hit = plan.key[i] == key[i];
+  fbp_context::BPPlan* found = nullptr;
+  for (auto& p : ctx->plans) {
+    bool same = p.valid;
+    for (int i = 0; i < 20 && same; ++i) same = p.key[i] == key[i];
+    if (same) {
+      found = &p;
+      break;
+    }
+  }
+  const bool hit = found != nullptr;
+  fbp_context::BPPlan& plan = hit ? *found : ctx->plans[ctx->plan_next];
   if (!hit) {
+    ctx->plan_next = (ctx->plan_next + 1) % (int)(sizeof(ctx->plans) / sizeof(ctx->plans[0]));
     plan.valid = false;
     if (ctx->span_cap < 4) {
       cudaFree(ctx->d_span);
@@ -1256,7 +1267,6 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   if (!use_quad) {
     if (quad) {
       // re-plan with the generic tile height
-      ctx->plan.valid = false;
       const int saved = ctx->bp_variant;
       ctx->bp_variant = FBP_BACKPROJECTOR_GENERIC;
       const int rc = launch_backproject(ctx, g, st, vol, clip_ylimit, mixed);
@@ -1272,7 +1282,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     smem = (size_t)stages * per_stage + 64;
   }
 
-  if (packed)
+  if (packed && !(st.pack_ready && st.filt_layout == layout))
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
   a.resident = 2 * ctx->num_sms;  // symmetric kernel: two CTAs per SM

@@ -59,6 +59,7 @@ struct Stack {
   float* inv_scale = nullptr;     // per view (x2: [inv | scale]) for the FP16 layouts
   int scale_cap = 0;              // views inv_scale has room for
   size_t f32_cap = 0;             // bytes allocated at f32 (buffers only grow: no cudaFree between jobs)
+  bool pack_ready = false;        // filt already holds the packed FP16 views of f32 (slabs of one reconstruction)
   // Log normalisation and FDK weights recorded by their calls and applied
   // inside the filter kernel's load (log first, then weight), or by a
   // standalone pass when something else reads the rows first.
@@ -134,14 +135,16 @@ struct fbp_context {
   void* h_pinned = nullptr;      // small pinned staging for per-call tables
   size_t h_pinned_bytes = 0;
 
-  // cached footprint plan
-  // cached backprojection plan: the largest detector window of any
-  // (tile, view) for the geometry (samples, rows including row v + 1)
+  // cached backprojection plans: the largest detector window of any
+  // (tile, view) for a geometry (samples, rows including row v + 1); several,
+  // so that the slabs of a streamed reconstruction keep theirs
   struct BPPlan {
     bool valid = false;
     double key[20] = {0};
     int box_u = 0, box_v = 0;
-  } plan;
+  } plans[16];
+  int plan_next = 0;
+  cudaStream_t copy_stream = nullptr;  // slab readback beside the backprojection (created on first use)
 };
 
 namespace fbp {
@@ -205,6 +208,7 @@ struct BPGeom {
   // rows, and the volume y-slices [y_off, y_off + ny) of ny_total (0: whole)
   int row_off = 0, nv_total = 0;
   int y_off = 0, ny_total = 0;
+  int vol_ystride = 0;  // y-slices between z planes of the output (0: ny); a slab of a whole volume
 };
 // Backproject the stack's content (filt when filtered, else f32 rows). In
 // the MIXED form (`mixed`) f32 content is first packed into the FP16 layout

@@ -149,6 +149,7 @@ SIGNATURES = {
     "fbp_write_volume": [_P, C.c_char_p],
     "fbp_projection_file_index": [C.c_char_p],
     "fbp_plan_slabs": [C.POINTER(Geometry), _I, _I, _I, _I, _I, C.POINTER(C.c_int)],
+    "fbp_reconstruct_fdk_to_host": [_P, _P, _I, _I, _I, C.POINTER(Geometry), _I, _I, _I, _P, _I],
     "fbp_project_forward_cone_to_projections": [_P, _F, _F, _F, _F, _F, _I, _F],
     "fbp_project_forward_cone_to_sinograms": [_P, _F, _F, _F, _F, _F, _I, _F],
     "fbp_project_forward_parallel_to_projections": [_P, _F, _I, _F],
@@ -390,6 +391,21 @@ class FBP3D:
                                              rotation_offset_radian=0.0) -> None:
         self.ctx.call("fbp_project_forward_parallel_to_sinograms", full_rotation_count, int(projection_count),
                       rotation_offset_radian)
+
+    def reconstruct_fdk_to_host(self, projections, geometry: "Geometry", filter_type: int, volume_h: int,
+                                volume_v: int, out=None, slabs: int = 8):
+        """fbp_reconstruct_fdk_to_host: host projections [count][rows][cols] in, host
+        [z][y][x] volume out; the slab readback overlaps the backprojection."""
+        n, rows, cols = projections.shape
+        if out is None:
+            out = np.empty((volume_h, volume_v, volume_h), np.float32)
+        p, pdev = _ptr(projections)
+        o, odev = _ptr(out)
+        if pdev or odev:
+            raise ValueError("reconstruct_fdk_to_host takes host buffers")
+        self.ctx.call("fbp_reconstruct_fdk_to_host", p, cols, rows, n, C.byref(geometry), int(filter_type),
+                      int(volume_h), int(volume_v), o, int(slabs))
+        return out
 
     def set_detector_rows(self, row_offset: int, total_rows: int) -> None:
         """The stacks hold rows [row_offset, row_offset + v) of a total_rows-row detector (0, 0: whole)."""

@@ -293,6 +293,14 @@ int fbp_project_backward_parallel_from_sinograms(fbp_context* ctx, float full_ro
  * optional clip) on the resident projections, geometry as above. */
 int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* geometry, int filter_type,
                         int volume_resolution_horizontal, int volume_resolution_vertical);
+/* Host buffers in, host volume out, overlapped (no counterpart in the reference): upload the
+ * [count][rows][cols] projections (pinned host memory recommended), FDK weights (cone),
+ * filter, then backproject the volume in `slabs` y-ranges (1..64) written straight into the
+ * context's h x v x h volume, each slab copied to `volume` ([z][y][x], host) on a second
+ * stream while the next slab computes. Returns when `volume` is complete. */
+int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int cols, int rows, int count,
+                                const fbp_geometry* geometry, int filter_type, int h, int v, float* volume,
+                                int slabs);
 
 /* ---- 2D (FBP2D.h:17-41) on caller-owned device buffers ---------------------
  * sinogram [views][bins], image [rows][cols]; filtered in place. */

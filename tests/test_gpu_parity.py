@@ -772,6 +772,29 @@ def test_forward_projection_agrees_with_analytic_line_integrals(fbp, oracle):
     assert err_p < 0.08 and err_r < 0.13
 
 
+# ------------------------------------------------ streamed reconstruction to host
+@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+def test_reconstruct_to_host_matches_the_stepwise_calls(fbp, oracle, phantoms, precision):
+    """Upload, weights, filter and slab-wise backprojection with the readback of
+    each slab overlapping the next: the same volume as the step-by-step calls
+    (the slabs' windows are re-based, so equality is to FP32 rounding)."""
+    c, proj = _cone_case(phantoms, oracle, 2)
+    ga = phantoms.geometry_args(c)
+    g = fbp.Geometry.cone(ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"],
+                          ga["full_rotation_count"], ga["offset"])
+    prec = getattr(fbp.Precision, precision)
+    a = fbp.FBP3D(0)
+    a.set_precision(prec)
+    whole = _gpu_fdk(a, c, proj, 0)
+    b = fbp.FBP3D(0)
+    b.set_precision(prec)
+    for slabs in (1, 5):
+        got = b.reconstruct_fdk_to_host(proj, g, 0, c["nx"], c["ny"], slabs=slabs)
+        err = relative_rmse(got, whole)
+        print(f"to_host {precision} slabs={slabs}: vs stepwise {err:.2e}")
+        assert err < 1e-6
+
+
 # ------------------------------------------------------------------ edge cases
 def _edge_case(oracle, **kw):
     c = dict(sod=300.0, sdd=520.0, du=1.25, dv=1.25, span=2 * math.pi, offset=0.1, nu=96, nv=72, nviews=48, nx=64,
