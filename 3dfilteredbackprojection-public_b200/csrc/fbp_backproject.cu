@@ -282,6 +282,28 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
   return d;
 }
 
+__device__ __forceinline__ unsigned long long pack2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long r) {
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+  return d;
+}
+// a + b per lane rounded toward zero, and a - b rounded to nearest (packed f32x2)
+__device__ __forceinline__ float2 fadd2_rz(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+  return unpack2(d);
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+  return unpack2(d);
+}
+
 __device__ __forceinline__ uint4 lds_u4(uint32_t addr) {
   uint4 v;
   asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
@@ -805,13 +827,19 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
           };
           if (!g.direct) {
             const uint32_t plane = (uint32_t)BU * 16;
+            static_assert(NY % 2 == 0, "voxels stepped in pairs");
+            const float2 magic2 = make_float2(kMagic, kMagic);
 #pragma unroll
-            for (int j = 0; j < NY; ++j) {
-              const float v = fmaf((float)j, dvv, vl);
-              const float t = __fadd_rz(v, kMagic);
-              const float fv = v - (t - kMagic);
-              const uint32_t addr = __float_as_uint(t) * RB + c0;
-              taps(lds_u4(addr), lds_u4(addr + plane), fv, j);  // slots 0, 1 | slots 2, 3
+            for (int j = 0; j < NY; j += 2) {
+              // v, floor and fraction of voxels j and j + 1 with packed FP32 ops
+              // (the same IEEE operations as the scalar form)
+              const float2 v2 = ffma2(make_float2((float)j, (float)(j + 1)), make_float2(dvv, dvv),
+                                      make_float2(vl, vl));
+              const float2 t2 = fadd2_rz(v2, magic2);
+              const float2 fv2 = fsub2(v2, fsub2(t2, magic2));
+              const uint32_t a0 = __float_as_uint(t2.x) * RB + c0, a1 = __float_as_uint(t2.y) * RB + c0;
+              taps(lds_u4(a0), lds_u4(a0 + plane), fv2.x, j);  // slots 0, 1 | slots 2, 3
+              taps(lds_u4(a1), lds_u4(a1 + plane), fv2.y, j + 1);
             }
           } else {
             // window not staged: read the elements from global memory (zero

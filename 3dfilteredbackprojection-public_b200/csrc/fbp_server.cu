@@ -134,15 +134,14 @@ struct fbp_server {
     const fbp_geometry& g = r.geometry;
     int rc = fbp_set_precision(c, r.precision);
     if (r.kind == FBP_JOB_CONE) {
+      // one call: upload, weights, filter, slab-wise backprojection with the
+      // volume readback overlapped (large volumes in 4 slabs)
+      fbp_geometry gc = g;
+      gc.kind = FBP_GEOMETRY_CONE;
       if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
-      if (!rc) rc = fbp_upload_projections(c, r.input, r.det_cols, r.det_rows, r.views, 0);
-      if (!rc) rc = fbp_apply_fdk_weights_to_projections(c, g.source_distance, g.detector_distance, g.detector_width);
-      if (!rc) rc = fbp_apply_filter_to_projections(c, r.filter_type);
       if (!rc)
-        rc = fbp_project_backward_cone_fdk_from_projections(c, g.source_distance, g.detector_distance,
-                                                            g.detector_width, g.volume_width, g.full_rotation_count,
-                                                            r.vol_h, r.vol_v, g.rotation_offset_radian);
-      if (!rc) rc = fbp_read_volume(c, r.output, 0);
+        rc = fbp_reconstruct_fdk_to_host(c, r.input, r.det_cols, r.det_rows, r.views, &gc, r.filter_type, r.vol_h,
+                                         r.vol_v, r.output, r.vol_v >= 256 ? 4 : 1);
     } else if (r.kind == FBP_JOB_FAN2D || r.kind == FBP_JOB_PARALLEL2D) {
       const size_t in = (size_t)r.det_cols * r.views * 4, out = (size_t)r.vol_h * r.vol_h * 4;
       rc = device_buffer(&w.d_in, &w.in_cap, in);
