@@ -6,8 +6,9 @@
 
 namespace fbp {
 
-__device__ __forceinline__ float load_pre(const RowSet& rs, long long r, int i) {
-  float x = rs.data[r * rs.pitch + i];
+// The pending pre-operations (log normalisation, then FDK weight) on the raw
+// sample x of row r, column i.
+__device__ __forceinline__ float pre_op(const RowSet& rs, long long r, int i, float x) {
   if (rs.log_norm) {
     float y = fmaxf(x, 1e-30f * rs.log_base);
     x = -logf(y / rs.log_base);
@@ -19,6 +20,10 @@ __device__ __forceinline__ float load_pre(const RowSet& rs, long long r, int i) 
     x *= rs.w_sdd * rsqrtf(rs.w_sdd * rs.w_sdd + u * u + v * v);
   }
   return x;
+}
+
+__device__ __forceinline__ float load_pre(const RowSet& rs, long long r, int i) {
+  return pre_op(rs, r, i, rs.data[r * rs.pitch + i]);
 }
 
 __device__ __forceinline__ int row_view(const RowSet& rs, long long r) {

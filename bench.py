@@ -175,6 +175,10 @@ def cpu_inputs(c: dict, nviews_sample: int):
 def reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
+    if args.workload == "serving":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving path (one "
+                          "reconstruction per process); its CPU arm is measured on the cone workloads"}), flush=True)
+        return
     c = workload(args.scale, args.workload)
     nsv = 8 if args.scale == 1 else 4
     proj, views = cpu_inputs(c, nsv)
