@@ -333,6 +333,69 @@ fbp::BPGeom cone_geom(const Stack& s, float sod, float odd, float det_w, float v
   return g;
 }
 
+// Autotuner: the first backprojection of a geometry (with autotuning on) times
+// each applicable kernel - the four-fold symmetric one and the generic one
+// with 16 or with 8 voxels per thread along y - on a central slab of up to 48
+// y-slices (written into the volume, which the real launch then overwrites)
+// and keeps the fastest for that geometry, form and stack layout.
+int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, bool mixed, int* variant) {
+  const double key[21] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
+                          (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz, (double)mixed,
+                          (double)(s.filtered ? s.filt_layout : -1), (double)g.row_off, (double)g.nv_total,
+                          (double)g.y_off, (double)g.ny_total, (double)s.sinogram};
+  for (const auto& t : ctx->tuned)
+    if (std::equal(key, key + 21, t.key)) {
+      *variant = t.variant;
+      return FBP_OK;
+    }
+  const int nt = std::min(g.ny, 48), y0 = (g.ny - nt) / 2;
+  fbp::BPGeom gt = g;
+  gt.ny_total = g.ny_total > 0 ? g.ny_total : g.ny;
+  gt.y_off = g.y_off + y0;
+  gt.ny = nt;
+  gt.vol_ystride = g.vol_ystride > 0 ? g.vol_ystride : g.ny;
+  const int cand[3] = {FBP_BACKPROJECTOR_SYMMETRIC, FBP_BACKPROJECTOR_GENERIC, FBP_BACKPROJECTOR_GENERIC_Y8};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FBP_TRY(fbp::cuda_check(ctx, cudaEventCreate(&e0), "event"));
+  FBP_TRY(fbp::cuda_check(ctx, cudaEventCreate(&e1), "event"));
+  const int saved_variant = ctx->bp_variant;
+  float best = 1e30f;
+  int rc = FBP_OK;
+  *variant = FBP_BACKPROJECTOR_GENERIC;
+  for (const int c : cand) {
+    ctx->bp_variant = c;
+    int r = fbp::launch_backproject(ctx, gt, s, ctx->vol + (size_t)y0 * g.nx, 0, mixed);  // plan, pack: untimed
+    if (r == FBP_ERR_UNSUPPORTED) continue;  // geometry not symmetric, windows too large, ...
+    if (r) {
+      rc = r;
+      break;
+    }
+    s.pack_ready = mixed && !s.filtered;  // the timed launch reuses the packed views
+    cudaEventRecord(e0, ctx->stream);
+    r = fbp::launch_backproject(ctx, gt, s, ctx->vol + (size_t)y0 * g.nx, 0, mixed);
+    cudaEventRecord(e1, ctx->stream);
+    if (r || (r = sync_host(ctx, true))) {
+      rc = r;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      *variant = c;
+    }
+  }
+  ctx->bp_variant = saved_variant;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  fbp_context::TuneEntry t;
+  std::copy(key, key + 21, t.key);
+  t.variant = *variant;
+  ctx->tuned.push_back(t);
+  return FBP_OK;
+}
+
 int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
   if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
@@ -359,7 +422,21 @@ int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
   FBP_TRY(flush_pending(ctx, s));
   FBP_TRY(ensure_volume(ctx, g.nx, g.ny, g.nz, false));
   const int ylim = ctx->clip_after_bp ? clip_limit : 0;
-  return fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, ctx->precision == FBP_PRECISION_MIXED);
+  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && g.ny > 1) {
+    int variant = FBP_BACKPROJECTOR_AUTO;
+    int rc = autotune_backprojector(ctx, s, g, mixed, &variant);
+    if (rc == FBP_OK) {
+      ctx->bp_variant = variant;
+      rc = fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, mixed);
+      ctx->bp_variant = FBP_BACKPROJECTOR_AUTO;
+    }
+    s.pack_ready = false;
+    // the outer slices can have wider windows than the tuning slab: the
+    // untuned selection still applies there
+    if (rc != FBP_ERR_UNSUPPORTED) return rc;
+  }
+  return fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, mixed);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
@@ -609,20 +686,28 @@ int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable) {
 
 int fbp_set_backprojector(fbp_context* ctx, int variant) {
   FBP_CTX(ctx);
-  if (variant < FBP_BACKPROJECTOR_AUTO || variant > FBP_BACKPROJECTOR_SYMMETRIC)
+  if (variant < FBP_BACKPROJECTOR_AUTO || variant > FBP_BACKPROJECTOR_GENERIC_Y8)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown backprojector variant");
   ctx->bp_variant = variant;
   for (auto& p : ctx->plans) p.valid = false;
   return FBP_OK;
 }
 
-int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v) {
+int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v,
+                            int* tile_ny) {
   if (!ctx) return FBP_ERR_INVALID_ARGUMENT;
   if (ctx->last_bp[0] < 0) return FBP_ERR_STATE;
   if (variant) *variant = ctx->last_bp[0];
   if (layout) *layout = ctx->last_bp[1];
   if (box_u) *box_u = ctx->last_bp[2];
   if (box_v) *box_v = ctx->last_bp[3];
+  if (tile_ny) *tile_ny = ctx->last_bp[4];
+  return FBP_OK;
+}
+
+int fbp_set_autotune(fbp_context* ctx, int enable) {
+  FBP_CTX(ctx);
+  ctx->autotune = enable ? 1 : 0;
   return FBP_OK;
 }
 
@@ -1156,6 +1241,12 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
   const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
   std::vector<cudaEvent_t> done(slabs, nullptr);
   int rc = FBP_OK;
+  const int saved_variant = ctx->bp_variant;
+  if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && v > 1) {
+    int variant = FBP_BACKPROJECTOR_AUTO;
+    rc = autotune_backprojector(ctx, s, gg, mixed, &variant);
+    ctx->bp_variant = variant;
+  }
   // y-slab k is backprojected straight into the whole volume, then copied to
   // the host on the copy stream while slab k + 1 computes
   for (int k = 0; k < slabs && rc == FBP_OK; ++k) {
@@ -1167,6 +1258,11 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
     gs.vol_ystride = v;
     const int ylim = ctx->clip_after_bp ? std::max(0, std::min(gs.ny, gs.nz - y0)) : 0;
     rc = fbp::launch_backproject(ctx, gs, s, ctx->vol + (size_t)y0 * h, ylim, mixed);
+    if (rc == FBP_ERR_UNSUPPORTED && ctx->bp_variant != saved_variant) {
+      // a tuned choice that an outer slab's windows do not allow
+      ctx->bp_variant = saved_variant;
+      rc = fbp::launch_backproject(ctx, gs, s, ctx->vol + (size_t)y0 * h, ylim, mixed);
+    }
     s.pack_ready = mixed && !s.filtered;  // the first slab packed the views: the others reuse them
     if (rc) break;
     if ((rc = fbp::cuda_check(ctx, cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming), "event")) ||
@@ -1180,6 +1276,7 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
                          "slab readback");
   }
   s.pack_ready = false;
+  ctx->bp_variant = saved_variant;
   ctx->minmax_valid = false;
   cudaStreamSynchronize(ctx->copy_stream);
   for (cudaEvent_t e : done)

@@ -1125,7 +1125,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   const long long iturns = llround(turns);
   const bool symmetric = !is2d && g.nx == g.nz && g.nx % 32 == 0 && g.nviews % 4 == 0 &&
                          fabs(turns - (double)iturns) < 1e-9 && iturns % 4 == 1;
-  const bool quad = symmetric && ctx->bp_variant != FBP_BACKPROJECTOR_GENERIC;
+  const bool quad = symmetric && (ctx->bp_variant == FBP_BACKPROJECTOR_AUTO ||
+                                  ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC);
   if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC && !symmetric)
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
                      "the four-fold symmetric backprojector needs nx == nz (a multiple of 32), views % 4 == 0 and "
@@ -1209,7 +1210,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   a.trig = ctx->d_trig;
 
   // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
-  const int TX = 16, TZ = 16, NY = is2d ? 1 : (quad ? 8 : 16);
+  const int TX = 16, TZ = 16, NY = is2d ? 1 : (quad || ctx->bp_variant == FBP_BACKPROJECTOR_GENERIC_Y8 ? 8 : 16);
   a.ntx = (g.nx + TX - 1) / TX;
   a.ntz = (g.nz + TZ - 1) / TZ;
   const int nty = (g.ny + NY - 1) / NY;
@@ -1380,13 +1381,17 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     if (int rc = launch_minmax_init(ctx, ctx->d_minmax)) return rc;
     a.minmax = ctx->d_minmax;
   }
-  ctx->last_bp[0] = use_quad ? FBP_BACKPROJECTOR_SYMMETRIC : FBP_BACKPROJECTOR_GENERIC;
+  ctx->last_bp[0] = use_quad    ? FBP_BACKPROJECTOR_SYMMETRIC
+                    : NY == 8   ? FBP_BACKPROJECTOR_GENERIC_Y8
+                                : FBP_BACKPROJECTOR_GENERIC;
   ctx->last_bp[1] = layout;
   ctx->last_bp[2] = bu;
   ctx->last_bp[3] = bv;
-  cudaError_t e = use_quad ? launch_quad(layout, maps, a, smem, kahan, ctx->stream)
-                 : is2d   ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
-                          : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
+  ctx->last_bp[4] = NY;
+  cudaError_t e = use_quad    ? launch_quad(layout, maps, a, smem, kahan, ctx->stream)
+                 : is2d      ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
+                 : NY == 8   ? launch_layout<16, 16, 8>(layout, maps, a, smem, kahan, ctx->stream)
+                             : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
   ctx->minmax_valid = e == cudaSuccess && a.minmax != nullptr;
   return cuda_check(ctx, e, "bp_kernel");

@@ -107,7 +107,13 @@ struct fbp_context {
   int bp_variant = FBP_BACKPROJECTOR_AUTO;
   int det_row_off = 0, det_rows_total = 0;  // fbp_set_detector_rows (0 rows: the whole detector)
   int slab_y0 = 0, slab_ny = 0;             // fbp_set_volume_slab (0 slices: the whole volume)
-  int last_bp[4] = {-1, -1, 0, 0};  // variant, layout, box_u, box_v of the last backprojection
+  int last_bp[5] = {-1, -1, 0, 0, 0};  // variant, layout, box_u, box_v, tile height of the last backprojection
+  int autotune = 0;                    // time the backprojector variants per geometry on first use
+  struct TuneEntry {
+    double key[21];
+    int variant;
+  };
+  std::vector<TuneEntry> tuned;        // autotuner choices per geometry
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched by this context
 

@@ -53,6 +53,7 @@ class Backprojector(enum.IntEnum):
     AUTO = 0
     GENERIC = 1
     SYMMETRIC = 2
+    GENERIC_Y8 = 3
 
 
 class FilterImpl(enum.IntEnum):
@@ -109,7 +110,9 @@ SIGNATURES = {
     "fbp_set_clip_after_backprojection": [_P, _I],
     "fbp_set_backprojector": [_P, _I],
     "fbp_memory_in_use": [_P, C.POINTER(C.c_size_t)],
-    "fbp_last_backprojection": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fbp_last_backprojection": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_int)],
+    "fbp_set_autotune": [_P, _I],
     "fbp_generate_blank_volume": [_P, _I, _I, _I],
     "fbp_generate_blank_projections": [_P, _I, _I, _I],
     "fbp_generate_blank_sinograms": [_P, _I, _I, _I],
@@ -361,11 +364,16 @@ class FBP3D:
 
     def last_backprojection(self) -> dict:
         """Kernel, staged layout and window box of the last backprojection."""
-        v, l, bu, bv = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        self.ctx.call("fbp_last_backprojection", C.byref(v), C.byref(l), C.byref(bu), C.byref(bv))
+        v, l, bu, bv, ny = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.ctx.call("fbp_last_backprojection", C.byref(v), C.byref(l), C.byref(bu), C.byref(bv), C.byref(ny))
         names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16"}
-        return {"kernel": "symmetric" if v.value == Backprojector.SYMMETRIC else "generic",
-                "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value)}
+        kernels = {Backprojector.SYMMETRIC: "symmetric", Backprojector.GENERIC_Y8: "generic_y8"}
+        return {"kernel": kernels.get(v.value, "generic"),
+                "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value), "tile_ny": ny.value}
+
+    def set_autotune(self, enable: bool) -> None:
+        """Time the backprojector variants on the first backprojection of each geometry and keep the fastest."""
+        self.ctx.call("fbp_set_autotune", 1 if enable else 0)
 
     # -- forward projection (FBP3D.cpp:212-330)
     def project_forward_cone_to_projections(self, xray_source_distance, detector_panel_distance, detector_width,

@@ -63,6 +63,8 @@ def parse_args():
     p.add_argument("--shard", choices=["replicas", "slabs"], default="replicas",
                    help="N>1: replicas = one independent volume per rank (weak scaling); slabs = one volume "
                         "split into y-slabs, each rank holding its detector row band (strong scaling)")
+    p.add_argument("--backprojector", choices=["auto", "generic", "generic_y8", "symmetric", "tuned"], default="auto",
+                   help="backprojector variant of both forms (tuned: timed per geometry on first use)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the CPU-baseline sample")
@@ -486,6 +488,10 @@ def main() -> None:
         s.set_stream(stream)
         s.set_precision(F.Precision.MIXED if form == "chosen" else F.Precision.FP32)
         s.set_clip_after_backprojection(True)
+        if args.backprojector == "tuned":
+            s.set_autotune(True)
+        elif args.backprojector != "auto":
+            s.set_backprojector(getattr(F.Backprojector, args.backprojector.upper()))
         if args.shard == "slabs":
             s.set_detector_rows(slab[2], c["nv"])
             s.set_volume_slab(slab[0], slab_ny)

@@ -63,6 +63,8 @@ extern "C" {
 #define FBP_BACKPROJECTOR_GENERIC 1   /* one 16x16x16 tile per CTA, any geometry    */
 #define FBP_BACKPROJECTOR_SYMMETRIC 2 /* four-fold orbit of tiles per CTA: square  */
                                       /* volume, views % 4 == 0 over one full turn */
+#define FBP_BACKPROJECTOR_GENERIC_Y8 3 /* generic with 16x16x8 tiles (8 voxels per  */
+                                       /* thread along y), any geometry            */
 
 /* ---- geometry kinds ------------------------------------------------------- */
 #define FBP_GEOMETRY_CONE 0     /* flat-panel cone beam, circular orbit         */
@@ -110,15 +112,25 @@ int fbp_set_filter_padding(fbp_context* ctx, int padded_length);
 int fbp_set_clip_after_backprojection(fbp_context* ctx, int enable);
 /* Backprojector variant (FBP_BACKPROJECTOR_*); AUTO by default. */
 int fbp_set_backprojector(fbp_context* ctx, int variant);
+/* 1: with the variant AUTO, the first backprojection of each geometry (form,
+ * staged layout, detector band and volume slab included) times the
+ * applicable kernels - symmetric, generic with 16 and with 8 voxels per
+ * thread along y - on a central slab of up to 48 y-slices and keeps the
+ * fastest for later calls of that geometry; 0 (default): AUTO picks the
+ * symmetric kernel when the geometry allows it. No counterpart in the
+ * reference, whose backprojection is one fixed shader. */
+int fbp_set_autotune(fbp_context* ctx, int enable);
 /* Device bytes held by ctx's buffers. */
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
 /* What the last backprojection ran (no counterpart in the reference, whose
- * backprojection is one fixed shader): *variant = FBP_BACKPROJECTOR_GENERIC or
- * FBP_BACKPROJECTOR_SYMMETRIC; *layout = staged view layout (0 FP32 rows,
+ * backprojection is one fixed shader): *variant = FBP_BACKPROJECTOR_GENERIC,
+ * _GENERIC_Y8 or _SYMMETRIC; *layout = staged view layout (0 FP32 rows,
  * 1 FP32 row pairs, 2 FP16 row pairs, 3 FP16 four-view gradient quads);
- * *box_u x *box_v = largest staged detector window in elements. Any output
- * pointer may be NULL. FBP_ERR_STATE before the first backprojection. */
-int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v);
+ * *box_u x *box_v = largest staged detector window in elements; *tile_ny =
+ * voxels per thread along y. Any output pointer may be NULL. FBP_ERR_STATE
+ * before the first backprojection. */
+int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, int* box_u, int* box_v,
+                            int* tile_ny);
 
 /* ---- buffers (FBP3D.cpp:16-56, 197-210) ----------------------------------- */
 int fbp_generate_blank_volume(fbp_context* ctx, int x_size, int y_size, int z_size);

@@ -382,17 +382,54 @@ def _sym_case(oracle, nviews=96, n=64, ny=40, offset=0.2):
     return c, oracle.project_ellipsoids_cone(E, c)
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_backprojector_variants_fp32(fbp, oracle, variant):
-    """Generic (1) and four-fold symmetric (2) backprojectors against the
-    oracle on a geometry both accept (square volume, 96 views, one turn)."""
+    """Generic (1), four-fold symmetric (2) and generic with 8-high tiles (3)
+    backprojectors against the oracle on a geometry all accept (square
+    volume, 96 views, one turn; 40 y-slices: a ragged last 8- or 16-high tile)."""
     c, proj = _sym_case(oracle)
     s = fbp.FBP3D(0)
     s.set_clip_after_backprojection(False)
     s.set_backprojector(variant)
     got = _gpu_fdk(s, c, proj, 0)
+    assert s.last_backprojection()["kernel"] == {1: "generic", 2: "symmetric", 3: "generic_y8"}[variant]
     ref = oracle.fdk(proj, c, 0)
     assert relative_rmse(got, ref) < TOL_FP32
+
+
+@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+def test_autotuned_backprojector(fbp, oracle, precision):
+    """With autotuning on, the first backprojection of a geometry times the
+    candidate kernels on a central slab and runs the fastest; the volume (and
+    the streamed reconstruction, which tunes the same way) must still match
+    the oracle, and a symmetric-incapable geometry (50-wide volume) tunes
+    among the generic kernels only. 192 views: with fewer, the FP16 rounding
+    of the MIXED form's filtered views averages out less (96 views give
+    1.08e-4 through the generic kernel)."""
+    tol = TOL_FP32 if precision == "FP32" else TOL_MIXED
+    prec = getattr(fbp.Precision, precision)
+    for n in (64, 50):
+        c, proj = _sym_case(oracle, nviews=192, n=n)
+        ref = oracle.fdk(proj, c, 0)
+        s = fbp.FBP3D(0)
+        s.set_clip_after_backprojection(False)
+        s.set_precision(prec)
+        s.set_autotune(True)
+        for _ in range(2):  # tuned, then from the tuning cache
+            got = _gpu_fdk(s, c, proj, 0)
+            info = s.last_backprojection()
+            err = relative_rmse(got, ref)
+            print(f"autotuned {precision} n={c['nx']}: {info} rel RMSE {err:.3e}")
+            assert err < tol
+            assert info["kernel"] in (("symmetric", "generic", "generic_y8") if n == 64 else ("generic", "generic_y8"))
+        sod, odd, w, vw, rot = _cone_args(c)
+        g = fbp.Geometry.cone(sod, odd, w, vw, rot, c["offset"])
+        t = fbp.FBP3D(0)
+        t.set_clip_after_backprojection(False)
+        t.set_precision(prec)
+        t.set_autotune(True)
+        got = t.reconstruct_fdk_to_host(proj, g, 0, c["nx"], c["ny"], slabs=3)
+        assert relative_rmse(got, ref) < tol
 
 
 @pytest.mark.parametrize("factor", [2, 1])
