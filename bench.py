@@ -66,6 +66,8 @@ def parse_args():
     p.add_argument("--backprojector", choices=["auto", "generic", "generic_y8", "symmetric", "tuned"], default="auto",
                    help="backprojector variant of both forms (tuned: timed per geometry on first use)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--oracle-voxels", type=int, default=200000,
+                   help="voxels of the sampled FP64-oracle accuracy check (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the CPU-baseline sample")
     return p.parse_args()
@@ -105,6 +107,46 @@ def _oracle():
     import oracle as O
     O.build(with_ref=False)
     return O
+
+
+def oracle_sample(c: dict, raw_rows, nvox: int) -> dict:
+    """FP64 oracle values of `nvox` seeded voxels in three y-slices near the
+    central plane (y = ny/2 and ny/2 +- ny/60), for the accuracy of a cone
+    workload too large for a whole-volume oracle. The voxels' projections stay
+    within a centred band of detector rows for every view (bounded with the
+    nearest possible source distance), so the oracle weights and filters only
+    that band: a centred band of nv' rows (nv' of nv's parity) has the same row
+    coordinates as the full detector. raw_rows(r0, r1) returns the raw
+    projections' rows [r0, r1) as a [view][row][u] FP32 array."""
+    import numpy as np
+    O = _oracle()
+    rng = np.random.default_rng(c["seed"] + 17)
+    yc = c["ny"] // 2
+    dy = max(1, c["ny"] // 60)
+    ys = np.clip(np.array([yc - dy, yc, yc + dy]), 0, c["ny"] - 1)
+    ymm = np.abs((ys + 0.5 - 0.5 * c["ny"]) * c["vox"]).max()
+    dmin = c["sod"] - math.hypot(0.5 * c["nx"] * c["vox"], 0.5 * c["nz"] * c["vox"])
+    if dmin <= 0:
+        return {}
+    half = int(math.ceil(ymm * c["sdd"] / dmin / c["dv"])) + 3
+    nvb = min(c["nv"], 2 * half + c["nv"] % 2)
+    r0 = (c["nv"] - nvb) // 2
+    ijk = np.stack([rng.integers(0, c["nx"], nvox), rng.choice(ys, nvox), rng.integers(0, c["nz"], nvox)], 1)
+    t0 = time.perf_counter()
+    p = O.fdk_weight(raw_rows(r0, r0 + nvb), c["sdd"], c["du"], c["dv"])
+    q = O.filter_rows(p.reshape(-1, c["nu"]), c["filter"]).reshape(p.shape)
+    del p
+    ref = O.bp_cone_points(q, c, ijk)
+    clip = ijk[:, 1] < c["nz"]  # the reference's clip extent (y-slices below z_size)
+    ref[clip] = np.maximum(ref[clip], 0.0)
+    return {"ijk": ijk, "ref": ref, "rows": (r0, r0 + nvb), "seconds": time.perf_counter() - t0,
+            "slices": [int(y) for y in ys]}
+
+
+def sample_error(got, ref) -> dict:
+    import numpy as np
+    d = np.asarray(got, np.float64) - ref
+    return {"rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref)), "max_abs": float(np.abs(d).max())}
 
 
 def cpu_sample(c: dict, proj_views, view_ids, target_s: float) -> dict:
@@ -568,6 +610,15 @@ def main() -> None:
         torch.cuda.empty_cache()
 
     accuracy = {}
+    if rank == 0 and world == 1 and args.shard != "slabs" and args.oracle_voxels > 0:
+        chk = oracle_sample(c, lambda r0, r1: pristine[:, r0:r1, :].cpu().numpy(), args.oracle_voxels)
+        if chk:
+            ix, iy, iz = (torch.as_tensor(chk["ijk"][:, i], device=dev) for i in range(3))
+            for form, vol in vols.items():
+                accuracy[f"{form}_vs_fp64_oracle"] = sample_error(vol[iz, iy, ix].double().cpu().numpy(), chk["ref"])
+            accuracy["oracle_sample"] = (f"{len(chk['ref'])} seeded voxels in y-slices {chk['slices']}, each "
+                                         f"backprojected in FP64 from detector rows {chk['rows'][0]}..{chk['rows'][1] - 1} "
+                                         f"weighted and filtered in FP64 ({chk['seconds']:.0f} s on the host)")
     if "chosen" in vols and "plain" in vols:
         a, b = vols["chosen"].double(), vols["plain"].double()
         accuracy["chosen_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
