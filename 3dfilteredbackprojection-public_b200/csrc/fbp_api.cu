@@ -252,7 +252,7 @@ int filter_stack(fbp_context* ctx, Stack& s, int filter_type) {
   if (n < s.u || (n & (n - 1)))
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "padded length must be a power of two >= the row width");
   FBP_TRY(fbp::ensure_filter_tables(ctx, n, filter_type));
-  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  const bool mixed = ctx->precision != FBP_PRECISION_FP32;
   int impl = ctx->filter_impl;
   if (impl == FBP_FILTER_IMPL_AUTO)
     impl = (mixed && fbp::toeplitz_supported(s.u)) ? FBP_FILTER_IMPL_TOEPLITZ : FBP_FILTER_IMPL_FFT;
@@ -340,7 +340,7 @@ fbp::BPGeom cone_geom(const Stack& s, float sod, float odd, float det_w, float v
 // and keeps the fastest for that geometry, form and stack layout.
 int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, bool mixed, int* variant) {
   const double key[21] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
-                          (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz, (double)mixed,
+                          (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz, (double)ctx->precision,
                           (double)(s.filtered ? s.filt_layout : -1), (double)g.row_off, (double)g.nv_total,
                           (double)g.y_off, (double)g.ny_total, (double)s.sinogram};
   for (const auto& t : ctx->tuned)
@@ -422,7 +422,7 @@ int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
   FBP_TRY(flush_pending(ctx, s));
   FBP_TRY(ensure_volume(ctx, g.nx, g.ny, g.nz, false));
   const int ylim = ctx->clip_after_bp ? clip_limit : 0;
-  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  const bool mixed = ctx->precision != FBP_PRECISION_FP32;
   if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && g.ny > 1) {
     int variant = FBP_BACKPROJECTOR_AUTO;
     int rc = autotune_backprojector(ctx, s, g, mixed, &variant);
@@ -524,9 +524,9 @@ int make_tensor_map_2d_bf16_sw128(fbp_context* ctx, CUtensorMap* map, void* base
 }
 
 int prepare_packed(fbp_context* ctx, Stack& s, int layout) {
-  const bool quad = layout == kLayoutQuadG16;
+  const bool quad = fbp::is_quad_layout(layout);
   const int fpitch = quad ? s.u + 1 : round_up(s.u, 4);
-  const size_t need = quad ? (size_t)(s.n / 4) * (s.v + 1) * (size_t)(s.u + 1) * 32
+  const size_t need = quad ? (size_t)(s.n / 4) * (s.v + 1) * (size_t)(s.u + 1) * Stack::elem_bytes(layout)
                            : (size_t)fpitch * s.filt_rows() * Stack::elem_bytes(layout);
   if (!s.filt || s.filt_bytes < need) {
     cudaFree(s.filt);
@@ -544,8 +544,10 @@ int prepare_packed(fbp_context* ctx, Stack& s, int layout) {
     s.scale_cap = s.n;
   }
   float* scale = s.inv_scale + s.n;
-  // the four-term difference of the gradient layout is at most 4 max|value|
-  if (int rc = launch_view_scales(ctx, rowset_of(s), quad ? 8192.f : 32768.f, scale, s.inv_scale)) return rc;
+  // the four-term difference of the gradient layout is at most 4 max|value|;
+  // the 24-bit layout keeps the FP32 exponent and needs no scale
+  if (layout != kLayoutQuadG24)
+    if (int rc = launch_view_scales(ctx, rowset_of(s), quad ? 8192.f : 32768.f, scale, s.inv_scale)) return rc;
   if (int rc = launch_pack(ctx, s, layout, s.filt, fpitch, scale)) return rc;
   s.filt_layout = layout;
   s.filt_pitch = fpitch;
@@ -656,7 +658,7 @@ int fbp_synchronize(fbp_context* ctx) {
 
 int fbp_set_precision(fbp_context* ctx, int precision) {
   FBP_CTX(ctx);
-  if (precision != FBP_PRECISION_FP32 && precision != FBP_PRECISION_MIXED)
+  if (precision != FBP_PRECISION_FP32 && precision != FBP_PRECISION_MIXED && precision != FBP_PRECISION_MIXED24)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown precision");
   ctx->precision = precision;
   return FBP_OK;
@@ -1238,7 +1240,7 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
     DeviceGuard guard(ctx->device);
     FBP_TRY(fbp::cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream"));
   }
-  const bool mixed = ctx->precision == FBP_PRECISION_MIXED;
+  const bool mixed = ctx->precision != FBP_PRECISION_FP32;
   std::vector<cudaEvent_t> done(slabs, nullptr);
   int rc = FBP_OK;
   const int saved_variant = ctx->bp_variant;

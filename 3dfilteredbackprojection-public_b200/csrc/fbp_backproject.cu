@@ -304,6 +304,16 @@ __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
   return unpack2(d);
 }
 
+// Value I (0..15) of a kLayoutQuadG24 element held in 12 words: its three
+// bytes sit at byte 3 I, and the float is rebuilt as (bytes << 8) | low byte.
+template <int I>
+__device__ __forceinline__ float dec24(const uint32_t (&w)[12]) {
+  constexpr int B = 3 * I, W = B >> 2, O = B & 3;
+  constexpr int W1 = W + 1 < 12 ? W + 1 : W;  // the last value needs no second word
+  constexpr unsigned sel = O | (O << 4) | ((O + 1) << 8) | ((O + 2) << 12);
+  return __uint_as_float(__byte_perm(w[W], w[W1], sel));
+}
+
 __device__ __forceinline__ uint4 lds_u4(uint32_t addr) {
   uint4 v;
   asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
@@ -581,8 +591,11 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   // two 16-byte loads per voxel step feed all four taps). The quads are
   // walked group-major, q = g + m K/4 for m = 0..3, so the slot of rotation
   // r, (m + r) mod 4, is a compile-time index in each of the four unrolled steps.
-  constexpr bool QG = LAYOUT == kLayoutQuadG16;
-  constexpr int ESZ = QG ? 32 : LAYOUT == kLayoutPair32 ? 8 : 4;
+  // QG24: the same with three 16-byte planes of 24-bit values and no scale.
+  constexpr bool QG24 = LAYOUT == kLayoutQuadG24;
+  constexpr bool QG = LAYOUT == kLayoutQuadG16 || QG24;
+  constexpr int ESZ = QG24 ? 48 : QG ? 32 : LAYOUT == kLayoutPair32 ? 8 : 4;
+  constexpr int NPL = QG24 ? 3 : 2;  // 16-byte planes per element row
   constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -802,17 +815,33 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
 #pragma unroll
           for (int r = 0; r < 4; ++r) Wr[r] = W * g.ws[r];
           // four bilinear taps from the 2 x 16 bytes of one element (slot of rotation r: (M + r) mod 4)
-          auto taps = [&](const uint4& L0, const uint4& L1, float fv, int j) {
-            const uint32_t wv[8] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w};
+          auto taps = [&](const uint4& L0, const uint4& L1, const uint4& L2, float fv, int j) {
             float A[4], G[4];
+            if constexpr (QG24) {
+              const uint32_t wv[12] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w, L2.x, L2.y, L2.z, L2.w};
+              // (A, G) = (a, b - a) + fu (c' - a, d - c' - b + a) for the slot of rotation r
+              auto slot = [&](auto slc, float& Ar, float& Gr) {
+                constexpr int SL = decltype(slc)::value;
+                const float2 ag = ffma2(make_float2(fu, fu), make_float2(dec24<4 * SL + 2>(wv), dec24<4 * SL + 3>(wv)),
+                                        make_float2(dec24<4 * SL>(wv), dec24<4 * SL + 1>(wv)));
+                Ar = ag.x;
+                Gr = ag.y;
+              };
+              slot(std::integral_constant<int, (M + 0) & 3>{}, A[0], G[0]);
+              slot(std::integral_constant<int, (M + 1) & 3>{}, A[1], G[1]);
+              slot(std::integral_constant<int, (M + 2) & 3>{}, A[2], G[2]);
+              slot(std::integral_constant<int, (M + 3) & 3>{}, A[3], G[3]);
+            } else {
+              const uint32_t wv[8] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w};
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const int sl = (M + r) & 3;
-              const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);      // (a, b - a)
-              const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);  // (c' - a, d - c' - b + a)
-              const float2 P = __half22float2(X1);
-              A[r] = fma_f16_f32(__low2half(fu2), __low2half(X2), P.x);
-              G[r] = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
+              for (int r = 0; r < 4; ++r) {
+                const int sl = (M + r) & 3;
+                const __half2 X1 = *reinterpret_cast<const __half2*>(&wv[2 * sl]);      // (a, b - a)
+                const __half2 X2 = *reinterpret_cast<const __half2*>(&wv[2 * sl + 1]);  // (c' - a, d - c' - b + a)
+                const float2 P = __half22float2(X1);
+                A[r] = fma_f16_f32(__low2half(fu2), __low2half(X2), P.x);
+                G[r] = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
+              }
             }
 #pragma unroll
             for (int pr = 0; pr < 2; ++pr) {
@@ -838,8 +867,10 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
               const float2 t2 = fadd2_rz(v2, magic2);
               const float2 fv2 = fsub2(v2, fsub2(t2, magic2));
               const uint32_t a0 = __float_as_uint(t2.x) * RB + c0, a1 = __float_as_uint(t2.y) * RB + c0;
-              taps(lds_u4(a0), lds_u4(a0 + plane), fv2.x, j);  // slots 0, 1 | slots 2, 3
-              taps(lds_u4(a1), lds_u4(a1 + plane), fv2.y, j + 1);
+              // slots 0, 1 | slots 2, 3 (QG24: the 48 bytes of the element)
+              const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+              taps(lds_u4(a0), lds_u4(a0 + plane), QG24 ? lds_u4(a0 + 2 * plane) : z4, fv2.x, j);
+              taps(lds_u4(a1), lds_u4(a1 + plane), QG24 ? lds_u4(a1 + 2 * plane) : z4, fv2.y, j + 1);
             }
           } else {
             // window not staged: read the elements from global memory (zero
@@ -853,13 +884,14 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
               const float t = __fadd_rz(v, kMagic);
               const float fv = v - (t - kMagic);
               const int row = g.e0 + (int)(__float_as_uint(t) - kMagicBits);
-              uint4 L0 = zero, L1 = zero;
+              uint4 L0 = zero, L1 = zero, L2 = zero;
               if (col_ok && row >= 0 && row < a.qg_rows) {
-                const uint4* p = a.qg + ((size_t)grp * a.qg_rows + row) * 2 * a.qg_pitch + col;
+                const uint4* p = a.qg + ((size_t)grp * a.qg_rows + row) * NPL * a.qg_pitch + col;
                 L0 = __ldg(p);
                 L1 = __ldg(p + a.qg_pitch);
+                if (QG24) L2 = __ldg(p + 2 * a.qg_pitch);
               }
-              taps(L0, L1, fv, j);
+              taps(L0, L1, L2, fv, j);
             }
           }
         } else {
@@ -1075,7 +1107,9 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
 
 template <int LAYOUT>
 cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
-  auto kern = kahan ? bp_quad_kernel<LAYOUT, 8, true> : bp_quad_kernel<LAYOUT, 8, false>;
+  auto kern = bp_quad_kernel<LAYOUT, 8, false>;
+  if constexpr (LAYOUT != kLayoutQuadG24)  // the 24-bit layout runs without compensation
+    if (kahan) kern = bp_quad_kernel<LAYOUT, 8, true>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   // all of L1 as shared memory, so that two CTAs of up to 113 KB share an SM
@@ -1095,6 +1129,8 @@ cudaError_t launch_quad(int layout, const BoxMaps& maps, const BPArgs& a, size_t
       return launch_quad_cfg<kLayoutPair16>(maps, a, smem, kahan, stream);
     case kLayoutQuadG16:
       return launch_quad_cfg<kLayoutQuadG16>(maps, a, smem, kahan, stream);
+    case kLayoutQuadG24:
+      return launch_quad_cfg<kLayoutQuadG24>(maps, a, smem, false, stream);
     default:
       return launch_quad_cfg<kLayoutRaw32>(maps, a, smem, kahan, stream);
   }
@@ -1117,7 +1153,10 @@ cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size
 
 int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed) {
   const double pi = 3.14159265358979323846;
-  const bool kahan = mixed;
+  // MIXED24: 24-bit views for the symmetric kernel (FP32 rows otherwise), no
+  // compensation (FP32 sums of FP32-precise taps, as the FP32 form)
+  const bool c24 = mixed && ctx->precision == FBP_PRECISION_MIXED24;
+  const bool kahan = mixed && !c24;
   // Four-fold symmetric path: square volume, views over one turn (or
   // 4m + 1 turns) with K % 4 == 0, an even number of 16-wide tiles per axis.
   const bool is2d = g.ny == 1;
@@ -1131,10 +1170,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
                      "the four-fold symmetric backprojector needs nx == nz (a multiple of 32), views % 4 == 0 and "
                      "views over one full turn");
-  // MIXED form over f32 rows: packed to FP16 for the selected kernel below
-  const bool packed = mixed && !st.filtered;
+  // MIXED forms over f32 rows: packed for the selected kernel below
+  const bool packed = mixed && !st.filtered && (quad || !c24);
   const int layout = st.filtered ? st.filt_layout
-                     : packed    ? (quad ? kLayoutQuadG16 : kLayoutPair16)
+                     : packed    ? (quad ? (c24 ? kLayoutQuadG24 : kLayoutQuadG16) : kLayoutPair16)
                                  : kLayoutRaw32;
   const int esize = Stack::elem_bytes(layout);
   BPArgs a{};
@@ -1166,8 +1205,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   }
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;
   // TMA: x * element size must be a multiple of 16 bytes (the interleaved
-  // layout's x counts 8-byte words, two per 16-byte plane element: always even)
-  a.align = layout == kLayoutQuadG16 ? 1 : layout == kLayoutPair32 ? 2 : 4;
+  // layouts' x counts 8-byte words, two per 16-byte plane element: always even)
+  a.align = is_quad_layout(layout) ? 1 : layout == kLayoutPair32 ? 2 : 4;
   a.sino_layout = st.sinogram ? 1 : 0;
   a.pair_rows = layout == kLayoutRaw32 ? 0 : 1;
   a.clip_ylimit = clip_ylimit;
@@ -1264,7 +1303,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   const int bu = (plan.box_u + a.align - 1) / a.align * a.align;
   // a pair element carries row v + 1 with it: one row less to stage
   const int bv = layout == kLayoutRaw32 ? plan.box_v : std::max(1, plan.box_v - 1);
-  if (layout != kLayoutQuadG16 && ((layout == kLayoutPair32 ? 2 * bu : bu) > 256 || bv > 256))
+  if (!is_quad_layout(layout) && ((layout == kLayoutPair32 ? 2 * bu : bu) > 256 || bv > 256))
     return set_error(ctx, FBP_ERR_UNSUPPORTED,
                      "detector footprint of a voxel tile exceeds the 256-element TMA box; geometry magnification "
                      "too large for the staged backprojector");
@@ -1283,7 +1322,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                                                               : (size_t)4 * 8 * 256 * sizeof(float);
     const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
     // the interleaved layout gathers windows that do not fit from global memory
-    const size_t entry = layout == kLayoutQuadG16 ? 0 : 4 * max_box;
+    const size_t entry = is_quad_layout(layout) ? 0 : 4 * max_box;
     if (entry > ring) {
       use_quad = false;  // the largest quad does not fit: generic path
       if (ctx->bp_variant == FBP_BACKPROJECTOR_SYMMETRIC)
@@ -1315,7 +1354,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
   a.resident = 2 * ctx->num_sms;  // symmetric kernel: two CTAs per SM
-  if (layout == kLayoutQuadG16) {
+  if (is_quad_layout(layout)) {
     a.qg = static_cast<const uint4*>(st.filt);
     a.qg_pitch = st.filt_pitch;
     a.qg_rows = st.v + 1;
@@ -1330,8 +1369,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   BoxMaps maps;
   // interleaved layout: boxes of at most 128 x 256 elements (TMA: 256 words per
   // box row) and at most the ring; larger windows are gathered directly
-  const int mbu = layout == kLayoutQuadG16 ? std::min(bu, 128) : bu;
-  const int mbv = layout == kLayoutQuadG16 ? std::min(bv, std::max(1, (int)(a.box_bytes / (32 * mbu)))) : bv;
+  const int mbu = is_quad_layout(layout) ? std::min(bu, 128) : bu;
+  const int mbv = is_quad_layout(layout) ? std::min(bv, std::max(1, (int)(a.box_bytes / (esize * mbu)))) : bv;
   for (int i = 0; i < kNW; ++i) {
     const int w = (mbu * (i + 1) + kNW - 1) / kNW;
     maps.w[i] = std::max(a.align, (w + a.align - 1) / a.align * a.align);
@@ -1341,10 +1380,11 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   maps.h[kNH - 1] = mbv;
   for (int i = 0; i < kNW; ++i)
     for (int j = 0; j < kNH; ++j) {
-      if (layout == kLayoutQuadG16) {  // [group][element row][plane][element column][2 x 8 bytes]
-        const uint64_t d4[4] = {2ull * pitch_el, 2, rows_v, (uint64_t)st.n / 4};
-        const uint64_t s4[3] = {16ull * pitch_el, 32ull * pitch_el, 32ull * pitch_el * rows_v};
-        const uint32_t b4[4] = {2u * maps.w[i], 2, (uint32_t)maps.h[j], 1};
+      if (is_quad_layout(layout)) {  // [group][element row][plane][element column][2 x 8 bytes]
+        const uint32_t planes = (uint32_t)esize / 16;
+        const uint64_t d4[4] = {2ull * pitch_el, planes, rows_v, (uint64_t)st.n / 4};
+        const uint64_t s4[3] = {16ull * pitch_el, (uint64_t)esize * pitch_el, (uint64_t)esize * pitch_el * rows_v};
+        const uint32_t b4[4] = {2u * maps.w[i], planes, (uint32_t)maps.h[j], 1};
         if (int rc = make_tensor_map_4d(ctx, &maps.map[i * kNH + j], CU_TENSOR_MAP_DATA_TYPE_UINT64,
                                         const_cast<void*>(base), d4, s4, b4))
           return rc;

@@ -288,6 +288,70 @@ __global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, i
   }
 }
 
+// 24-bit store of an FP32 value for kLayoutQuadG24: the top three bytes S of
+// a stored value are read back as the float with bits (S << 8) | (S & 0xff).
+// That map is monotonic in S, so the nearest of the three candidates around
+// the truncation x >> 8 is the nearest representable value (ties to the
+// lower magnitude); the sign byte is carried along unchanged.
+__device__ __forceinline__ uint32_t store24(float x) {
+  const uint32_t b = __float_as_uint(x), sign = b & 0x80000000u, mag = b & 0x7fffffffu;
+  const uint32_t t = mag >> 8;
+  uint32_t best = t, err = 0xffffffffu;
+#pragma unroll
+  for (int d = -1; d <= 1; ++d) {
+    const uint32_t s = t + d;
+    if ((d < 0 && t == 0) || s > 0x7fffffu) continue;
+    const uint32_t back = (s << 8) | (s & 0xffu);
+    const uint32_t e = back > mag ? back - mag : mag - back;
+    if (e < err) {
+      err = e;
+      best = s;
+    }
+  }
+  return (sign >> 8) | best;  // 24 bits: sign, exponent, 15 significand bits
+}
+
+// f32 rows -> kLayoutQuadG24: one thread per (group g, element row e, element
+// column s); the 16 values (slot-major: a, b - a, c' - a, d - c' - b + a) are
+// stored as 3-byte little-endian fields of 12 words, written as three
+// 16-byte plane entries.
+__global__ void pack_quadg24_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
+                                    uint4* out) {
+  const int Q = n_views >> 2, P = m + 1;
+  const long long total = (long long)Q * (n_v + 1) * P;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long ge = t / P;
+    const int sc = (int)(t - ge * P);
+    const int g = (int)(ge / (n_v + 1)), e = (int)(ge - (long long)g * (n_v + 1));
+    const int c = sc - 1;
+    uint32_t w[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) w[i] = 0u;
+#pragma unroll
+    for (int slot = 0; slot < 4; ++slot) {
+      const int view = g + slot * Q;
+      auto at = [&](int iv, int iu) -> float {
+        if (iv < 0 || iv >= n_v || iu < 0 || iu >= m) return 0.f;
+        const long long r = sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv;
+        return src[r * spitch + iu];
+      };
+      const float pa = at(e - 1, c), pb = at(e, c), pc = at(e - 1, c + 1), pd = at(e, c + 1);
+      const float val[4] = {pa, pb - pa, pc - pa, (pd - pc) - (pb - pa)};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t s24 = store24(val[q]);
+        const int byte = 3 * (4 * slot + q), wi = byte >> 2, sh = 8 * (byte & 3);
+        w[wi] |= s24 << sh;
+        if (sh > 8) w[wi + 1] |= s24 >> (32 - sh);
+      }
+    }
+    out[(3 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
+    out[(3 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
+    out[(3 * ge + 2) * P + sc] = make_uint4(w[8], w[9], w[10], w[11]);
+  }
+}
+
 // Natural-order complex FFT of rows (FFFT::fft_radix2 / inverse_fft_radix2,
 // FastFourierTransformGPU.cpp:3-36): inverse = conj, FFT, conj, divide by n.
 __global__ void __launch_bounds__(256) fft_rows_kernel(float2* data, int n, int log2n, int rows,
@@ -468,6 +532,13 @@ int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long lo
     pack_quadg16_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
                                                                             view_scale, static_cast<uint4*>(out));
     return launched(ctx, "pack_quadg16_kernel");
+  }
+  if (layout == kLayoutQuadG24) {
+    if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
+    const long long total = (long long)(s.n / 4) * (s.v + 1) * (s.u + 1);
+    pack_quadg24_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
+                                                                            static_cast<uint4*>(out));
+    return launched(ctx, "pack_quadg24_kernel");
   }
   return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown packed layout");
 }

@@ -39,7 +39,16 @@ enum FiltLayout : int {
   // 16 bytes per column), so neighbouring columns are 16 bytes apart; a
   // bilinear tap is a + fu (c' - a) + fv ((b - a) + fu (...)).
   kLayoutQuadG16 = 3,
+  // The same four-view gradient quantities (MIXED24 form) as 24-bit values:
+  // an FP32 whose low byte is dropped on store and rebuilt on load as a copy
+  // of its lowest stored byte; the pack picks the stored value whose rebuilt
+  // float is nearest, so the error is that of rounding to 16 significant
+  // bits. No scale (the FP32 exponent is kept). 4 slots x 4 values x 3 bytes
+  // = 48 bytes per element, three 16-byte planes per element row.
+  kLayoutQuadG24 = 4,
 };
+
+constexpr bool is_quad_layout(int layout) { return layout == kLayoutQuadG16 || layout == kLayoutQuadG24; }
 
 // A stack of detector rows. Projections are [view][v][u] (rows ordered view
 // major), sinograms [v][view][u] (rows ordered v major). Rows of u samples
@@ -71,7 +80,7 @@ struct Stack {
   size_t rows() const { return (size_t)v * n; }
   size_t bytes32() const { return (size_t)pitch * rows() * sizeof(float); }
   static int elem_bytes(int layout) {
-    return layout == kLayoutQuadG16 ? 32 : layout == kLayoutPair32 ? 8 : 4;
+    return layout == kLayoutQuadG24 ? 48 : layout == kLayoutQuadG16 ? 32 : layout == kLayoutPair32 ? 8 : 4;
   }
   // element rows of the filtered buffer (pair layouts carry one extra row per view)
   size_t filt_rows() const { return (size_t)(v + 1) * n; }
@@ -193,8 +202,9 @@ int launch_elementwise_pre(fbp_context* ctx, const RowSet& rs);  // weight / log
 // Per-view scales for FP16 storage: scale = largest power of two with
 // scale * max|row value of the view| <= limit; inv = 1 / scale.
 int launch_view_scales(fbp_context* ctx, const RowSet& rs, float limit, float* view_scale, float* inv_scale);
-// Pack the stack's f32 rows into an FP16 backprojector layout (kLayoutPair16
-// with row pitch `pitch` elements, or kLayoutQuadG16) using per-view scales.
+// Pack the stack's f32 rows into a compact backprojector layout: kLayoutPair16
+// with row pitch `pitch` elements or kLayoutQuadG16 (FP16 with the per-view
+// scales view_scale), or kLayoutQuadG24 (24-bit, no scale).
 int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long long pitch, const float* view_scale);
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse);
 int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift);

@@ -59,8 +59,11 @@ size_t estimate_bytes(const fbp_request& r) {
   const size_t cols4 = (size_t)(r.det_cols + 3) / 4 * 4;
   if (r.kind == FBP_JOB_CONE) {
     const size_t stack = cols4 * r.det_rows * r.views * 4;
-    const size_t packed = r.precision == FBP_PRECISION_MIXED ? (size_t)r.views * (r.det_rows + 1) * (r.det_cols + 1) * 8
-                                                             : cols4 * (r.det_rows + 1) * r.views * 8;
+    // packed views: FP16 quads 8 bytes per sample, 24-bit quads 12, FP32 pairs 8
+    const size_t per = r.precision == FBP_PRECISION_MIXED24 ? 12 : 8;
+    const size_t packed = r.precision != FBP_PRECISION_FP32
+                              ? (size_t)r.views * (r.det_rows + 1) * (r.det_cols + 1) * per
+                              : cols4 * (r.det_rows + 1) * r.views * 8;
     const size_t vol = (size_t)r.vol_h * r.vol_v * r.vol_h * 4;
     const size_t split = std::min<size_t>((size_t)r.det_rows * r.views, 65536) * (cols4 + 64) * 4;
     return stack + packed + vol + split + (64u << 20);

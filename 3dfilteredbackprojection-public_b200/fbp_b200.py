@@ -47,6 +47,7 @@ class FilterType(enum.IntEnum):
 class Precision(enum.IntEnum):
     FP32 = 0
     MIXED = 1
+    MIXED24 = 2
 
 
 class Backprojector(enum.IntEnum):
@@ -366,7 +367,7 @@ class FBP3D:
         """Kernel, staged layout and window box of the last backprojection."""
         v, l, bu, bv, ny = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
         self.ctx.call("fbp_last_backprojection", C.byref(v), C.byref(l), C.byref(bu), C.byref(bv), C.byref(ny))
-        names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16"}
+        names = {0: "rows32", 1: "pairs32", 2: "pairs16", 3: "quads16", 4: "quads24"}
         kernels = {Backprojector.SYMMETRIC: "symmetric", Backprojector.GENERIC_Y8: "generic_y8"}
         return {"kernel": kernels.get(v.value, "generic"),
                 "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value), "tile_ny": ny.value}

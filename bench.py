@@ -42,6 +42,9 @@ sys.path.insert(0, str(PKG))
 METRIC = "FDK Gvox·view/s"
 FILTER_NAMES = {0: "ram_lak", 1: "shepp_logan", 2: "cosine", 3: "hann", 4: "ramp_sampled"}
 UNIT = "Gvox·view/s"
+# bench forms: precision, bytes per stored filtered sample, storage note
+FORMS = {"chosen": ("MIXED", 2, "f16 filtered views"), "chosen24": ("MIXED24", 3, "24-bit filtered views"),
+         "plain": ("FP32", 4, "f32")}
 
 
 def parse_args():
@@ -59,7 +62,8 @@ def parse_args():
     p.add_argument("--slots", type=int, default=5, help="serving: concurrent jobs of the chosen form")
     p.add_argument("--load", type=float, default=0.7,
                    help="serving: Poisson arrival rate as a fraction of the plain one-at-a-time capacity")
-    p.add_argument("--forms", default="chosen,plain", help="comma list of chosen,plain")
+    p.add_argument("--forms", default="chosen,chosen24,plain", help="comma list of " + ",".join(FORMS))
+    p.add_argument("--head", default="chosen", choices=list(FORMS), help="form of the headline value")
     p.add_argument("--shard", choices=["replicas", "slabs"], default="replicas",
                    help="N>1: replicas = one independent volume per rank (weak scaling); slabs = one volume "
                         "split into y-slabs, each rank holding its detector row band (strong scaling)")
@@ -528,7 +532,7 @@ def main() -> None:
     def make_solver(form: str):
         s = F.FBP3D(local_rank)
         s.set_stream(stream)
-        s.set_precision(F.Precision.MIXED if form == "chosen" else F.Precision.FP32)
+        s.set_precision(getattr(F.Precision, FORMS[form][0]))
         s.set_clip_after_backprojection(True)
         if args.backprojector == "tuned":
             s.set_autotune(True)
@@ -597,13 +601,14 @@ def main() -> None:
 
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     res, vols = {}, {}
+    smem_bw = None
     for form in forms:
         s = make_solver(form)
         res[form] = timed(s, pristine)
         res[form]["kernel"] = s.last_backprojection()
         vols[form] = torch.empty((c["nz"], slab_ny, c["nx"]), dtype=torch.float32, device=dev)
         s.read_volume(vols[form])
-        if form == "chosen":
+        if smem_bw is None:
             smem_bw = s.measure_smem_bandwidth()
         s.ctx.close()
         del s
@@ -619,17 +624,17 @@ def main() -> None:
             accuracy["oracle_sample"] = (f"{len(chk['ref'])} seeded voxels in y-slices {chk['slices']}, each "
                                          f"backprojected in FP64 from detector rows {chk['rows'][0]}..{chk['rows'][1] - 1} "
                                          f"weighted and filtered in FP64 ({chk['seconds']:.0f} s on the host)")
-    if "chosen" in vols and "plain" in vols:
-        a, b = vols["chosen"].double(), vols["plain"].double()
-        accuracy["chosen_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
-        accuracy["chosen_vs_plain_max_abs"] = float((a - b).abs().max())
+    for form in [f for f in vols if f != "plain" and "plain" in vols]:
+        a, b = vols[form].double(), vols["plain"].double()
+        accuracy[f"{form}_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        accuracy[f"{form}_vs_plain_max_abs"] = float((a - b).abs().max())
         del a, b
     vols.clear()
     torch.cuda.empty_cache()
 
     # ---- end to end through the C ABI with pinned host buffers (chosen form)
     e2e = None
-    head = "chosen" if "chosen" in res else forms[0]
+    head = args.head if args.head in res else forms[0]
     if not args.no_e2e:
         host_proj = torch.empty(tuple(pristine.shape), dtype=torch.float32, pin_memory=True)
         host_proj.copy_(pristine)
@@ -647,7 +652,7 @@ def main() -> None:
     h = res[head]
     value = job_units / (h["ms"] * 1e-3) / 1e9
     # roofline of the dominant kernel (the backprojector)
-    esize = 2 if head == "chosen" else 4
+    esize = FORMS[head][1]
     bp_s = h["bp_ms"] * 1e-3
     band_rows = slab[3] - slab[2]
     local_units = c["nx"] * slab_ny * c["nz"] * c["nviews"]  # this rank's updates
@@ -664,7 +669,7 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True,
         "scaling": "strong" if args.shard == "slabs" else "weak",
-        "vs_baseline": None, "dtype": "f32", "storage_dtype": "f16 filtered views" if head == "chosen" else "f32",
+        "vs_baseline": None, "dtype": "f32", "storage_dtype": FORMS[head][2],
         "data": data_note(c),
         "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "voxel_mm": c["vox"],
                    "views": c["nviews"], "detector": [c["nu"], c["nv"]], "pitch_mm": c["du"],
@@ -679,8 +684,8 @@ def main() -> None:
                      "note": "backprojector algorithmic HBM bytes (filtered views read once + volume written "
                              "once); the kernel is bound by shared-memory gathers, see roofline_smem"},
         "roofline_smem": {"bound": "smem", "achieved": gather_bytes / bp_s / 1e12,
-                          "peak": smem_bw / 1e12 if "chosen" in res else None, "unit": "TB/s",
-                          "frac": (gather_bytes / bp_s) / smem_bw if "chosen" in res else None,
+                          "peak": smem_bw / 1e12, "unit": "TB/s",
+                          "frac": (gather_bytes / bp_s) / smem_bw,
                           "bytes_per_update": 4 * esize},
         "gpu_launches": h["launches"],
         "clocks": h["clocks"],
@@ -690,8 +695,8 @@ def main() -> None:
         line[f"form_{form}"] = {"value": job_units / (r["ms"] * 1e-3) / 1e9, "ms_per_step": r["ms"],
                                 "filter_ms": r["filter_ms"], "backprojection_ms": r["bp_ms"],
                                 "gpu_launches": r["launches"], "clocks": r["clocks"], "backprojector": r["kernel"]}
-    if "chosen" in res and "plain" in res:
-        line["chosen_over_plain"] = res["plain"]["ms"] / res["chosen"]["ms"]
+    for form in [f for f in res if f != "plain" and "plain" in res]:
+        line[f"{form}_over_plain"] = res["plain"]["ms"] / res[form]["ms"]
     if e2e is not None:
         line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

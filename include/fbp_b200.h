@@ -50,8 +50,15 @@ extern "C" {
 /* MIXED: split-BF16 tensor-core Toeplitz filter (FP32 accumulate), FP16    */
 /*        filtered views with a per-view power-of-two scale, Kahan-          */
 /*        compensated FP32 accumulation over view chunks.                    */
+/* MIXED24: split-BF16 Toeplitz filter, 24-bit filtered views (FP32 with   */
+/*        the low byte dropped: 16 significant bits, FP32 exponent) for the  */
+/*        four-fold symmetric backprojector (FP32 views otherwise), FP32     */
+/*        accumulation. 12 bytes of shared-memory gathers per update (FP32   */
+/*        16, MIXED 8), for inputs whose noise leaves FP16 storage short of  */
+/*        1e-4 relative error.                                              */
 #define FBP_PRECISION_FP32 0
 #define FBP_PRECISION_MIXED 1
+#define FBP_PRECISION_MIXED24 2
 
 /* ---- filter implementations ---------------------------------------------- */
 #define FBP_FILTER_IMPL_AUTO 0     /* FFT for FP32, Toeplitz GEMM for MIXED */
@@ -125,7 +132,8 @@ int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
 /* What the last backprojection ran (no counterpart in the reference, whose
  * backprojection is one fixed shader): *variant = FBP_BACKPROJECTOR_GENERIC,
  * _GENERIC_Y8 or _SYMMETRIC; *layout = staged view layout (0 FP32 rows,
- * 1 FP32 row pairs, 2 FP16 row pairs, 3 FP16 four-view gradient quads);
+ * 1 FP32 row pairs, 2 FP16 row pairs, 3 FP16 four-view gradient quads,
+ * 4 24-bit four-view gradient quads);
  * *box_u x *box_v = largest staged detector window in elements; *tile_ny =
  * voxels per thread along y. Any output pointer may be NULL. FBP_ERR_STATE
  * before the first backprojection. */

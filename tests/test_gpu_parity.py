@@ -3,6 +3,7 @@
 Tolerances (relative RMSE = ||x - oracle|| / ||oracle||):
   FP32 form:   1e-5 for whole reconstructions, 1e-6 for filtered rows
   MIXED form:  1e-4 (FP16 filtered views with per-view scale, Kahan sums)
+  MIXED24:     3e-5 (24-bit filtered views, FP32 sums)
 """
 from __future__ import annotations
 
@@ -18,6 +19,8 @@ pytestmark = pytest.mark.gpu
 TOL_FP32 = 1e-5
 TOL_ROWS = 1e-6
 TOL_MIXED = 1e-4
+# MIXED24: split-BF16 filter + 24-bit views (16 significant bits), FP32 sums
+TOL_MIXED24 = 3e-5
 # tensor-core filter: split-BF16 operands (hi + lo) with FP32 accumulation;
 # a numpy emulation of the same split gives 0.7e-5 .. 1.3e-5 on these rows
 TOL_TOEPLITZ_ROWS = 5e-5
@@ -280,6 +283,64 @@ def test_mixed_precision_cone(fbp, oracle, phantoms):
     err = relative_rmse(got, ref)
     print(f"mixed cone128 rel RMSE {err:.3e}")
     assert err < TOL_MIXED
+
+
+@pytest.mark.parametrize("square", [True, False])
+def test_mixed24_cone(fbp, oracle, phantoms, square):
+    """MIXED24 through the symmetric kernel (24-bit interleaved quads) and, for a
+    volume the symmetric kernel does not take, the generic kernel on FP32 rows."""
+    if square:
+        c, proj = _cone_case(phantoms, oracle, 2)
+    else:
+        c, proj = _sym_case(oracle, nviews=96, n=50)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED24)
+    got = _gpu_fdk(s, c, proj, 0)
+    info = s.last_backprojection()
+    err = relative_rmse(got, oracle.fdk(proj, c, 0))
+    print(f"mixed24 {c['nx']}^2 x {c['ny']}: {info} rel RMSE {err:.3e}")
+    assert info["layout"] == ("quads24" if square else "rows32")
+    assert err < TOL_MIXED24
+
+
+def test_noisy_views_fp16_short_of_1e4_24bit_within(fbp, oracle, phantoms):
+    """Noisy projections (Poisson I0 = 5e4 as on the large workload) with a
+    Hann ramp: the reconstruction is noise-dominated, and FP16 view storage
+    leaves it near its storage floor while 24-bit views stay FP32-class."""
+    c, proj = _cone_case(phantoms, oracle, 2)
+    c = dict(c, filter=3)
+    proj = phantoms.poisson_log(proj, 5e4, np.random.default_rng(9))
+    ref = oracle.fdk(proj, c, 3)
+    errs = {}
+    for prec in ("MIXED", "MIXED24"):
+        s = fbp.FBP3D(0)
+        s.set_clip_after_backprojection(False)
+        s.set_precision(getattr(fbp.Precision, prec))
+        errs[prec] = relative_rmse(_gpu_fdk(s, c, proj, 3), ref)
+    print(f"noisy 128^3 Hann: {errs}")
+    assert errs["MIXED24"] < TOL_MIXED24
+    assert errs["MIXED24"] < errs["MIXED"] / 3
+
+
+def test_mixed24_unstaged_windows(fbp, oracle):
+    """High magnification: 24-bit windows too large for the ring are gathered
+    from global memory (three planes per element row)."""
+    c = dict(sod=120.0, sdd=360.0, du=1.0, dv=1.0, span=2 * math.pi, offset=0.1, nu=256, nv=256,
+             nviews=192, nx=64, ny=40, nz=64, vox=1.0)
+    from phantoms import random_ellipsoids
+    E = random_ellipsoids(np.random.default_rng(37), 10, 0.5 * c["nx"] * c["vox"])
+    proj = oracle.project_ellipsoids_cone(E, c)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED24)
+    s.set_backprojector(fbp.Backprojector.SYMMETRIC)
+    got = _gpu_fdk(s, c, proj, 0)
+    info = s.last_backprojection()
+    err = relative_rmse(got, oracle.fdk(proj, c, 0))
+    print(f"high magnification MIXED24: {info} rel RMSE {err:.3e}")
+    assert info["kernel"] == "symmetric" and info["layout"] == "quads24"
+    assert err < TOL_MIXED24
 
 
 @pytest.mark.parametrize("impl", ["FFT", "TOEPLITZ"])
@@ -594,7 +655,7 @@ def test_write_volume_slices(fbp, oracle, tmp_path):
 
 
 # ------------------------------------------------------- y-slab sharding (e)
-@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+@pytest.mark.parametrize("precision", ["FP32", "MIXED", "MIXED24"])
 def test_slab_sharding_matches_whole_volume(fbp, oracle, phantoms, precision):
     """The ranks of a 3-slab plan, run one after another on one GPU: each
     context holds only its detector row band and its y-slab; the slabs put
@@ -621,7 +682,7 @@ def test_slab_sharding_matches_whole_volume(fbp, oracle, phantoms, precision):
         parts.append(part)
     vol = np.concatenate(parts, axis=1)
     ref = oracle.fdk(proj, c, 0)
-    tol = TOL_FP32 if precision == "FP32" else TOL_MIXED
+    tol = {"FP32": TOL_FP32, "MIXED": TOL_MIXED, "MIXED24": TOL_MIXED24}[precision]
     print(f"slabs {plan}: vs whole {relative_rmse(vol, whole):.2e}, vs oracle {relative_rmse(vol, ref):.2e}")
     assert relative_rmse(vol, whole) < tol
     assert relative_rmse(vol, ref) < tol
@@ -810,7 +871,7 @@ def test_forward_projection_agrees_with_analytic_line_integrals(fbp, oracle):
 
 
 # ------------------------------------------------ streamed reconstruction to host
-@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+@pytest.mark.parametrize("precision", ["FP32", "MIXED", "MIXED24"])
 def test_reconstruct_to_host_matches_the_stepwise_calls(fbp, oracle, phantoms, precision):
     """Upload, weights, filter and slab-wise backprojection with the readback of
     each slab overlapping the next: the same volume as the step-by-step calls
