@@ -68,3 +68,34 @@ def test_twentyfour_bit_format_meets_1e4(taps):
     err = _rel(t, sum(w * f24(x) for w, x in zip(t["wts"], t["corners"])))
     print("24-bit corners", err)
     assert err < 2e-5
+
+
+def test_24bit_store_rule_picks_the_nearest_value():
+    """The 24-bit view format stores the top three bytes S of an FP32 and reads
+    back the float with bits (S << 8) | (S & 0xff); the pack keeps the best of
+    the candidates t - 1, t, t + 1 around the truncation t = bits >> 8. A
+    brute-force search over t - 3 .. t + 3 finds nothing nearer, and the
+    rebuilt values err like rounding to 16 significant bits (|err| <= 2^-15
+    relative, mean ~0)."""
+    rng = np.random.default_rng(11)
+    x = (rng.standard_normal(400_000) * np.exp(rng.uniform(-20, 20, 400_000))).astype(np.float32)
+    mag = x.view(np.uint32).astype(np.int64) & 0x7FFFFFFF
+    t = mag >> 8
+
+    def back(s):
+        return (s << 8) | (s & 0xFF)
+
+    def pick(lo, hi):
+        cand = np.stack([t + d for d in range(lo, hi + 1)])
+        ok = (cand >= 0) & (cand <= 0x7FFFFF)
+        err = np.where(ok, np.abs(back(np.clip(cand, 0, 0x7FFFFF)) - mag), np.iinfo(np.int64).max)
+        return np.take_along_axis(cand, np.argmin(err, axis=0)[None], 0)[0], err.min(axis=0)
+
+    s1, e1 = pick(-1, 1)
+    s3, e3 = pick(-3, 3)
+    assert np.array_equal(e1, e3)
+    sign = x.view(np.uint32).astype(np.int64) & 0x80000000
+    got = (sign | back(s1)).astype(np.uint32).view(np.float32).astype(np.float64)
+    rel = (got - x) / np.abs(x.astype(np.float64))
+    assert np.abs(rel).max() <= 2.0 ** -15
+    assert abs(rel.mean()) < 1e-7
