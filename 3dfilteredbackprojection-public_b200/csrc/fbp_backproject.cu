@@ -320,6 +320,13 @@ __device__ __forceinline__ uint4 lds_u4(uint32_t addr) {
   return v;
 }
 
+// Hardware approximate reciprocal (max 1 ulp error; D is a distance ratio near 1).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // FP16 x FP16 + FP32 with one rounding to FP32.
 __device__ __forceinline__ float fma_f16_f32(__half a, __half b, float c) {
   float d;
@@ -569,17 +576,22 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
 
 constexpr int kQuadEntries = 8;  // outstanding view-quads per CTA
 constexpr int kKahanQuads = 4;   // quads (16 views) per Kahan fold
-constexpr int kFoldQG = 32;      // quads per Kahan fold when the running sums live in shared memory
+constexpr int kFoldQG = 64;      // quads per Kahan fold when the running sums live in shared memory
 
-struct QuadCoef {
+// 16-byte aligned so that consumers read a record with vector loads
+struct alignas(16) QuadCoef {
   float Dx, Dz, D0, Nx, Nz, N0, Vx, Vz, V0;
   float ws[4];  // per-view extra weight of the four views (FP16 views: 1 / scale)
   int skip;
-  int box;      // staged window: width (elements) | rows << 16
-  int off;      // byte offset of the entry's first window in the ring
   int sub;      // bytes between the entry's four windows
   int direct;   // interleaved layout: window not staged, consumers gather it from global memory
   int u0, e0;   // direct: element column / element row of the window origin
+  // consumer constants of the window, formed once by the producer
+  uint32_t cbase;  // ring address of element column 0 minus kMagicBits element rows
+  uint32_t rb;     // bytes per staged element row
+  uint32_t plane;  // interleaved layout: bytes between the 16-byte planes of an element row
+  int bu2;         // last element column a tap may start at (box width - 2)
+  float vmax;      // exclusive bound on the window-local v of a tap
 };
 
 // 288 threads, two CTAs per SM: 9 warps each put 5 warps on some SM
@@ -645,6 +657,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
       bool skip = true, direct = false;
       qc.skip = 1;
+      qc.rb = 0;
       if (it < K) {
         ViewCoef vc;
         bool overflow = false, behind = false;
@@ -671,11 +684,16 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
 #pragma unroll
         for (int r = 0; r < 4; ++r) qc.ws[r] = a.inv_scale ? a.inv_scale[(k + r * Q) % K] : 1.0f;
         qc.skip = skip;
-        qc.box = direct ? (need_u | (rows << 16)) : (maps.w[wi] | (maps.h[hi] << 16));
+        // window: width (elements) and rows
+        const int BU = direct ? need_u : maps.w[wi], BV = direct ? rows : maps.h[hi];
         qc.sub = sub;
         qc.direct = direct;
         qc.u0 = u0 + 1;
         qc.e0 = v0 + a.pair_rows;
+        qc.rb = (uint32_t)(BU * ESZ);
+        qc.plane = (uint32_t)(BU * 16);
+        qc.bu2 = BU - 2;
+        qc.vmax = (float)(BV - kRowTail) - (float)(kSlack / 2);
       }
       const int nb = min(32, K - kb);
       for (int i = 0; i < nb; ++i) {
@@ -701,7 +719,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
         const int off = start % R;
         if (lane == i) {
-          qc.off = off;
+          qc.cbase = smem_u32(smem) + (uint32_t)off - kMagicBits * qc.rb;
           coef[e] = qc;
         }
         if (lane == 0) end_pos[e] = start + qneed;
@@ -778,7 +796,6 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         }
       }
   }
-  const uint32_t ring = smem_u32(smem);
   int e = 0;
   uint32_t ph = 0;
   bool bad = false, stop = false;
@@ -794,7 +811,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
     const QuadCoef g = coef[e];
     if (!g.skip) {
       const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
-      const float rD = __frcp_rn(D);
+      const float rD = rcp_approx(D);
       const float ul = fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)) * rD;
       const float vl = fmaf(g.Vx, fx, fmaf(g.Vz, fz, g.V0)) * rD;
       const float dvv = a.dvn * rD;
@@ -803,20 +820,18 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
       const int iu = (int)fuf;
       const float fu = ul - fuf;
       const float vlast = fmaf((float)(NY - 1), dvv, vl);
-      const int BU = g.box & 0xffff, BV = g.box >> 16;
-      const uint32_t RB = (uint32_t)(BU * ESZ);
-      const float vmax_ok = (float)(BV - kRowTail) - (float)(kSlack / 2);
-      if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
-        const uint32_t sub = (uint32_t)g.sub;
-        const uint32_t c0 = ring + (uint32_t)g.off + (uint32_t)(iu * (QG ? 16 : ESZ)) - kMagicBits * RB;
+      const uint32_t RB = g.rb;
+      if (iu >= 0 && iu <= g.bu2 && vl >= 0.f && vlast < g.vmax) {
+        const uint32_t c0 = g.cbase + (uint32_t)(iu * (QG ? 16 : ESZ));
         const __half2 fu2 = __float2half2_rn(fu);
         if constexpr (QG) {
           float Wr[4];
 #pragma unroll
           for (int r = 0; r < 4; ++r) Wr[r] = W * g.ws[r];
-          // four bilinear taps from the 2 x 16 bytes of one element (slot of rotation r: (M + r) mod 4)
-          auto taps = [&](const uint4& L0, const uint4& L1, const uint4& L2, float fv, int j) {
-            float A[4], G[4];
+          // (A, G) of the four rotations at one voxel from the 2 x 16 bytes of
+          // its element (slot of rotation r: (M + r) mod 4): A = u-lerp of row
+          // e - 1, G = u-lerp of the row difference
+          auto decode = [&](const uint4& L0, const uint4& L1, const uint4& L2, float (&A)[4], float (&G)[4]) {
             if constexpr (QG24) {
               const uint32_t wv[12] = {L0.x, L0.y, L0.z, L0.w, L1.x, L1.y, L1.z, L1.w, L2.x, L2.y, L2.z, L2.w};
               // (A, G) = (a, b - a) + fu (c' - a, d - c' - b + a) for the slot of rotation r
@@ -843,6 +858,9 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
                 G[r] = fma_f16_f32(__low2half(fu2), __high2half(X2), P.y);
               }
             }
+          };
+          // rotation pairs (0, 1), (2, 3) of one voxel: v-lerp and weighted sum as packed pairs
+          auto rot_pairs = [&](const float (&A)[4], const float (&G)[4], float fv, int j) {
 #pragma unroll
             for (int pr = 0; pr < 2; ++pr) {
               float& d0 = KAHAN ? part[KAHAN ? 2 * pr : 0][KAHAN ? j : 0] : acc[2 * pr][j];
@@ -855,7 +873,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
             }
           };
           if (!g.direct) {
-            const uint32_t plane = (uint32_t)BU * 16;
+            const uint32_t plane = g.plane;
             static_assert(NY % 2 == 0, "voxels stepped in pairs");
             const float2 magic2 = make_float2(kMagic, kMagic);
 #pragma unroll
@@ -869,8 +887,11 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
               const uint32_t a0 = __float_as_uint(t2.x) * RB + c0, a1 = __float_as_uint(t2.y) * RB + c0;
               // slots 0, 1 | slots 2, 3 (QG24: the 48 bytes of the element)
               const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
-              taps(lds_u4(a0), lds_u4(a0 + plane), QG24 ? lds_u4(a0 + 2 * plane) : z4, fv2.x, j);
-              taps(lds_u4(a1), lds_u4(a1 + plane), QG24 ? lds_u4(a1 + 2 * plane) : z4, fv2.y, j + 1);
+              float A0[4], G0[4];
+              decode(lds_u4(a0), lds_u4(a0 + plane), QG24 ? lds_u4(a0 + 2 * plane) : z4, A0, G0);
+              rot_pairs(A0, G0, fv2.x, j);
+              decode(lds_u4(a1), lds_u4(a1 + plane), QG24 ? lds_u4(a1 + 2 * plane) : z4, A0, G0);
+              rot_pairs(A0, G0, fv2.y, j + 1);
             }
           } else {
             // window not staged: read the elements from global memory (zero
@@ -891,10 +912,13 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
                 L1 = __ldg(p + a.qg_pitch);
                 if (QG24) L2 = __ldg(p + 2 * a.qg_pitch);
               }
-              taps(L0, L1, L2, fv, j);
+              float A[4], G[4];
+              decode(L0, L1, L2, A, G);
+              rot_pairs(A, G, fv, j);
             }
           }
         } else {
+          const uint32_t sub = (uint32_t)g.sub;
           float wa[4], wb[4], Wr[4];
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
@@ -946,8 +970,8 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   static_assert(kKahanQuads == 4 && kFoldQG % 4 == 0, "folds on whole groups of four quads");
   if constexpr (QG) {
     int kq = 0;
+    grp = g0;  // view group of quads q .. q + 3: (q / 4 + g0) mod K / 4, stepped
     for (int q = 0; q < K; q += 4) {
-      grp = ((q >> 2) + g0) % (K >> 2);
       step(std::integral_constant<int, 0>{});
       if (stop) break;
       step(std::integral_constant<int, 1>{});
@@ -960,6 +984,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         kq = 0;
         fold();
       }
+      if (++grp == Q) grp = 0;
     }
   } else {
     int kq = 0;
