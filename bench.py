@@ -13,7 +13,10 @@ is the chosen form (split-precision: FP16 filtered views with per-view scale,
 Kahan-compensated FP32 accumulation) with inputs resident in HBM; the plain
 FP32 form is reported beside it. `e2e` repeats the chosen form through the C
 ABI with pinned host buffers: the projection upload and the volume readback
-are inside the timed region. Multi-GPU runs (torchrun) reconstruct one
+are inside the timed region. The K reconstructions run from two host threads
+with one context and stream each, so one reconstruction's transfers overlap
+the other's kernels; `e2e.serial` is the same with one context, one call
+after another. Multi-GPU runs (torchrun) reconstruct one
 independent volume per rank (weak scaling, no collective on the data path);
 times are the max over ranks.
 
@@ -32,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 from pathlib import Path
 
@@ -529,9 +533,9 @@ def main() -> None:
 
     sod, odd, w, vw, rot = ga["sod"], ga["odd"], ga["detector_width"], ga["volume_width"], ga["full_rotation_count"]
 
-    def make_solver(form: str):
+    def make_solver(form: str, on_stream=None):
         s = F.FBP3D(local_rank)
-        s.set_stream(stream)
+        s.set_stream(stream if on_stream is None else on_stream)
         s.set_precision(getattr(F.Precision, FORMS[form][0]))
         s.set_clip_after_backprojection(True)
         if args.backprojector == "tuned":
@@ -599,6 +603,53 @@ def main() -> None:
         return dict(ms=ms, filter_ms=filt_ms, bp_ms=bp_ms, launches=launches, clocks=clk,
                     wall_ms=t_wall * 1e3 / args.steps)
 
+    def pipelined(solvers, src, dsts) -> dict:
+        """K reconstructions through e2e_step, alternating over the solvers from
+        one host thread each; the second thread starts one projection upload
+        later (the H2D time measured here) so the two uploads do not split the
+        link. Device-timed: events on the torch stream around the whole run,
+        after a device-wide synchronisation on both sides."""
+        for i in range(max(args.warmup, len(solvers))):
+            e2e_step(solvers[i % len(solvers)], src, dsts[i % len(solvers)])
+        probe = torch.empty(1 << 28, dtype=torch.float32, device=dev)  # 1 GiB
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flat = src.view(-1)[: probe.numel()]
+        h0.record()
+        probe.copy_(flat, non_blocking=True)
+        h1.record()
+        h1.synchronize()
+        delay_s = h0.elapsed_time(h1) * 1e-3 * (src.numel() / probe.numel())
+        del probe, flat
+        counts = [args.steps // len(solvers) + (1 if i < args.steps % len(solvers) else 0)
+                  for i in range(len(solvers))]
+        errors = []
+
+        def worker(i):
+            try:
+                if i:
+                    time.sleep(delay_s)
+                for _ in range(counts[i]):
+                    e2e_step(solvers[i], src, dsts[i])
+            except Exception as exc:  # re-raised on the main thread
+                errors.append(exc)
+
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        start.record()
+        threads = [threading.Thread(target=worker, args=(i,)) for i in range(len(solvers)) if counts[i]]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        torch.cuda.synchronize()
+        end.record()
+        end.synchronize()
+        barrier()
+        if errors:
+            raise errors[0]
+        return dict(ms=max_over_ranks(start.elapsed_time(end) / args.steps), delay_ms=delay_s * 1e3)
+
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     res, vols = {}, {}
     smem_bw = None
@@ -641,12 +692,27 @@ def main() -> None:
         host_vol = torch.empty((c["nz"], slab_ny, c["nx"]), dtype=torch.float32, pin_memory=True)
         s = make_solver(head)
         r = timed(s, host_proj, readback=host_vol, streamed=args.shard != "slabs")
-        s.ctx.close()
-        del s
         e2e = {"value": job_units / (r["ms"] * 1e-3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(sum_over_ranks(host_proj.numel() * 4)),
                "d2h_bytes_per_step": int(sum_over_ranks(host_vol.numel() * 4)),
                "ms_per_step": r["ms"]}
+        if args.shard != "slabs":
+            # the same calls from two host threads, each with its own context and
+            # stream: one reconstruction's upload and readback overlap the other's
+            # kernels (every step still moves its own inputs and volume)
+            host_vol2 = torch.empty_like(host_vol, pin_memory=True)
+            s2 = make_solver(head, torch.cuda.Stream(dev))
+            p = pipelined([s, s2], host_proj, [host_vol, host_vol2])
+            e2e = {"value": job_units / (p["ms"] * 1e-3) / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": e2e["h2d_bytes_per_step"], "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
+                   "ms_per_step": p["ms"], "contexts": 2, "launch_delay_ms": p["delay_ms"],
+                   "serial": {"value": e2e["value"], "ms_per_step": e2e["ms_per_step"]},
+                   "note": "fbp_reconstruct_fdk_to_host from two host threads with one context and stream each; "
+                           "serial: one context, one call after another"}
+            s2.ctx.close()
+            del s2, host_vol2
+        s.ctx.close()
+        del s
         del host_proj, host_vol
 
     h = res[head]
