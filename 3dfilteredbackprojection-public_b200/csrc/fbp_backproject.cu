@@ -292,10 +292,15 @@ __device__ __forceinline__ float2 unpack2(unsigned long long r) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
   return d;
 }
-// a + b per lane rounded toward zero, and a - b rounded to nearest (packed f32x2)
+// a + b per lane rounded toward zero or to nearest, and a - b rounded to nearest (packed f32x2)
 __device__ __forceinline__ float2 fadd2_rz(float2 a, float2 b) {
   unsigned long long d;
   asm("add.rz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+  return unpack2(d);
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
   return unpack2(d);
 }
 __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
@@ -876,12 +881,15 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
             const uint32_t plane = g.plane;
             static_assert(NY % 2 == 0, "voxels stepped in pairs");
             const float2 magic2 = make_float2(kMagic, kMagic);
+            // v of voxels j and j + 1, stepped by 2 dvv from (vl, vl + dvv): no
+            // per-pair constants (a few ulps of v from the repeated additions)
+            const float dv2 = 2.f * dvv;
+            const float2 step2 = make_float2(dv2, dv2);
+            float2 v2 = make_float2(vl, vl + dvv);
 #pragma unroll
             for (int j = 0; j < NY; j += 2) {
-              // v, floor and fraction of voxels j and j + 1 with packed FP32 ops
-              // (the same IEEE operations as the scalar form)
-              const float2 v2 = ffma2(make_float2((float)j, (float)(j + 1)), make_float2(dvv, dvv),
-                                      make_float2(vl, vl));
+              // floor and fraction of voxels j and j + 1 with packed FP32 ops
+              if (j) v2 = fadd2(v2, step2);
               const float2 t2 = fadd2_rz(v2, magic2);
               const float2 fv2 = fsub2(v2, fsub2(t2, magic2));
               const uint32_t a0 = __float_as_uint(t2.x) * RB + c0, a1 = __float_as_uint(t2.y) * RB + c0;
