@@ -149,6 +149,7 @@ int fbp_free_projections(fbp_context* ctx);
 int fbp_free_sinograms(fbp_context* ctx);
 int fbp_get_volume_size(const fbp_context* ctx, int* x, int* y, int* z);
 int fbp_get_projections_size(const fbp_context* ctx, int* u, int* v, int* count);
+int fbp_get_sinograms_size(const fbp_context* ctx, int* u, int* v, int* count); /* u x v detector, count views */
 
 /* ---- transfers --------------------------------------------------------------
  * `*_on_device` = 1: the pointer is device memory of ctx's device, else host
@@ -166,6 +167,13 @@ int fbp_store_projection(fbp_context* ctx, const float* src, int projection_inde
 int fbp_load_projection(fbp_context* ctx, int projection_index, float* dst, int dst_on_device);      /* FBP3D.cpp:706-716 */
 int fbp_store_sinogram(fbp_context* ctx, const float* src, int y_index, int src_on_device);           /* FBP3D.cpp:742-753 */
 int fbp_load_sinogram(fbp_context* ctx, int y_index, float* dst, int dst_on_device);                  /* FBP3D.cpp:730-740 */
+/* One projection [v][u] (view projection_index) gathered from / scattered into the
+ * sinogram stack [v][view][u]; read_projections_as_sinograms stores each file this way
+ * (FBP3D.cpp:167). */
+int fbp_load_projection_from_sinograms(fbp_context* ctx, int projection_index, float* dst,
+                                       int dst_on_device);                                             /* FBP3D.cpp:755-765 */
+int fbp_store_projection_to_sinograms(fbp_context* ctx, const float* src, int projection_index,
+                                      int src_on_device);                                              /* FBP3D.cpp:767-778 */
 /* Slices of the volume: x-slice is [z][y], y-slice [z][x], z-slice [y][x]
  * (FBP3D.cpp:639-704). */
 int fbp_load_volume_slice_x(fbp_context* ctx, int x_index, float* dst, int dst_on_device);
@@ -326,7 +334,10 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
  * sinogram [views][bins], image [rows][cols]; filtered in place. */
 /* Weight (fan: SDD/sqrt(SDD^2+u^2)) and filter every row; fan_sdd <= 0 means
  * parallel beam (no weight). Combines FBP2D::apply_filter on the shifted
- * spectrum with the surrounding FFFT calls (Mains/fbp_parallel2d_main.cpp:31-41). */
+ * spectrum with the surrounding FFFT calls (Mains/fbp_parallel2d_main.cpp:31-41).
+ * The context's filter implementation / precision choose the arithmetic as for
+ * the 3D stacks: the FP32 FFT, or (MIXED, MIXED24, or FBP_FILTER_IMPL_TOEPLITZ)
+ * the tcgen05 split-BF16 Toeplitz product, which needs 64 <= bins <= 8192. */
 int fbp2d_filter_sinogram(fbp_context* ctx, float* sinogram, int bins, int views, int filter_type,
                           float fan_sdd, float detector_width);
 /* The same filtering without a context and without allocating device memory,
@@ -337,10 +348,13 @@ int fbp2d_filter_sinogram(fbp_context* ctx, float* sinogram, int bins, int views
  * cudaStream_t (NULL: the legacy default stream); its tables live in an
  * 80 KiB file-scope device array, so padded_length (0: next power of two >=
  * bins) may be at most 4096 - longer rows are rejected with
- * FBP_ERR_UNSUPPORTED. The first call on a device looks up that array's
- * device address; make it before any stream capture. All calls share the
- * array: calls whose work overlaps on the GPU race and must be serialised.
- * Errors are reported through fbp_last_error(NULL). */
+ * FBP_ERR_UNSUPPORTED. Every call looks up that array's device address in
+ * the current context; the first call on a device also loads the library's
+ * device code there, so make it before any stream capture. All calls share
+ * the array: calls whose work overlaps on the GPU race and must be
+ * serialised. A CUDA error pending from the caller's earlier work is
+ * reported (and cleared) before any launch. Errors are reported through
+ * fbp_last_error(NULL). */
 int fbp2d_filter_sinogram_noalloc(float* sinogram, int bins, int views, int filter_type, float fan_sdd,
                                   float detector_width, int padded_length, void* cuda_stream);
 /* 2D backprojection (FBP2D.cpp:96-122 for parallel beam; flat-detector fan
