@@ -210,33 +210,39 @@ int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int
   return sync_host(ctx, !on_dev);
 }
 
-int download_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, float* dst, int on_dev) {
+// Rows row0, row0 + row_step, ... (nrows of them) to dst, packed [nrows][u].
+// row_step 1 is a contiguous band; row_step = views picks one view's rows
+// out of a sinogram stack [v][view][u].
+int download_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, float* dst, int on_dev, size_t row_step = 1) {
   if (!dst) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null destination pointer");
   FBP_TRY(flush_pending(ctx, s));
   if (s.filtered) {
     // unpack just these rows into a scratch f32 block
     float* tmp = static_cast<float*>(fbp::scratch(ctx, sizeof(float) * nrows * s.pitch));
     if (!tmp) return FBP_ERR_OUT_OF_MEMORY;
-    FBP_TRY(fbp::launch_unpack_rows(ctx, s, row0, nrows, tmp, s.pitch));
+    FBP_TRY(fbp::launch_unpack_rows(ctx, s, row0, nrows, tmp, s.pitch, (long long)row_step));
     FBP_TRY(fbp::cuda_check(ctx,
                             cudaMemcpy2DAsync(dst, (size_t)s.u * 4, tmp, (size_t)s.pitch * 4, (size_t)s.u * 4, nrows,
                                               kind_of(true, on_dev), ctx->stream),
                             "row download"));
   } else {
     FBP_TRY(fbp::cuda_check(ctx,
-                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, s.f32 + row0 * s.pitch, (size_t)s.pitch * 4,
+                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step,
                                               (size_t)s.u * 4, nrows, kind_of(true, on_dev), ctx->stream),
                             "row download"));
   }
   return sync_host(ctx, !on_dev);
 }
 
-int upload_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, const float* src, int on_dev) {
+// Rows row0, row0 + row_step, ... (nrows of them) from src, packed [nrows][u].
+int upload_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, const float* src, int on_dev,
+                size_t row_step = 1) {
   if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
   FBP_TRY(materialize_f32(ctx, s));
   FBP_TRY(fbp::cuda_check(ctx,
-                          cudaMemcpy2DAsync(s.f32 + row0 * s.pitch, (size_t)s.pitch * 4, src, (size_t)s.u * 4,
-                                            (size_t)s.u * 4, nrows, kind_of(on_dev, true), ctx->stream),
+                          cudaMemcpy2DAsync(s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step, src,
+                                            (size_t)s.u * 4, (size_t)s.u * 4, nrows, kind_of(on_dev, true),
+                                            ctx->stream),
                           "row upload"));
   return sync_host(ctx, !on_dev);
 }
@@ -784,6 +790,14 @@ int fbp_get_projections_size(const fbp_context* ctx, int* u, int* v, int* n) {
   return FBP_OK;
 }
 
+int fbp_get_sinograms_size(const fbp_context* ctx, int* u, int* v, int* n) {
+  if (!ctx || !u || !v || !n) return FBP_ERR_INVALID_ARGUMENT;
+  *u = ctx->sino.u;
+  *v = ctx->sino.v;
+  *n = ctx->sino.n;
+  return FBP_OK;
+}
+
 // ---------------------------------------------------------------- transfers
 int fbp_upload_projections(fbp_context* ctx, const float* src, int u, int v, int n, int on_dev) {
   FBP_CTX(ctx);
@@ -833,6 +847,22 @@ int fbp_load_sinogram(fbp_context* ctx, int y, float* dst, int on_dev) {
   FBP_TRY(require_stack(ctx, ctx->sino, "load_sinogram"));
   if (y < 0 || y >= ctx->sino.v) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "sinogram index out of range");
   return download_rows(ctx, ctx->sino, (size_t)y * ctx->sino.n, ctx->sino.n, dst, on_dev);
+}
+
+// One projection [v][u] (view `index`) out of / into the sinogram stack
+// [v][view][u]: rows index, index + views, ... (FBP3D.cpp:755-778).
+int fbp_load_projection_from_sinograms(fbp_context* ctx, int index, float* dst, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "load_projection_from_sinograms"));
+  if (index < 0 || index >= ctx->sino.n) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "projection index out of range");
+  return download_rows(ctx, ctx->sino, (size_t)index, ctx->sino.v, dst, on_dev, (size_t)ctx->sino.n);
+}
+
+int fbp_store_projection_to_sinograms(fbp_context* ctx, const float* src, int index, int on_dev) {
+  FBP_CTX(ctx);
+  FBP_TRY(require_stack(ctx, ctx->sino, "store_projection_to_sinograms"));
+  if (index < 0 || index >= ctx->sino.n) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "projection index out of range");
+  return upload_rows(ctx, ctx->sino, (size_t)index, ctx->sino.v, src, on_dev, (size_t)ctx->sino.n);
 }
 
 static int volume_slice(fbp_context* ctx, int axis, int index, float* host_or_dev, int on_dev, bool load) {
@@ -1354,7 +1384,26 @@ int fbp2d_filter_sinogram(fbp_context* ctx, float* sino, int bins, int views, in
     rs.w_du = det_w / bins;
     rs.w_dv = 0.f;
   }
-  return fbp::launch_filter_fft(ctx, rs, n);
+  // the context's precision / implementation switch, as for the 3D stacks:
+  // MIXED and MIXED24 filter on the tensor cores (split-BF16 Toeplitz product)
+  int impl = ctx->filter_impl;
+  if (impl == FBP_FILTER_IMPL_AUTO)
+    impl = (ctx->precision != FBP_PRECISION_FP32 && fbp::toeplitz_supported(bins)) ? FBP_FILTER_IMPL_TOEPLITZ
+                                                                                     : FBP_FILTER_IMPL_FFT;
+  if (impl != FBP_FILTER_IMPL_TOEPLITZ) return fbp::launch_filter_fft(ctx, rs, n);
+  if (!fbp::toeplitz_supported(bins))
+    return fbp::set_error(ctx, FBP_ERR_UNSUPPORTED, "Toeplitz filter needs 64 <= bins <= 8192");
+  // the GEMM's row split reads 16-byte vectors: stage the rows at a pitch of
+  // a multiple of 4 floats, filter them in place there and copy them back
+  Stack st;
+  FBP_TRY(stage_2d(ctx, sino, bins, views, st, 0));
+  rs.data = st.f32;
+  rs.pitch = st.pitch;
+  FBP_TRY(fbp::launch_filter_toeplitz(ctx, rs, n, filter_type));
+  return fbp::cuda_check(ctx,
+                         cudaMemcpy2DAsync(sino, (size_t)bins * 4, st.f32, (size_t)st.pitch * 4, (size_t)bins * 4,
+                                           views, cudaMemcpyDeviceToDevice, ctx->stream),
+                         "2D filtered rows copy-back");
 }
 
 int fbp2d_project_backward(fbp_context* ctx, const float* sino, int bins, int views, const fbp_geometry* geom,

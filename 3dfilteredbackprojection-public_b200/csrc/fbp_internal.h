@@ -209,7 +209,9 @@ int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long lo
 int launch_fft_rows(fbp_context* ctx, float2* data, int n, int rows, int inverse);
 int launch_fft_shift_rows(fbp_context* ctx, float2* data, int n, int rows, int shift);
 // Copy filtered rows [row0, row0 + nrows) of a pair layout back to FP32 rows.
-int launch_unpack_rows(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst, long long dst_pitch);
+// rows row0, row0 + row_step, ... (nrows of them) of the filtered buffer, as FP32 rows of dst
+int launch_unpack_rows(fbp_context* ctx, const Stack& s, size_t row0, size_t nrows, float* dst, long long dst_pitch,
+                       long long row_step = 1);
 bool toeplitz_supported(int m);
 
 // ---- backprojection (fbp_backproject.cu) ----

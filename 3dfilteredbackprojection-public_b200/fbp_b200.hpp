@@ -60,6 +60,10 @@ class FBP2D {
   explicit FBP2D(int device = 0) : owned_(std::make_shared<Context>(device)), ctx_(owned_->get()) {}
   explicit FBP2D(fbp_context* shared) : ctx_(shared) {}
 
+  // Precision form of apply_filter: FBP_PRECISION_FP32 (FFT) or MIXED /
+  // MIXED24 (tcgen05 split-BF16 Toeplitz product); no counterpart in the reference.
+  void set_precision(int precision) { check(ctx_, fbp_set_precision(ctx_, precision)); }
+  void set_filter_impl(int impl) { check(ctx_, fbp_set_filter_impl(ctx_, impl)); }
   // Weight (fan beam when fan_sdd > 0) and filter every row of a device
   // sinogram [views][bins] in place (FBP2D::apply_filter with the FFT calls
   // around it, FBP2D.cpp:124-144).
@@ -248,6 +252,13 @@ class FBP3D {
   }
   void store_sinogram(const float* src, int y_index, bool on_device = false) {
     check(c(), fbp_store_sinogram(c(), src, y_index, on_device));
+  }
+  // FBP3D.cpp:755-778: one [v][u] projection out of / into the sinogram stack
+  void load_projection_from_sinograms(int projection_index, float* out, bool on_device = false) {
+    check(c(), fbp_load_projection_from_sinograms(c(), projection_index, out, on_device));
+  }
+  void store_projection_to_sinograms(const float* src, int projection_index, bool on_device = false) {
+    check(c(), fbp_store_projection_to_sinograms(c(), src, projection_index, on_device));
   }
   void read_volume(float* out, bool on_device = false) { check(c(), fbp_read_volume(c(), out, on_device)); }
 

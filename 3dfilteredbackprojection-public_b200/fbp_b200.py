@@ -122,6 +122,7 @@ SIGNATURES = {
     "fbp_free_sinograms": [_P],
     "fbp_get_volume_size": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
     "fbp_get_projections_size": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
+    "fbp_get_sinograms_size": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
     "fbp_upload_projections": [_P, _P, _I, _I, _I, _I],
     "fbp_upload_sinograms": [_P, _P, _I, _I, _I, _I],
     "fbp_download_projections": [_P, _P, _I],
@@ -130,6 +131,8 @@ SIGNATURES = {
     "fbp_load_projection": [_P, _I, _P, _I],
     "fbp_store_sinogram": [_P, _P, _I, _I],
     "fbp_load_sinogram": [_P, _I, _P, _I],
+    "fbp_load_projection_from_sinograms": [_P, _I, _P, _I],
+    "fbp_store_projection_to_sinograms": [_P, _P, _I, _I],
     "fbp_load_volume_slice_x": [_P, _I, _P, _I],
     "fbp_load_volume_slice_y": [_P, _I, _P, _I],
     "fbp_load_volume_slice_z": [_P, _I, _P, _I],
@@ -476,6 +479,12 @@ class FBP3D:
         self.ctx.call("fbp_get_projections_size", C.byref(u), C.byref(v), C.byref(n))
         return u.value, v.value, n.value
 
+    def sinograms_size(self) -> tuple[int, int, int]:
+        """(detector columns, detector rows, views) of the sinogram stack."""
+        u, v, n = C.c_int(), C.c_int(), C.c_int()
+        self.ctx.call("fbp_get_sinograms_size", C.byref(u), C.byref(v), C.byref(n))
+        return u.value, v.value, n.value
+
     # -- transfers
     def upload_projections(self, projections) -> None:
         """[count][v][u] float32 array / tensor (replaces read_projections' upload)."""
@@ -520,6 +529,21 @@ class FBP3D:
         p, dev = _ptr(target)
         self.ctx.call("fbp_load_sinogram", y_index, p, dev)
         return target
+
+    def load_projection_from_sinograms(self, projection_index: int, target=None):
+        """FBP3D::load_projection_from_sinograms (FBP3D.cpp:755-765): view
+        projection_index of the sinogram stack as a [v][u] projection."""
+        u, v, _ = self.sinograms_size()
+        target = np.empty((v, u), np.float32) if target is None else target
+        p, dev = _ptr(target)
+        self.ctx.call("fbp_load_projection_from_sinograms", projection_index, p, dev)
+        return target
+
+    def store_projection_to_sinograms(self, source, projection_index: int) -> None:
+        """FBP3D::store_projection_to_sinograms (FBP3D.cpp:767-778): a [v][u]
+        projection into view projection_index of the sinogram stack."""
+        p, dev = _ptr(source)
+        self.ctx.call("fbp_store_projection_to_sinograms", p, projection_index, dev)
 
     def _slice(self, axis: str, index: int, target, load: bool):
         x, y, z = self.volume_size()
@@ -661,6 +685,14 @@ class FBP2D:
         self.torch = torch
         self.device = torch.device("cuda", device)
         self.ctx = context or Context(device)
+
+    def set_precision(self, precision: int) -> None:
+        """Precision form of apply_filter: FP32 (FFT) or MIXED / MIXED24
+        (tcgen05 split-BF16 Toeplitz product)."""
+        self.ctx.call("fbp_set_precision", int(precision))
+
+    def set_filter_impl(self, impl: int) -> None:
+        self.ctx.call("fbp_set_filter_impl", int(impl))
 
     def _dev(self, x):
         if _is_torch(x) and x.is_cuda:

@@ -76,6 +76,10 @@ def test_cpp_dropin_header_compiles(tmp_path):
         "  solver.apply_filter_to_projections(fbp::FBP2D::FilterType::SHEPP_LOGAN);\n"
         "  solver.project_backward_cone_fdk_from_projections(730.87f, 669.04f, 409.60f, 213.84f, 1, 8, 8, 0);\n"
         "  float slice[64];\n  solver.load_volume_slice_y(0, slice);\n"
+        "  solver.generate_blank_sinograms(8, 8, 4);\n"
+        "  solver.store_projection_to_sinograms(slice, 2);\n"
+        "  solver.load_projection_from_sinograms(2, slice);\n"
+        "  fbp::FBP2D f2;\n  f2.set_precision(FBP_PRECISION_MIXED);\n"
         "  return 0;\n}\n")
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", f"-I{ROOT / 'include'}", f"-I{PKG}", str(src)],
                        capture_output=True, text=True)
