@@ -49,6 +49,9 @@ UNIT = "Gvox·view/s"
 # bench forms: precision, bytes per stored filtered sample, storage note
 FORMS = {"chosen": ("MIXED", 2, "f16 filtered views"), "chosen24": ("MIXED24", 3, "24-bit filtered views"),
          "plain": ("FP32", 4, "f32")}
+# arithmetic / storage types of each form, for the line's dtype
+DTYPES = {"chosen": "f32 accumulate / f16 filtered views", "chosen24": "f32 accumulate / 24-bit filtered views",
+          "plain": "f32"}
 
 
 def parse_args():
@@ -74,8 +77,10 @@ def parse_args():
     p.add_argument("--backprojector", choices=["auto", "generic", "generic_y8", "symmetric", "tuned"], default="auto",
                    help="backprojector variant of both forms (tuned: timed per geometry on first use)")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--oracle-voxels", type=int, default=200000,
-                   help="voxels of the sampled FP64-oracle accuracy check (0: skip)")
+    p.add_argument("--oracle-voxels", type=int, default=1000000,
+                   help="uniformly drawn voxels of the sampled FP64-oracle accuracy check (0: skip the check)")
+    p.add_argument("--oracle-slice-voxels", type=int, default=100000,
+                   help="voxels in each y-slice band of the FP64-oracle accuracy check")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the CPU-baseline sample")
     return p.parse_args()
@@ -89,7 +94,9 @@ def workload(scale: int, name: str = "cone1440") -> dict:
 
 def measured_traffic(workload_name: str, form: str):
     """DRAM bytes (read + write) of one backprojector launch for this workload
-    and form, from the ncu capture recorded in profiles/ (None if absent)."""
+    and form, read from the ncu summary committed in profiles/ (None if
+    absent). The summary holds a capture of a smaller case of the same
+    workload, scaled to a full launch by the voxel-view updates."""
     try:
         for line in (ROOT / "profiles" / "bp_dram_traffic.txt").read_text().splitlines():
             f = line.split()
@@ -117,44 +124,62 @@ def _oracle():
     return O
 
 
-def oracle_sample(c: dict, raw_rows, nvox: int) -> dict:
-    """FP64 oracle values of `nvox` seeded voxels in three y-slices near the
-    central plane (y = ny/2 and ny/2 +- ny/60), for the accuracy of a cone
-    workload too large for a whole-volume oracle. The voxels' projections stay
-    within a centred band of detector rows for every view (bounded with the
-    nearest possible source distance), so the oracle weights and filters only
-    that band: a centred band of nv' rows (nv' of nv's parity) has the same row
-    coordinates as the full detector. raw_rows(r0, r1) returns the raw
-    projections' rows [r0, r1) as a [view][row][u] FP32 array."""
+def oracle_sample(c: dict, raw_views, nvox: int, slice_vox: int = 100_000, chunk: int = 24) -> dict:
+    """FP64 oracle values of seeded voxels spread over the whole volume, for
+    the accuracy of a cone workload too large for a whole-volume oracle:
+    `slice_vox` voxels in each of the y-slices near y = 0, ny/4, ny/2, 3 ny/4
+    and ny - 1 and, when ny > nz, one in the band y >= nz that the reference's
+    clip extent leaves unclipped (FBP3D.cpp:448), plus `nvox` voxels drawn
+    uniformly over the volume (near-source tiles included). The oracle weights
+    and filters the whole detector in FP64, `chunk` views at a time, and adds
+    each chunk's backprojection at the sampled voxels (a chunk of views is the
+    same orbit arc with its share of the pi / K scale). raw_views(k0, k1)
+    returns views [k0, k1) of the raw projections as a [view][v][u] FP32 array.
+    Returns the voxels (ix, iy, iz), their FP64 values and the index range of
+    each band."""
     import numpy as np
     O = _oracle()
     rng = np.random.default_rng(c["seed"] + 17)
-    yc = c["ny"] // 2
-    dy = max(1, c["ny"] // 60)
-    ys = np.clip(np.array([yc - dy, yc, yc + dy]), 0, c["ny"] - 1)
-    ymm = np.abs((ys + 0.5 - 0.5 * c["ny"]) * c["vox"]).max()
-    dmin = c["sod"] - math.hypot(0.5 * c["nx"] * c["vox"], 0.5 * c["nz"] * c["vox"])
-    if dmin <= 0:
-        return {}
-    half = int(math.ceil(ymm * c["sdd"] / dmin / c["dv"])) + 3
-    nvb = min(c["nv"], 2 * half + c["nv"] % 2)
-    r0 = (c["nv"] - nvb) // 2
-    ijk = np.stack([rng.integers(0, c["nx"], nvox), rng.choice(ys, nvox), rng.integers(0, c["nz"], nvox)], 1)
+    nx, ny, nz, K = c["nx"], c["ny"], c["nz"], c["nviews"]
+    ys = [1, ny // 4, ny // 2, (3 * ny) // 4, ny - 2]
+    if ny > nz:
+        ys.insert(4, nz + (ny - nz) // 2)
+    ys = sorted({int(min(max(y, 0), ny - 1)) for y in ys})
+    parts, bands, at = [], {}, 0
+    for y in ys:
+        parts.append(np.stack([rng.integers(0, nx, slice_vox), np.full(slice_vox, y), rng.integers(0, nz, slice_vox)], 1))
+        bands[f"y={y}" + (" (unclipped band)" if y >= nz else "")] = (at, at + slice_vox)
+        at += slice_vox
+    if nvox > 0:
+        parts.append(np.stack([rng.integers(0, nx, nvox), rng.integers(0, ny, nvox), rng.integers(0, nz, nvox)], 1))
+        bands["random voxels"] = (at, at + nvox)
+    ijk = np.ascontiguousarray(np.concatenate(parts).astype(np.int32))
     t0 = time.perf_counter()
-    p = O.fdk_weight(raw_rows(r0, r0 + nvb), c["sdd"], c["du"], c["dv"])
-    q = O.filter_rows(p.reshape(-1, c["nu"]), c["filter"]).reshape(p.shape)
-    del p
-    ref = O.bp_cone_points(q, c, ijk)
-    clip = ijk[:, 1] < c["nz"]  # the reference's clip extent (y-slices below z_size)
+    ref = np.zeros(len(ijk), np.float64)
+    for k0 in range(0, K, chunk):
+        k1 = min(K, k0 + chunk)
+        p = O.fdk_weight(raw_views(k0, k1), c["sdd"], c["du"], c["dv"])
+        q = O.filter_rows(p.reshape(-1, c["nu"]), c["filter"]).reshape(p.shape)
+        del p
+        arc = dict(c, span=c["span"] * (k1 - k0) / K, offset=c["offset"] + c["span"] * k0 / K)
+        ref += O.bp_cone_points(q, arc, ijk) * ((k1 - k0) / K)
+        del q
+    clip = ijk[:, 1] < nz  # the reference's clip extent (y-slices below z_size)
     ref[clip] = np.maximum(ref[clip], 0.0)
-    return {"ijk": ijk, "ref": ref, "rows": (r0, r0 + nvb), "seconds": time.perf_counter() - t0,
-            "slices": [int(y) for y in ys]}
+    return {"ijk": ijk, "ref": ref, "bands": bands, "seconds": time.perf_counter() - t0,
+            "threads": O.num_threads()}
 
 
-def sample_error(got, ref) -> dict:
+def sample_error(got, ref, bands=None) -> dict:
+    """Relative RMSE and max abs error of `got` against the FP64 `ref`,
+    overall and (bands: name -> index range) per band."""
     import numpy as np
     d = np.asarray(got, np.float64) - ref
-    return {"rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref)), "max_abs": float(np.abs(d).max())}
+    out = {"rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref)), "max_abs": float(np.abs(d).max())}
+    if bands:
+        out["bands"] = {k: {"rel_rmse": float(np.linalg.norm(d[a:b]) / np.linalg.norm(ref[a:b])),
+                            "max_abs": float(np.abs(d[a:b]).max())} for k, (a, b) in bands.items()}
+    return out
 
 
 def cpu_sample(c: dict, proj_views, view_ids, target_s: float) -> dict:
@@ -256,6 +281,12 @@ def reference_arm(args, rank: int, world: int) -> None:
                    "detector": [c["nu"], c["nv"]], "filter": FILTER_NAMES[c["filter"]], "parallelism": "host cores"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": r0["cores"], "kind": kind, "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        # each step times a sample of the job and extrapolates: ms_per_step is
+        # the full job's estimated time, not the time the step took
+        "extrapolated": True,
+        "sampled_fraction": {"filter_rows": r0["sample_rows"] / (c["nviews"] * c["nv"]),
+                             "backprojection_updates": r0["sample_updates"] / updates_of(c)},
+        "sample_seconds_per_step": statistics.mean(r["sample_seconds"] for r in results),
     }
     print(json.dumps(line), flush=True)
 
@@ -667,14 +698,16 @@ def main() -> None:
 
     accuracy = {}
     if rank == 0 and world == 1 and args.shard != "slabs" and args.oracle_voxels > 0:
-        chk = oracle_sample(c, lambda r0, r1: pristine[:, r0:r1, :].cpu().numpy(), args.oracle_voxels)
-        if chk:
-            ix, iy, iz = (torch.as_tensor(chk["ijk"][:, i], device=dev) for i in range(3))
-            for form, vol in vols.items():
-                accuracy[f"{form}_vs_fp64_oracle"] = sample_error(vol[iz, iy, ix].double().cpu().numpy(), chk["ref"])
-            accuracy["oracle_sample"] = (f"{len(chk['ref'])} seeded voxels in y-slices {chk['slices']}, each "
-                                         f"backprojected in FP64 from detector rows {chk['rows'][0]}..{chk['rows'][1] - 1} "
-                                         f"weighted and filtered in FP64 ({chk['seconds']:.0f} s on the host)")
+        chk = oracle_sample(c, lambda k0, k1: pristine[k0:k1].cpu().numpy(), args.oracle_voxels,
+                            args.oracle_slice_voxels)
+        ix, iy, iz = (torch.as_tensor(chk["ijk"][:, i], device=dev, dtype=torch.long) for i in range(3))
+        for form, vol in vols.items():
+            accuracy[f"{form}_vs_fp64_oracle"] = sample_error(vol[iz, iy, ix].double().cpu().numpy(), chk["ref"],
+                                                              chk["bands"])
+        accuracy["oracle_sample"] = (f"{args.oracle_slice_voxels} seeded voxels in each y-slice band and "
+                                     f"{args.oracle_voxels} seeded voxels uniform over the volume, each "
+                                     f"backprojected in FP64 from the whole detector weighted and filtered "
+                                     f"in FP64 ({chk['seconds']:.0f} s on {chk['threads']} host threads)")
     for form in [f for f in vols if f != "plain" and "plain" in vols]:
         a, b = vols[form].double(), vols["plain"].double()
         accuracy[f"{form}_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
@@ -735,7 +768,7 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True,
         "scaling": "strong" if args.shard == "slabs" else "weak",
-        "vs_baseline": None, "dtype": "f32", "storage_dtype": FORMS[head][2],
+        "vs_baseline": None, "dtype": DTYPES[head], "storage_dtype": FORMS[head][2],
         "data": data_note(c),
         "config": {"workload": c["name"], "volume_xyz": [c["nx"], c["ny"], c["nz"]], "voxel_mm": c["vox"],
                    "views": c["nviews"], "detector": [c["nu"], c["nv"]], "pitch_mm": c["du"],
@@ -747,6 +780,9 @@ def main() -> None:
         "stages_ms": {"filter": h["filter_ms"], "backprojection": h["bp_ms"]},
         "roofline": {"bound": "hbm", "achieved": hbm_bytes / bp_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": hbm_bytes / bp_s / 1e9 / hbm_peak, "traffic": traffic,
+                     "traffic_source": "profiles/bp_dram_traffic.txt (ncu dram__bytes_read.sum + "
+                                       "dram__bytes_write.sum of one launch, not measured in this run)",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
                      "note": "backprojector algorithmic HBM bytes (filtered views read once + volume written "
                              "once); the kernel is bound by shared-memory gathers, see roofline_smem"},
         "roofline_smem": {"bound": "smem", "achieved": gather_bytes / bp_s / 1e12,
@@ -769,7 +805,7 @@ def main() -> None:
         proj, views = cpu_inputs(c, 8 if args.scale == 1 else 4)
         r = cpu_sample(c, proj, views, target_s=args.cpu_seconds)
         line["cpu_baseline"] = {
-            "value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+            "value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference" if r["use_ref"] else "port",
             "sample": (f"{r['sample_rows']} detector rows filtered with the reference's own FFT "
                        f"({'compiled from its sources' if r['use_ref'] else 'oracle restatement'}), "
                        f"{r['sample_updates']:.3g} updates of the FP32 CPU backprojector restatement, "

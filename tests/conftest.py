@@ -32,7 +32,7 @@ def relative_rmse(x, ref):
 @pytest.fixture(scope="session")
 def oracle():
     import oracle as O
-    O.build(with_ref=O.REF_PATH.exists() or Path("/root/reference").exists())
+    O.build(with_ref=True)  # the reference FFT is built only where its sources are present
     return O
 
 
