@@ -402,7 +402,9 @@ int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, boo
   return FBP_OK;
 }
 
-int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
+// Checks, sharding offsets, pending row operations and the volume buffer of
+// a backprojection; *ylim = clip extent, *mixed = reduced-precision form.
+int setup_backproject(fbp_context* ctx, Stack& s, fbp::BPGeom& g, int* ylim, bool* mixed) {
   if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0)
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "volume resolution must be positive");
   // sharding: detector row band and volume y-slab set on the context
@@ -427,8 +429,15 @@ int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
     return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "detector and volume widths must be positive");
   FBP_TRY(flush_pending(ctx, s));
   FBP_TRY(ensure_volume(ctx, g.nx, g.ny, g.nz, false));
-  const int ylim = ctx->clip_after_bp ? clip_limit : 0;
-  const bool mixed = ctx->precision != FBP_PRECISION_FP32;
+  *ylim = ctx->clip_after_bp ? clip_limit : 0;
+  *mixed = ctx->precision != FBP_PRECISION_FP32;
+  return FBP_OK;
+}
+
+int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
+  int ylim = 0;
+  bool mixed = false;
+  FBP_TRY(setup_backproject(ctx, s, g, &ylim, &mixed));
   if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && g.ny > 1) {
     int variant = FBP_BACKPROJECTOR_AUTO;
     int rc = autotune_backprojector(ctx, s, g, mixed, &variant);
@@ -628,6 +637,10 @@ int fbp_destroy(fbp_context* ctx) {
     cudaFree(ctx->ttab.th);
     cudaFree(ctx->d_scratch);
     cudaFreeHost(ctx->h_pinned);
+    cudaFree(ctx->d_batch);
+    cudaFreeHost(ctx->h_batch);
+    if (ctx->ev_batch_copy) cudaEventDestroy(ctx->ev_batch_copy);
+    if (ctx->ev_sync) cudaEventDestroy(ctx->ev_sync);
     if (ctx->copy_stream) {
       cudaStreamSynchronize(ctx->copy_stream);
       cudaStreamDestroy(ctx->copy_stream);
@@ -716,6 +729,14 @@ int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, i
 int fbp_set_autotune(fbp_context* ctx, int enable) {
   FBP_CTX(ctx);
   ctx->autotune = enable ? 1 : 0;
+  return FBP_OK;
+}
+
+int fbp_set_symmetric_tile(fbp_context* ctx, int voxels_per_thread_y) {
+  FBP_CTX(ctx);
+  if (voxels_per_thread_y != 0 && voxels_per_thread_y != 8 && voxels_per_thread_y != 16)
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "symmetric tile height must be 0, 8 or 16");
+  ctx->quad_tile_ny = voxels_per_thread_y;
   return FBP_OK;
 }
 
@@ -1188,6 +1209,84 @@ int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float sod, 
   FBP_CTX(ctx);
   FBP_TRY(require_stack(ctx, ctx->proj, "project_backward_cone_fdk_from_projections"));
   return backproject(ctx, ctx->proj, cone_geom(ctx->proj, sod, odd, det_w, vol_w, rot, h, v, offset));
+}
+
+int fbp_project_backward_cone_fdk_batch(fbp_context* const* contexts, const fbp_geometry* geometries,
+                                        const int* volume_h, const int* volume_v, int count, fbp_context* launcher) {
+  FBP_CTX(launcher);
+  if (!contexts || !geometries || !volume_h || !volume_v || count <= 0)
+    return fbp::set_error(launcher, FBP_ERR_INVALID_ARGUMENT, "bad batch arguments");
+  for (int i = 0; i < count; ++i) {
+    if (!contexts[i] || contexts[i]->device != launcher->device)
+      return fbp::set_error(launcher, FBP_ERR_INVALID_ARGUMENT, "batch contexts must be on the launcher's device");
+    if (geometries[i].kind != FBP_GEOMETRY_CONE)
+      return fbp::set_error(launcher, FBP_ERR_INVALID_ARGUMENT, "batched backprojection takes cone-beam geometries");
+  }
+  struct Plans {
+    std::vector<fbp::BPLaunchPlan*> p;
+    ~Plans() {
+      for (auto* x : p) fbp::free_bp_plan(x);
+    }
+  } plans;
+  // plan every job on its own stream (weights, filter, packing, footprint pass)
+  for (int i = 0; i < count; ++i) {
+    fbp_context* c = contexts[i];
+    const fbp_geometry& ge = geometries[i];
+    FBP_TRY(require_stack(c, c->proj, "project_backward_cone_fdk_batch"));
+    fbp::BPGeom g = cone_geom(c->proj, ge.source_distance, ge.detector_distance, ge.detector_width, ge.volume_width,
+                              ge.full_rotation_count, volume_h[i], volume_v[i], ge.rotation_offset_radian);
+    int ylim = 0;
+    bool mixed = false;
+    if (int rc = setup_backproject(c, c->proj, g, &ylim, &mixed))
+      return fbp::set_error(launcher, rc, std::string("batch job ") + std::to_string(i) + ": " + c->last_error);
+    plans.p.push_back(fbp::new_bp_plan());
+    if (int rc = fbp::plan_backproject(c, g, c->proj, c->vol, ylim, mixed, plans.p.back()))
+      return fbp::set_error(launcher, rc, std::string("batch job ") + std::to_string(i) + ": " + c->last_error);
+  }
+  auto event = [&](fbp_context* c) -> cudaEvent_t {
+    if (!c->ev_sync) cudaEventCreateWithFlags(&c->ev_sync, cudaEventDisableTiming);
+    return c->ev_sync;
+  };
+  // jobs that share a batch key run in one persistent launch on the
+  // launcher's stream (after their own streams' work); the rest alone
+  std::vector<bool> done(count, false);
+  for (int i = 0; i < count; ++i) {
+    if (done[i]) continue;
+    const long long key = fbp::bp_plan_batch_key(*plans.p[i]);
+    if (key == 0) {
+      done[i] = true;
+      FBP_TRY(fbp::launch_bp_plan(contexts[i], *plans.p[i]));
+      continue;
+    }
+    std::vector<fbp::BPLaunchPlan*> group;
+    std::vector<fbp_context*> members;
+    for (int k = i; k < count; ++k)
+      if (!done[k] && fbp::bp_plan_batch_key(*plans.p[k]) == key) {
+        done[k] = true;
+        group.push_back(plans.p[k]);
+        members.push_back(contexts[k]);
+      }
+    for (fbp_context* c : members)
+      if (c != launcher) {
+        cudaEvent_t ev = event(c);
+        if (fbp::cuda_check(launcher, ev ? cudaEventRecord(ev, c->stream) : cudaErrorInvalidResourceHandle,
+                            "batch ready event") ||
+            fbp::cuda_check(launcher, cudaStreamWaitEvent(launcher->stream, ev, 0), "batch ready wait"))
+          return FBP_ERR_CUDA;
+      }
+    FBP_TRY(fbp::launch_bp_batch(launcher, group.data(), (int)group.size()));
+    cudaEvent_t lev = event(launcher);
+    if (fbp::cuda_check(launcher, lev ? cudaEventRecord(lev, launcher->stream) : cudaErrorInvalidResourceHandle,
+                        "batch done event"))
+      return FBP_ERR_CUDA;
+    for (fbp_context* c : members) {
+      if (c != launcher && fbp::cuda_check(launcher, cudaStreamWaitEvent(c->stream, lev, 0), "batch done wait"))
+        return FBP_ERR_CUDA;
+      c->last_bp[0] = FBP_BACKPROJECTOR_SYMMETRIC;
+      c->minmax_valid = false;
+    }
+  }
+  return FBP_OK;
 }
 
 int fbp_project_backward_cone_fdk_from_sinograms(fbp_context* ctx, float sod, float odd, float det_w, float vol_w,

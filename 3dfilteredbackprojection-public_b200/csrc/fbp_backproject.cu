@@ -583,13 +583,19 @@ constexpr int kQuadEntries = 8;  // outstanding view-quads per CTA
 constexpr int kKahanQuads = 4;   // quads (16 views) per Kahan fold
 constexpr int kFoldQG = 64;      // quads per Kahan fold when the running sums live in shared memory
 
-// 16-byte aligned so that consumers read a record with vector loads
+// Quad record flags.
+constexpr int kQSkip = 1;    // the tile footprint misses the detector (or failed a check): no taps
+constexpr int kQDirect = 2;  // interleaved layout: window not staged, consumers gather it from global memory
+constexpr int kQFirst = 4;   // first quad of a work item (a tile orbit and y-slab of one job)
+constexpr int kQLast = 8;    // last quad of a work item: the consumers store its voxels next
+constexpr int kQExit = 16;   // multi-job launch: the queue is empty, the CTA leaves
+
+// 16-byte aligned so that consumers read a record with vector loads (96 bytes)
 struct alignas(16) QuadCoef {
   float Dx, Dz, D0, Nx, Nz, N0, Vx, Vz, V0;
   float ws[4];  // per-view extra weight of the four views (FP16 views: 1 / scale)
-  int skip;
+  int flags;    // kQ* bits
   int sub;      // bytes between the entry's four windows
-  int direct;   // interleaved layout: window not staged, consumers gather it from global memory
   int u0, e0;   // direct: element column / element row of the window origin
   // consumer constants of the window, formed once by the producer
   uint32_t cbase;  // ring address of element column 0 minus kMagicBits element rows
@@ -597,12 +603,96 @@ struct alignas(16) QuadCoef {
   uint32_t plane;  // interleaved layout: bytes between the 16-byte planes of an element row
   int bu2;         // last element column a tap may start at (box width - 2)
   float vmax;      // exclusive bound on the window-local v of a tap
+  float dvn;       // the job's v step per voxel times D
+  int item;        // work item of this quad
+};
+static_assert(sizeof(QuadCoef) == 96, "six 16-byte loads per record");
+
+// Multi-job launch (several reconstructions in one persistent launch): one
+// entry per job in global memory; the work items of job j are
+// [item0, item0 + nbh * nbh * nty), ordered y-slab, then z, then x.
+struct QuadJob {
+  BPArgs a;
+  long long item0;
+  int nbh;  // representative tiles per axis
+  int nty;  // y-slabs
+};
+struct QuadQueue {
+  const QuadJob* jobs;    // sorted by item0
+  const BoxMaps* maps;    // one grid of tensor maps per job
+  int njobs;
+  long long nitems;
+  unsigned long long* next;  // work-item counter (zero before the launch)
+  int* err;                  // device error word of the launch
+  int ring;                  // ring bytes of every CTA
 };
 
-// 288 threads, two CTAs per SM: 9 warps each put 5 warps on some SM
-// sub-partitions (16K registers each), so at most 96 registers per thread.
-template <int LAYOUT, int NY, bool KAHAN>
-__global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
+__device__ __forceinline__ int find_job(const QuadQueue& qq, long long item) {
+  int lo = 0, hi = qq.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (qq.jobs[mid].item0 <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ const BPArgs& job_args(const BPArgs& a, const QuadQueue& qq, int jb) {
+  if constexpr (MULTI) return qq.jobs[jb].a;
+  else return a;
+}
+template <bool MULTI>
+__device__ __forceinline__ const BoxMaps& job_maps(const BoxMaps& m, const QuadQueue& qq, int jb) {
+  if constexpr (MULTI) return qq.maps[jb];
+  else return m;
+}
+
+// Tile of a work item and the first view (group) of its walk. The walk starts
+// at an offset advanced by about K views per `resident` CTAs in tile order
+// (interleaved layout: by view groups): tiles that run at the same time then
+// read the same views (their windows share L2) instead of all starting at view
+// 0. The offset depends only on the tile, so results are the same whichever
+// CTA, launch or batch computes it.
+struct ItemTile {
+  int ix0, iy0, iz0;
+  int g0, k0;
+};
+template <bool QG, int NY>
+__device__ __forceinline__ ItemTile item_tile(const BPArgs& ja, long long t, int nbh) {
+  ItemTile it;
+  const long long per = (long long)nbh * nbh;
+  const int by = (int)(t / per);
+  const int rem = (int)(t - (long long)by * per);
+  const int bz = rem / nbh, bx = rem - bz * nbh;
+  it.ix0 = bx * 16;
+  it.iz0 = bz * 16;
+  it.iy0 = by * NY;
+  const int K = ja.nviews;
+  it.g0 = QG ? (int)((t * (K >> 2) / max(1, ja.resident)) % (K >> 2)) : 0;
+  it.k0 = QG ? 0 : (int)((t * K / max(1, ja.resident)) % K);
+  return it;
+}
+
+// 288 threads. OCC = 2 CTAs per SM: 9 warps each put 5 warps on some SM
+// sub-partitions (16K registers each), so at most 96 registers per thread,
+// and each CTA gets half of the shared memory. OCC = 1: up to 168 registers
+// and all of the shared memory, for 16 voxels per thread along y (64
+// accumulators a thread, the window staged once for twice the voxels).
+//
+// MULTI = false: one job, one work item (tile orbit and y-slab) per CTA, from
+// the block index. MULTI = true: a persistent launch of OCC CTAs per SM over
+// the work items of several jobs (uneven sizes, each with its own geometry,
+// views and tensor maps, all of one staged layout); the producer takes the
+// next item from the queue's counter and streams its quads into the ring
+// without a pause between items, the consumers reset their sums at an item's
+// first quad and store its voxels after its last. An item's arithmetic and
+// view order do not depend on the launch, so a job's volume is the same bits
+// alone or batched with others.
+template <int LAYOUT, int NY, bool KAHAN, int OCC, bool MULTI>
+__global__ void __launch_bounds__(256 + 32, OCC)
+    bp_quad_kernel(const __grid_constant__ BoxMaps maps, const __grid_constant__ BPArgs a,
+                   const __grid_constant__ QuadQueue qq) {
   constexpr int TX = 16, TZ = 16, NCW = 8, E = kQuadEntries;
   // QG: the four views of a quad come interleaved in one window (one copy,
   // two 16-byte loads per voxel step feed all four taps). The quads are
@@ -616,20 +706,8 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int R = a.box_bytes;  // ring bytes
-  const int K = a.nviews, Q = K >> 2;
-  const int nbh = a.ntx >> 1;  // representative tiles per axis (lower-left quadrant)
-  const int bx = blockIdx.x % nbh, bz = blockIdx.x / nbh;
-  // The CTA starts its walk over the views at an offset advanced by about K
-  // views per `resident` CTAs in launch order (interleaved layout: by view
-  // groups). A CTA that starts after others have progressed then reads the
-  // same views at the same time (their windows share L2) instead of
-  // restarting at view 0; the offset depends only on the block index, so
-  // results stay deterministic.
-  const long long bid = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-  const int g0 = QG ? (int)((bid * (K >> 2) / max(1, a.resident)) % (K >> 2)) : 0;  // first view group
-  const int k0 = QG ? 0 : (int)((bid * K / max(1, a.resident)) % K);                 // first view (other layouts)
-  const int ix0 = bx * TX, iz0 = bz * TZ, iy0 = blockIdx.y * NY;
+  const int R = MULTI ? qq.ring : a.box_bytes;  // ring bytes
+  int* const err = MULTI ? qq.err : a.err;
 
   QuadCoef* coef = reinterpret_cast<QuadCoef*>(smem + R);
   uint64_t* full = reinterpret_cast<uint64_t*>(coef + E);
@@ -639,7 +717,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   float* comp = reinterpret_cast<float*>(smem + R + E * sizeof(QuadCoef) + E * 16 + E * 4 + 64);
 
   if (tid == 0) {
-    *s_abort = *(volatile int*)a.err != 0;
+    *s_abort = *(volatile int*)err != 0;
     for (int e = 0; e < E; ++e) {
       mbar_init(&full[e], 1);
       mbar_init(&empty[e], NCW);
@@ -652,120 +730,170 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
 
   if (warp == NCW) {
     // ---------------------------------------------------------------- producer
-    int head = 0, tail = 0, oldest = 0, issued = 0;
-    for (int kb = 0; kb < K && !*s_abort; kb += 32) {
-      const int it = kb + lane;  // iteration (ring entry order)
-      // view of the representative tile; rotation r uses view (k + r Q) mod K
-      const int gq = QG ? ((it >> 2) + g0) % Q : 0;  // view group of iteration it
-      const int k = QG ? gq + (it & 3) * Q : (it + k0) % K;
-      QuadCoef qc;
-      int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
-      bool skip = true, direct = false;
-      qc.skip = 1;
-      qc.rb = 0;
-      if (it < K) {
-        ViewCoef vc;
-        bool overflow = false, behind = false;
-        int need_u = 0, need_v = 0;
-        skip = tile_view_coef(a, k, ix0, iy0, iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, need_u, need_v, overflow,
-                              behind);
-        if (overflow) atomicCAS(a.err, 0, kDevFootprint);
-        if (behind) atomicCAS(a.err, 0, kDevGeometry);
-        if (overflow || behind) skip = true;
-        int wi = 0, hi = 0;
-        const int rows = need_v - a.pair_rows;
-        while (wi < kNW - 1 && maps.w[wi] < need_u) ++wi;
-        while (hi < kNH - 1 && maps.h[hi] < rows) ++hi;
-        mi = wi * kNH + hi;
-        tx_bytes = maps.w[wi] * maps.h[hi] * ESZ;
-        sub = (tx_bytes + 127) & ~127;
-        // interleaved layout: a window wider than the widest box or larger than
-        // the ring (rare near-source tiles) is read from global memory instead
-        direct = QG && !skip && (need_u > maps.w[kNW - 1] || rows > maps.h[kNH - 1] || sub > R);
-        need = (skip || direct) ? 0 : (QG ? sub : 4 * sub);
-        qc.Dx = vc.Dx; qc.Dz = vc.Dz; qc.D0 = vc.D0;
-        qc.Nx = vc.Nx; qc.Nz = vc.Nz; qc.N0 = vc.N0;
-        qc.Vx = vc.Vx; qc.Vz = vc.Vz; qc.V0 = vc.V0;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) qc.ws[r] = a.inv_scale ? a.inv_scale[(k + r * Q) % K] : 1.0f;
-        qc.skip = skip;
-        // window: width (elements) and rows
-        const int BU = direct ? need_u : maps.w[wi], BV = direct ? rows : maps.h[hi];
-        qc.sub = sub;
-        qc.direct = direct;
-        qc.u0 = u0 + 1;
-        qc.e0 = v0 + a.pair_rows;
-        qc.rb = (uint32_t)(BU * ESZ);
-        qc.plane = (uint32_t)(BU * 16);
-        qc.bu2 = BU - 2;
-        qc.vmax = (float)(BV - kRowTail) - (float)(kSlack / 2);
+    // head / tail: ring bytes allocated / freed; oldest: first quad not yet
+    // known to be released; seq: quads issued since the launch (all items)
+    int head = 0, tail = 0, oldest = 0, seq = 0;
+    bool more = true, first = true;
+    while (more && !*s_abort) {
+      // the next work item: this CTA's tile, or the queue's next item
+      long long item;
+      if constexpr (MULTI) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(qq.next, 1ull);
+        item = (long long)__shfl_sync(0xffffffffu, t, 0);
+        if (item >= qq.nitems) break;
+      } else {
+        if (!first) break;
+        item = (long long)blockIdx.y * gridDim.x + blockIdx.x;
       }
-      const int nb = min(32, K - kb);
-      for (int i = 0; i < nb; ++i) {
-        const int q = kb + i;
-        const int e = q % E;
-        const int qneed = __shfl_sync(0xffffffffu, need, i);
-        // allocate qneed contiguous ring bytes: wrap to 0 when the tail end is too short
-        const int pos = head % R;
-        const int start = pos + qneed > R ? head + (R - pos) : head;
-        bool ok = true;
-        while (oldest < q && (oldest <= q - E || start + qneed - tail > R)) {
-          if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, a.err)) {
-            ok = false;
+      first = false;
+      const int jb = MULTI ? find_job(qq, item) : 0;
+      const BPArgs& ja = job_args<MULTI>(a, qq, jb);
+      const BoxMaps& jm = job_maps<MULTI>(maps, qq, jb);
+      const long long t_local = MULTI ? item - qq.jobs[jb].item0 : item;
+      const ItemTile til = item_tile<QG, NY>(ja, t_local, MULTI ? qq.jobs[jb].nbh : ja.ntx >> 1);
+      const int K = ja.nviews, Q = K >> 2;
+      for (int kb = 0; kb < K && !*s_abort; kb += 32) {
+        const int it = kb + lane;  // quad of the item (ring entry order)
+        // view of the representative tile; rotation r uses view (k + r Q) mod K
+        const int gq = QG ? ((it >> 2) + til.g0) % Q : 0;  // view group of quad it
+        const int k = QG ? gq + (it & 3) * Q : (it + til.k0) % K;
+        QuadCoef qc;
+        int u0 = 0, v0 = 0, mi = 0, need = 0, sub = 0, tx_bytes = 0;
+        bool skip = true, direct = false;
+        qc.flags = kQSkip;
+        qc.rb = 0;
+        if (it < K) {
+          ViewCoef vc;
+          bool overflow = false, behind = false;
+          int need_u = 0, need_v = 0;
+          skip = tile_view_coef(ja, k, til.ix0, til.iy0, til.iz0, TX - 1, NY - 1, TZ - 1, vc, u0, v0, need_u,
+                                need_v, overflow, behind);
+          // checks of the job's geometry go to the job's error word
+          if (overflow) atomicCAS(ja.err, 0, kDevFootprint);
+          if (behind) atomicCAS(ja.err, 0, kDevGeometry);
+          if (overflow || behind) skip = true;
+          int wi = 0, hi = 0;
+          const int rows = need_v - ja.pair_rows;
+          while (wi < kNW - 1 && jm.w[wi] < need_u) ++wi;
+          while (hi < kNH - 1 && jm.h[hi] < rows) ++hi;
+          mi = wi * kNH + hi;
+          tx_bytes = jm.w[wi] * jm.h[hi] * ESZ;
+          sub = (tx_bytes + 127) & ~127;
+          // interleaved layout: a window wider than the widest box or larger than
+          // the ring (rare near-source tiles) is read from global memory instead
+          direct = QG && !skip && (need_u > jm.w[kNW - 1] || rows > jm.h[kNH - 1] || sub > R);
+          need = (skip || direct) ? 0 : (QG ? sub : 4 * sub);
+          qc.Dx = vc.Dx; qc.Dz = vc.Dz; qc.D0 = vc.D0;
+          qc.Nx = vc.Nx; qc.Nz = vc.Nz; qc.N0 = vc.N0;
+          qc.Vx = vc.Vx; qc.Vz = vc.Vz; qc.V0 = vc.V0;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) qc.ws[r] = ja.inv_scale ? ja.inv_scale[(k + r * Q) % K] : 1.0f;
+          qc.flags = (skip ? kQSkip : 0) | (direct ? kQDirect : 0) | (it == 0 ? kQFirst : 0) |
+                     (it == K - 1 ? kQLast : 0);
+          // window: width (elements) and rows
+          const int BU = direct ? need_u : jm.w[wi], BV = direct ? rows : jm.h[hi];
+          qc.sub = sub;
+          qc.u0 = u0 + 1;
+          qc.e0 = v0 + ja.pair_rows;
+          qc.rb = (uint32_t)(BU * ESZ);
+          qc.plane = (uint32_t)(BU * 16);
+          qc.bu2 = BU - 2;
+          qc.vmax = (float)(BV - kRowTail) - (float)(kSlack / 2);
+          qc.dvn = ja.dvn;
+          qc.item = (int)item;
+        }
+        const int nb = min(32, K - kb);
+        for (int i = 0; i < nb; ++i) {
+          const int q = seq + i;  // ring sequence number
+          const int e = q % E;
+          const int qneed = __shfl_sync(0xffffffffu, need, i);
+          // allocate qneed contiguous ring bytes: wrap to 0 when the tail end is too short
+          const int pos = head % R;
+          const int start = pos + qneed > R ? head + (R - pos) : head;
+          bool ok = true;
+          while (oldest < q && (oldest <= q - E || start + qneed - tail > R)) {
+            if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, err)) {
+              ok = false;
+              break;
+            }
+            tail = end_pos[oldest % E];
+            ++oldest;
+          }
+          if (!ok) {
+            *s_abort = 1;
+            more = false;
             break;
           }
-          tail = end_pos[oldest % E];
-          ++oldest;
-        }
-        if (!ok) {
-          *s_abort = 1;
-          break;
-        }
-        if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
-        const int off = start % R;
-        if (lane == i) {
-          qc.cbase = smem_u32(smem) + (uint32_t)off - kMagicBits * qc.rb;
-          coef[e] = qc;
-        }
-        if (lane == 0) end_pos[e] = start + qneed;
-        head = start + qneed;
-        const int sk = __shfl_sync(0xffffffffu, (int)(skip || direct), i);
-        const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
-        const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
-        const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
-        // view of the representative tile at iteration q (the interleaved layout addresses its group instead)
-        const int ck = QG ? 0 : __shfl_sync(0xffffffffu, k, i);
-        __syncwarp();
-        if (lane == 0) {
-          if (sk) {
-            mbar_arrive(&full[e]);
-          } else if (QG) {
-            // group gq, slots = views gq + s Q; element column u0 + 1 holds columns u0, u0 + 1
-            mbar_arrive_expect_tx(&full[e], (uint32_t)ctx);
-            tma_load_4d(smem + off, &maps.map[cmi], 2 * (cu0 + 1), 0, cv0 + a.pair_rows, ((q >> 2) + g0) % Q,
-                        &full[e]);
-          } else {
-            mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
-            const CUtensorMap* m = &maps.map[cmi];
-            const int x = LAYOUT == kLayoutPair32 ? 2 * cu0 : cu0;
-            const int e0 = cv0 + a.pair_rows;
+          if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
+          const int off = start % R;
+          if (lane == i) {
+            qc.cbase = smem_u32(smem) + (uint32_t)off - kMagicBits * qc.rb;
+            coef[e] = qc;
+          }
+          if (lane == 0) end_pos[e] = start + qneed;
+          head = start + qneed;
+          const int sk = __shfl_sync(0xffffffffu, (int)(skip || direct), i);
+          const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
+          const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
+          const int ctx = __shfl_sync(0xffffffffu, tx_bytes, i);
+          // view of the representative tile at quad kb + i (the interleaved layout addresses its group)
+          const int ck = QG ? 0 : __shfl_sync(0xffffffffu, k, i);
+          __syncwarp();
+          if (lane == 0) {
+            if (sk) {
+              mbar_arrive(&full[e]);
+            } else if (QG) {
+              // group gq, slots = views gq + s Q; element column u0 + 1 holds columns u0, u0 + 1
+              mbar_arrive_expect_tx(&full[e], (uint32_t)ctx);
+              tma_load_4d(smem + off, &jm.map[cmi], 2 * (cu0 + 1), 0, cv0 + ja.pair_rows,
+                          (((kb + i) >> 2) + til.g0) % Q, &full[e]);
+            } else {
+              mbar_arrive_expect_tx(&full[e], (uint32_t)(4 * ctx));
+              const CUtensorMap* m = &jm.map[cmi];
+              const int x = LAYOUT == kLayoutPair32 ? 2 * cu0 : cu0;
+              const int e0 = cv0 + ja.pair_rows;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              void* dst = smem + off + r * csub;
-              const int kv = (ck + r * Q) % K;
-              if (a.sino_layout)
-                tma_load_3d(dst, m, x, kv, e0, &full[e]);
-              else
-                tma_load_3d(dst, m, x, e0, kv, &full[e]);
+              for (int r = 0; r < 4; ++r) {
+                void* dst = smem + off + r * csub;
+                const int kv = (ck + r * Q) % K;
+                if (ja.sino_layout)
+                  tma_load_3d(dst, m, x, kv, e0, &full[e]);
+                else
+                  tma_load_3d(dst, m, x, e0, kv, &full[e]);
+              }
             }
           }
+          __syncwarp();
+        }
+        if (!more) break;
+        seq += nb;
+      }
+    }
+    if (MULTI && !*s_abort) {
+      // queue empty: one record that tells the consumers to leave
+      const int q = seq, e = q % E;
+      bool ok = true;
+      while (oldest < q && oldest <= q - E) {
+        if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, err)) {
+          ok = false;
+          break;
+        }
+        ++oldest;
+      }
+      if (ok) {
+        if (lane == 0) {
+          coef[e].flags = kQExit | kQSkip;
+          mbar_arrive(&full[e]);
         }
         __syncwarp();
-        issued = q + 1;
+        ++seq;
+      } else {
+        *s_abort = 1;
       }
     }
     // leave only when every copy issued into this CTA's memory has landed
-    for (int q = max(0, issued - E); q < issued; ++q) mbar_wait(&full[q % E], (q / E) & 1, a.err);
+    for (int q = max(0, seq - E); q < seq; ++q) mbar_wait(&full[q % E], (q / E) & 1, err);
     return;
   }
 
@@ -783,44 +911,67 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
   float* accs = comp;  // SMACC: FP32 running sums, then BF16 compensations
   __nv_bfloat16* compb = reinterpret_cast<__nv_bfloat16*>(comp + 4 * NY * 256);
   float acc[4][NY], part[KAHAN ? 4 : 1][KAHAN ? NY : 1];
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int j = 0; j < NY; ++j) acc[r][j] = 0.f;
-  if (KAHAN) {
+  // a new work item: zero every sum of this thread
+  auto reset = [&]() {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int j = 0; j < NY; ++j) {
-        part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
-        if (SMACC) {
-          accs[(r * NY + j) * 256 + tid] = 0.f;
-          compb[(r * NY + j) * 256 + tid] = __float2bfloat16_rn(0.f);
-        } else {
-          comp[(r * NY + j) * 256 + tid] = 0.f;
+      for (int j = 0; j < NY; ++j) acc[r][j] = 0.f;
+    if (KAHAN) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int j = 0; j < NY; ++j) {
+          part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
+          if (SMACC) {
+            accs[(r * NY + j) * 256 + tid] = 0.f;
+            compb[(r * NY + j) * 256 + tid] = __float2bfloat16_rn(0.f);
+          } else {
+            comp[(r * NY + j) * 256 + tid] = 0.f;
+          }
         }
-      }
-  }
+    }
+  };
+  reset();
   int e = 0;
   uint32_t ph = 0;
-  bool bad = false, stop = false;
-  int grp = 0;  // interleaved layout: view group of the current four quads
+  bool bad = false, stop = false, last = false, leave = false;
+  int grp = 0;        // interleaved layout: view group of the current four quads
+  long long item = -1;  // work item being accumulated
+  int jb = 0;         // its job
   // one quad: wait for its window, apply it to the 4 x NY voxels, release it
   auto step = [&](auto mc) {
     constexpr int M = decltype(mc)::value;
-    if (!mbar_wait(&full[e], ph, a.err)) {
+    if (!mbar_wait(&full[e], ph, err)) {
       *s_abort = 1;
       stop = true;
       return;
     }
     const QuadCoef g = coef[e];
-    if (!g.skip) {
+    if (g.flags & (kQExit | kQFirst)) {
+      if (g.flags & kQExit) {  // multi-job launch: no more items (always at a group start)
+        leave = true;
+      } else {
+        item = g.item;
+        if constexpr (MULTI) {
+          jb = find_job(qq, item);
+          const BPArgs& ja = qq.jobs[jb].a;
+          const ItemTile til = item_tile<QG, NY>(ja, item - qq.jobs[jb].item0, qq.jobs[jb].nbh);
+          grp = til.g0;
+        } else {
+          grp = item_tile<QG, NY>(a, item, a.ntx >> 1).g0;
+        }
+      }
+    }
+    last = (g.flags & kQLast) != 0;
+    if (!(g.flags & kQSkip)) {
+      // explicit roundings (no contraction): the same bits in every instantiation
       const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
       const float rD = rcp_approx(D);
-      const float ul = fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)) * rD;
-      const float vl = fmaf(g.Vx, fx, fmaf(g.Vz, fz, g.V0)) * rD;
-      const float dvv = a.dvn * rD;
-      const float W = rD * rD;
+      const float ul = __fmul_rn(fmaf(g.Nx, fx, fmaf(g.Nz, fz, g.N0)), rD);
+      const float vl = __fmul_rn(fmaf(g.Vx, fx, fmaf(g.Vz, fz, g.V0)), rD);
+      const float dvv = __fmul_rn(g.dvn, rD);
+      const float W = __fmul_rn(rD, rD);
       const float fuf = floorf(ul);
       const int iu = (int)fuf;
       const float fu = ul - fuf;
@@ -832,7 +983,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         if constexpr (QG) {
           float Wr[4];
 #pragma unroll
-          for (int r = 0; r < 4; ++r) Wr[r] = W * g.ws[r];
+          for (int r = 0; r < 4; ++r) Wr[r] = __fmul_rn(W, g.ws[r]);
           // (A, G) of the four rotations at one voxel from the 2 x 16 bytes of
           // its element (slot of rotation r: (M + r) mod 4): A = u-lerp of row
           // e - 1, G = u-lerp of the row difference
@@ -877,7 +1028,7 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
               d1 = d.y;
             }
           };
-          if (!g.direct) {
+          if (!(g.flags & kQDirect)) {
             const uint32_t plane = g.plane;
             static_assert(NY % 2 == 0, "voxels stepped in pairs");
             const float2 magic2 = make_float2(kMagic, kMagic);
@@ -904,8 +1055,9 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
           } else {
             // window not staged: read the elements from global memory (zero
             // outside the stored extent, as the TMA fill would give)
+            const BPArgs& ja = job_args<MULTI>(a, qq, jb);
             const int col = g.u0 + iu;
-            const bool col_ok = col >= 0 && col < a.qg_pitch;
+            const bool col_ok = col >= 0 && col < ja.qg_pitch;
             const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
             for (int j = 0; j < NY; ++j) {
@@ -914,11 +1066,11 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
               const float fv = v - (t - kMagic);
               const int row = g.e0 + (int)(__float_as_uint(t) - kMagicBits);
               uint4 L0 = zero, L1 = zero, L2 = zero;
-              if (col_ok && row >= 0 && row < a.qg_rows) {
-                const uint4* p = a.qg + ((size_t)grp * a.qg_rows + row) * NPL * a.qg_pitch + col;
+              if (col_ok && row >= 0 && row < ja.qg_rows) {
+                const uint4* p = ja.qg + ((size_t)grp * ja.qg_rows + row) * NPL * ja.qg_pitch + col;
                 L0 = __ldg(p);
-                L1 = __ldg(p + a.qg_pitch);
-                if (QG24) L2 = __ldg(p + 2 * a.qg_pitch);
+                L1 = __ldg(p + ja.qg_pitch);
+                if (QG24) L2 = __ldg(p + 2 * ja.qg_pitch);
               }
               float A[4], G[4];
               decode(L0, L1, L2, A, G);
@@ -930,9 +1082,9 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
           float wa[4], wb[4], Wr[4];
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
-            Wr[r] = W * g.ws[r];
-            wa[r] = Wr[r] - Wr[r] * fu;
-            wb[r] = Wr[r] * fu;
+            Wr[r] = __fmul_rn(W, g.ws[r]);
+            wb[r] = __fmul_rn(Wr[r], fu);
+            wa[r] = __fsub_rn(Wr[r], wb[r]);
           }
 #pragma unroll
           for (int j = 0; j < NY; ++j) {
@@ -975,13 +1127,55 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
       }
   };
+  // the item's sums into its voxels: four rotated columns,
+  // (x, z) -> (n-1-z, x) -> (n-1-x, n-1-z) -> (z, n-1-x)
+  auto store = [&]() {
+    if (KAHAN) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int j = 0; j < NY; ++j) {
+          const int i = (r * NY + j) * 256 + tid;
+          const float sum = SMACC ? accs[i] : acc[r][j];
+          const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
+          acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - c);
+        }
+    }
+    const BPArgs& ja = job_args<MULTI>(a, qq, jb);
+    const ItemTile til = item_tile<QG, NY>(ja, MULTI ? item - qq.jobs[jb].item0 : item,
+                                           MULTI ? qq.jobs[jb].nbh : a.ntx >> 1);
+    const int n = ja.nx;
+    const int ix = til.ix0 + tx, iz = til.iz0 + tz;
+    const int cx[4] = {ix, n - 1 - iz, n - 1 - ix, iz};
+    const int cz[4] = {iz, ix, n - 1 - iz, n - 1 - ix};
+    float* const vol = ja.vol;
+    const int ystride = ja.vol_ystride, ny = ja.ny, ylim = ja.clip_ylimit;
+    const float scale = ja.scale;
+    float lo = __int_as_float(0x7f800000), hi = -lo;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      float* out = vol + ((size_t)cz[r] * ystride) * n + cx[r];
+#pragma unroll
+      for (int j = 0; j < NY; ++j) {
+        const int iy = til.iy0 + j;
+        if (iy < ny) {
+          float val = acc[r][j] * scale;
+          if (iy < ylim) val = fmaxf(val, 0.f);
+          out[(size_t)iy * n] = val;
+          lo = fminf(lo, val);
+          hi = fmaxf(hi, val);
+        }
+      }
+    }
+    if (ja.minmax) fold_minmax(ja.minmax, lo, hi);
+  };
   static_assert(kKahanQuads == 4 && kFoldQG % 4 == 0, "folds on whole groups of four quads");
-  if constexpr (QG) {
-    int kq = 0;
-    grp = g0;  // view group of quads q .. q + 3: (q / 4 + g0) mod K / 4, stepped
-    for (int q = 0; q < K; q += 4) {
+  int kq = 0;
+  for (;;) {
+    if constexpr (QG) {
+      // a group of four quads (an item's quads come in whole groups)
       step(std::integral_constant<int, 0>{});
-      if (stop) break;
+      if (stop || leave) break;
       step(std::integral_constant<int, 1>{});
       if (stop) break;
       step(std::integral_constant<int, 2>{});
@@ -992,55 +1186,28 @@ __global__ void __launch_bounds__(256 + 32, 2) bp_quad_kernel(const __grid_const
         kq = 0;
         fold();
       }
-      if (++grp == Q) grp = 0;
-    }
-  } else {
-    int kq = 0;
-    for (int q = 0; q < K; ++q) {
+      const int Qj = job_args<MULTI>(a, qq, jb).nviews >> 2;
+      if (++grp == Qj) grp = 0;
+    } else {
       step(std::integral_constant<int, 0>{});
-      if (stop) break;
+      if (stop || leave) break;
       if (KAHAN && ++kq == kKahanQuads) {
         kq = 0;
         fold();
       }
     }
-  }
-  if (bad) atomicCAS(a.err, 0, kDevFootprint);
-  if (KAHAN) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int j = 0; j < NY; ++j) {
-        const int i = (r * NY + j) * 256 + tid;
-        const float sum = SMACC ? accs[i] : acc[r][j];
-        const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
-        acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - c);
-      }
-  }
-  if (*s_abort) return;
-
-  // four rotated columns: (x, z) -> (n-1-z, x) -> (n-1-x, n-1-z) -> (z, n-1-x)
-  const int n = a.nx;
-  const int ix = ix0 + tx, iz = iz0 + tz;
-  const int cx[4] = {ix, n - 1 - iz, n - 1 - ix, iz};
-  const int cz[4] = {iz, ix, n - 1 - iz, n - 1 - ix};
-  float lo = __int_as_float(0x7f800000), hi = -lo;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    float* out = a.vol + ((size_t)cz[r] * a.vol_ystride) * a.nx + cx[r];
-#pragma unroll
-    for (int j = 0; j < NY; ++j) {
-      const int iy = iy0 + j;
-      if (iy < a.ny) {
-        float val = acc[r][j] * a.scale;
-        if (iy < a.clip_ylimit) val = fmaxf(val, 0.f);
-        out[(size_t)iy * a.nx] = val;
-        lo = fminf(lo, val);
-        hi = fmaxf(hi, val);
-      }
+    if (last) {
+      if (bad) atomicCAS(job_args<MULTI>(a, qq, jb).err, 0, kDevFootprint);
+      bad = false;
+      if (*s_abort) break;
+      store();
+      if (!MULTI) break;
+      reset();
+      kq = 0;
+      last = false;
     }
   }
-  if (a.minmax) fold_minmax(a.minmax, lo, hi);
+  if (bad) atomicCAS(err, 0, kDevFootprint);
 }
 
 // Footprint pre-pass: one warp per tile (lanes over views) finds the
@@ -1138,35 +1305,42 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
   return cudaGetLastError();
 }
 
-template <int LAYOUT>
+template <int LAYOUT, int NY, int OCC>
 cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
-  auto kern = bp_quad_kernel<LAYOUT, 8, false>;
+  auto kern = bp_quad_kernel<LAYOUT, NY, false, OCC, false>;
   if constexpr (LAYOUT != kLayoutQuadG24)  // the 24-bit layout runs without compensation
-    if (kahan) kern = bp_quad_kernel<LAYOUT, 8, true>;
+    if (kahan) kern = bp_quad_kernel<LAYOUT, NY, true, OCC, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   // all of L1 as shared memory, so that two CTAs of up to 113 KB share an SM
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  dim3 grid((a.ntx / 2) * (a.ntz / 2), (a.ny + 7) / 8);
-  kern<<<grid, 256 + 32, smem, stream>>>(maps, a);
+  dim3 grid((a.ntx / 2) * (a.ntz / 2), (a.ny + NY - 1) / NY);
+  kern<<<grid, 256 + 32, smem, stream>>>(maps, a, QuadQueue{});
   return cudaGetLastError();
 }
 
-cudaError_t launch_quad(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
-                        cudaStream_t stream) {
+template <int NY, int OCC>
+cudaError_t launch_quad_ny(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
+                           cudaStream_t stream) {
   switch (layout) {
     case kLayoutPair32:
-      return launch_quad_cfg<kLayoutPair32>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutPair32, NY, OCC>(maps, a, smem, kahan, stream);
     case kLayoutPair16:
-      return launch_quad_cfg<kLayoutPair16>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutPair16, NY, OCC>(maps, a, smem, kahan, stream);
     case kLayoutQuadG16:
-      return launch_quad_cfg<kLayoutQuadG16>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutQuadG16, NY, OCC>(maps, a, smem, kahan, stream);
     case kLayoutQuadG24:
-      return launch_quad_cfg<kLayoutQuadG24>(maps, a, smem, false, stream);
+      return launch_quad_cfg<kLayoutQuadG24, NY, OCC>(maps, a, smem, false, stream);
     default:
-      return launch_quad_cfg<kLayoutRaw32>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutRaw32, NY, OCC>(maps, a, smem, kahan, stream);
   }
+}
+
+cudaError_t launch_quad(int layout, int ny_tile, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
+                        cudaStream_t stream) {
+  return ny_tile == 16 ? launch_quad_ny<16, 1>(layout, maps, a, smem, kahan, stream)
+                       : launch_quad_ny<8, 2>(layout, maps, a, smem, kahan, stream);
 }
 
 template <int TX, int TZ, int NY>
@@ -1184,7 +1358,21 @@ cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size
 
 }  // namespace
 
-int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed) {
+// A planned backprojection: everything a launch needs (arguments, tensor
+// maps, shared memory) after the footprint pass and the packing.
+struct BPLaunchPlan {
+  BPArgs a;
+  BoxMaps maps;
+  size_t smem = 0;
+  int layout = 0, ny_tile = 0, occ = 2;
+  bool use_quad = false, kahan = false, is2d = false;
+};
+
+BPLaunchPlan* new_bp_plan() { return new BPLaunchPlan(); }
+void free_bp_plan(BPLaunchPlan* p) { delete p; }
+
+int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed,
+                     BPLaunchPlan* plan_out) {
   const double pi = 3.14159265358979323846;
   // MIXED24: 24-bit views for the symmetric kernel (FP32 rows otherwise), no
   // compensation (FP32 sums of FP32-precise taps, as the FP32 form)
@@ -1282,7 +1470,11 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   a.trig = ctx->d_trig;
 
   // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
-  const int TX = 16, TZ = 16, NY = is2d ? 1 : (quad || ctx->bp_variant == FBP_BACKPROJECTOR_GENERIC_Y8 ? 8 : 16);
+  // symmetric kernel: 16 voxels per thread along y with one CTA per SM, or 8
+  // with two (a per-context choice; 0 = 16)
+  const int quad_ny = ctx->quad_tile_ny == 8 ? 8 : 16;
+  const int TX = 16, TZ = 16,
+            NY = is2d ? 1 : quad ? quad_ny : (ctx->bp_variant == FBP_BACKPROJECTOR_GENERIC_Y8 ? 8 : 16);
   a.ntx = (g.nx + TX - 1) / TX;
   a.ntz = (g.nz + TZ - 1) / TZ;
   const int nty = (g.ny + NY - 1) / NY;
@@ -1342,8 +1534,10 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
                      "too large for the staged backprojector");
   a.box_u = bu;
   a.box_v = bv;
-  // two CTAs per SM: each gets half of the 228 KB shared memory
-  const size_t smem_cap = 113 * 1024;
+  // two CTAs per SM: each gets half of the 228 KB shared memory; the
+  // symmetric kernel with 16 voxels per thread runs one CTA per SM
+  const int occ = (quad && NY == 16) ? 1 : 2;
+  const size_t smem_cap = occ == 1 ? (size_t)kMaxDynamicSmem : 113 * 1024;
   const size_t max_box = (size_t)(bu * bv * esize + 127) / 128 * 128;
   size_t smem = 0;
   bool use_quad = quad;
@@ -1351,8 +1545,8 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     // byte ring for the windows + entry records (+ Kahan compensations)
     const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(int)) + 64;
     // Kahan compensations (interleaved layout: FP32 running sums + BF16 compensations)
-    const size_t comp = !kahan ? 0 : layout == kLayoutQuadG16 ? (size_t)4 * 8 * 256 * (4 + 2)
-                                                              : (size_t)4 * 8 * 256 * sizeof(float);
+    const size_t comp = !kahan ? 0 : layout == kLayoutQuadG16 ? (size_t)4 * NY * 256 * (4 + 2)
+                                                              : (size_t)4 * NY * 256 * sizeof(float);
     const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
     // the interleaved layout gathers windows that do not fit from global memory
     const size_t entry = is_quad_layout(layout) ? 0 : 4 * max_box;
@@ -1370,7 +1564,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
       // re-plan with the generic tile height
       const int saved = ctx->bp_variant;
       ctx->bp_variant = FBP_BACKPROJECTOR_GENERIC;
-      const int rc = launch_backproject(ctx, g, st, vol, clip_ylimit, mixed);
+      const int rc = plan_backproject(ctx, g, st, vol, clip_ylimit, mixed, plan_out);
       ctx->bp_variant = saved;
       return rc;
     }
@@ -1386,7 +1580,7 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
   if (packed && !(st.pack_ready && st.filt_layout == layout))
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
-  a.resident = 2 * ctx->num_sms;  // symmetric kernel: two CTAs per SM
+  a.resident = occ * ctx->num_sms;  // CTAs resident at once (view-group skew of the symmetric kernel)
   if (is_quad_layout(layout)) {
     a.qg = static_cast<const uint4*>(st.filt);
     a.qg_pitch = st.filt_pitch;
@@ -1454,20 +1648,152 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
     if (int rc = launch_minmax_init(ctx, ctx->d_minmax)) return rc;
     a.minmax = ctx->d_minmax;
   }
-  ctx->last_bp[0] = use_quad    ? FBP_BACKPROJECTOR_SYMMETRIC
+  BPLaunchPlan& p = *plan_out;
+  p.a = a;
+  p.maps = maps;
+  p.smem = smem;
+  p.layout = layout;
+  p.ny_tile = NY;
+  p.occ = occ;
+  p.use_quad = use_quad;
+  p.kahan = kahan;
+  p.is2d = is2d;
+  return FBP_OK;
+}
+
+int launch_bp_plan(fbp_context* ctx, const BPLaunchPlan& p) {
+  const int NY = p.ny_tile;
+  ctx->last_bp[0] = p.use_quad  ? FBP_BACKPROJECTOR_SYMMETRIC
                     : NY == 8   ? FBP_BACKPROJECTOR_GENERIC_Y8
                                 : FBP_BACKPROJECTOR_GENERIC;
-  ctx->last_bp[1] = layout;
-  ctx->last_bp[2] = bu;
-  ctx->last_bp[3] = bv;
+  ctx->last_bp[1] = p.layout;
+  ctx->last_bp[2] = p.a.box_u;
+  ctx->last_bp[3] = p.a.box_v;
   ctx->last_bp[4] = NY;
-  cudaError_t e = use_quad    ? launch_quad(layout, maps, a, smem, kahan, ctx->stream)
-                 : is2d      ? launch_layout<16, 16, 1>(layout, maps, a, smem, kahan, ctx->stream)
-                 : NY == 8   ? launch_layout<16, 16, 8>(layout, maps, a, smem, kahan, ctx->stream)
-                             : launch_layout<16, 16, 16>(layout, maps, a, smem, kahan, ctx->stream);
+  cudaError_t e = p.use_quad ? launch_quad(p.layout, NY, p.maps, p.a, p.smem, p.kahan, ctx->stream)
+                  : p.is2d   ? launch_layout<16, 16, 1>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream)
+                  : NY == 8  ? launch_layout<16, 16, 8>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream)
+                             : launch_layout<16, 16, 16>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
-  ctx->minmax_valid = e == cudaSuccess && a.minmax != nullptr;
+  ctx->minmax_valid = e == cudaSuccess && p.a.minmax != nullptr;
   return cuda_check(ctx, e, "bp_kernel");
+}
+
+int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed) {
+  BPLaunchPlan p;
+  if (int rc = plan_backproject(ctx, g, st, vol, clip_ylimit, mixed, &p)) return rc;
+  return launch_bp_plan(ctx, p);
+}
+
+long long bp_plan_batch_key(const BPLaunchPlan& p) {
+  if (!p.use_quad) return 0;  // the persistent launch runs the four-fold symmetric kernel
+  return 1 + p.layout + 16LL * p.ny_tile + 1024LL * (p.kahan ? 1 : 0) + 4096LL * p.occ + 65536LL * p.a.box_bytes;
+}
+
+namespace {
+
+template <int LAYOUT, int NY, int OCC>
+cudaError_t launch_quad_multi_cfg(const QuadQueue& qq, size_t smem, bool kahan, int grid, cudaStream_t stream) {
+  auto kern = bp_quad_kernel<LAYOUT, NY, false, OCC, true>;
+  if constexpr (LAYOUT != kLayoutQuadG24)
+    if (kahan) kern = bp_quad_kernel<LAYOUT, NY, true, OCC, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  static const BoxMaps no_maps{};
+  static const BPArgs no_args{};
+  kern<<<grid, 256 + 32, smem, stream>>>(no_maps, no_args, qq);
+  return cudaGetLastError();
+}
+
+template <int NY, int OCC>
+cudaError_t launch_quad_multi_ny(int layout, const QuadQueue& qq, size_t smem, bool kahan, int grid,
+                                 cudaStream_t stream) {
+  switch (layout) {
+    case kLayoutPair32:
+      return launch_quad_multi_cfg<kLayoutPair32, NY, OCC>(qq, smem, kahan, grid, stream);
+    case kLayoutQuadG16:
+      return launch_quad_multi_cfg<kLayoutQuadG16, NY, OCC>(qq, smem, kahan, grid, stream);
+    case kLayoutQuadG24:
+      return launch_quad_multi_cfg<kLayoutQuadG24, NY, OCC>(qq, smem, false, grid, stream);
+    default:
+      return cudaErrorInvalidValue;  // other layouts run one launch per job
+  }
+}
+
+}  // namespace
+
+// Several jobs' symmetric backprojections (plans with one batch key) in one
+// persistent launch on the launcher's stream: OCC CTAs per SM walk a queue
+// of (job, tile orbit, y-slab) work items, largest jobs first in the order
+// given. The job table goes up through the launcher's pinned staging.
+int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n) {
+  if (n <= 0) return FBP_OK;
+  const BPLaunchPlan& p0 = *plans[0];
+  const long long key = bp_plan_batch_key(p0);
+  if (key == 0) return set_error(L, FBP_ERR_INVALID_ARGUMENT, "backprojection plan cannot run in a batch");
+  if (p0.layout != kLayoutPair32 && p0.layout != kLayoutQuadG16 && p0.layout != kLayoutQuadG24)
+    return set_error(L, FBP_ERR_UNSUPPORTED, "batched backprojection supports FP32 pairs and interleaved quads");
+  const size_t jobs_bytes = (sizeof(QuadJob) * n + 63) / 64 * 64;
+  const size_t maps_bytes = sizeof(BoxMaps) * n;
+  const size_t bytes = jobs_bytes + maps_bytes + 64;
+  if (L->batch_cap < bytes) {
+    cudaFree(L->d_batch);
+    L->d_batch = nullptr;
+    L->batch_cap = 0;
+    if (cuda_check(L, cudaMalloc(&L->d_batch, bytes), "cudaMalloc(batch table)")) return FBP_ERR_OUT_OF_MEMORY;
+    L->batch_cap = bytes;
+  }
+  if (L->h_batch_cap < bytes) {
+    // the previous table may still be on its way up
+    if (L->h_batch && cuda_check(L, cudaStreamSynchronize(L->stream), "batch staging sync")) return FBP_ERR_CUDA;
+    cudaFreeHost(L->h_batch);
+    L->h_batch = nullptr;
+    L->h_batch_cap = 0;
+    if (cuda_check(L, cudaMallocHost(&L->h_batch, bytes), "cudaMallocHost(batch table)")) return FBP_ERR_OUT_OF_MEMORY;
+    L->h_batch_cap = bytes;
+  } else if (L->ev_batch_copy) {
+    if (cuda_check(L, cudaEventSynchronize(L->ev_batch_copy), "batch staging reuse")) return FBP_ERR_CUDA;
+  }
+  unsigned char* h = static_cast<unsigned char*>(L->h_batch);
+  QuadJob* hj = reinterpret_cast<QuadJob*>(h);
+  BoxMaps* hm = reinterpret_cast<BoxMaps*>(h + jobs_bytes);
+  long long items = 0;
+  for (int i = 0; i < n; ++i) {
+    const BPLaunchPlan& p = *plans[i];
+    if (bp_plan_batch_key(p) != key)
+      return set_error(L, FBP_ERR_INVALID_ARGUMENT, "a batch needs one staged layout, tile height and ring size");
+    hj[i] = QuadJob{};
+    hj[i].a = p.a;
+    hj[i].a.minmax = nullptr;  // no histogram range for batched jobs
+    hj[i].item0 = items;
+    hj[i].nbh = p.a.ntx >> 1;
+    hj[i].nty = (p.a.ny + p.ny_tile - 1) / p.ny_tile;
+    hm[i] = p.maps;
+    items += (long long)hj[i].nbh * hj[i].nbh * hj[i].nty;
+  }
+  *reinterpret_cast<unsigned long long*>(h + jobs_bytes + maps_bytes) = 0ull;
+  unsigned char* d = static_cast<unsigned char*>(L->d_batch);
+  if (cuda_check(L, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, L->stream), "batch table upload"))
+    return FBP_ERR_CUDA;
+  if (!L->ev_batch_copy && cuda_check(L, cudaEventCreateWithFlags(&L->ev_batch_copy, cudaEventDisableTiming),
+                                      "batch event"))
+    return FBP_ERR_CUDA;
+  if (cuda_check(L, cudaEventRecord(L->ev_batch_copy, L->stream), "batch event record")) return FBP_ERR_CUDA;
+  QuadQueue qq;
+  qq.jobs = reinterpret_cast<const QuadJob*>(d);
+  qq.maps = reinterpret_cast<const BoxMaps*>(d + jobs_bytes);
+  qq.njobs = n;
+  qq.nitems = items;
+  qq.next = reinterpret_cast<unsigned long long*>(d + jobs_bytes + maps_bytes);
+  qq.err = L->d_err;
+  qq.ring = p0.a.box_bytes;
+  const int grid = (int)std::min<long long>(items, (long long)p0.occ * L->num_sms);
+  cudaError_t e = p0.ny_tile == 16 ? launch_quad_multi_ny<16, 1>(p0.layout, qq, p0.smem, p0.kahan, grid, L->stream)
+                                   : launch_quad_multi_ny<8, 2>(p0.layout, qq, p0.smem, p0.kahan, grid, L->stream);
+  if (e == cudaSuccess) L->launches++;
+  return cuda_check(L, e, "bp_quad_kernel (batch)");
 }
 
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit) {

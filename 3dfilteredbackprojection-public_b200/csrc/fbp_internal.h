@@ -114,6 +114,7 @@ struct fbp_context {
   int pad_len = 0;
   int clip_after_bp = 1;
   int bp_variant = FBP_BACKPROJECTOR_AUTO;
+  int quad_tile_ny = 0;  // symmetric backprojector: voxels per thread along y (8 or 16; 0 = 16)
   int det_row_off = 0, det_rows_total = 0;  // fbp_set_detector_rows (0 rows: the whole detector)
   int slab_y0 = 0, slab_ny = 0;             // fbp_set_volume_slab (0 slices: the whole volume)
   int last_bp[5] = {-1, -1, 0, 0, 0};  // variant, layout, box_u, box_v, tile height of the last backprojection
@@ -160,6 +161,13 @@ struct fbp_context {
   } plans[16];
   int plan_next = 0;
   cudaStream_t copy_stream = nullptr;  // slab readback beside the backprojection (created on first use)
+  // batched backprojection launched from this context (grow only)
+  void* d_batch = nullptr;             // job table, tensor maps and work counter
+  size_t batch_cap = 0;
+  void* h_batch = nullptr;             // pinned staging of the table
+  size_t h_batch_cap = 0;
+  cudaEvent_t ev_batch_copy = nullptr; // the staged table has gone up
+  cudaEvent_t ev_sync = nullptr;       // cross-stream ordering of batched jobs
 };
 
 namespace fbp {
@@ -232,6 +240,17 @@ struct BPGeom {
 // the MIXED form (`mixed`) f32 content is first packed into the FP16 layout
 // the selected kernel reads (prepare_packed), with Kahan-compensated sums.
 int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed);
+// The same in two steps: plan (footprint pass, packing, tensor maps; work on
+// ctx's stream) and launch. Plans with the same non-zero batch key can also run
+// together in one persistent launch on another context's stream.
+struct BPLaunchPlan;
+BPLaunchPlan* new_bp_plan();
+void free_bp_plan(BPLaunchPlan* p);
+int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed,
+                     BPLaunchPlan* plan);
+int launch_bp_plan(fbp_context* ctx, const BPLaunchPlan& p);
+long long bp_plan_batch_key(const BPLaunchPlan& p);
+int launch_bp_batch(fbp_context* launcher, BPLaunchPlan* const* plans, int n);
 // (fbp_api.cu) size the stack's packed buffer for `layout`, compute the
 // per-view scales and pack the f32 rows into it.
 int prepare_packed(fbp_context* ctx, Stack& s, int layout);

@@ -114,6 +114,9 @@ SIGNATURES = {
     "fbp_last_backprojection": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int)],
     "fbp_set_autotune": [_P, _I],
+    "fbp_set_symmetric_tile": [_P, _I],
+    "fbp_project_backward_cone_fdk_batch": [C.POINTER(C.c_void_p), C.POINTER(Geometry), C.POINTER(_I),
+                                            C.POINTER(_I), _I, _P],
     "fbp_generate_blank_volume": [_P, _I, _I, _I],
     "fbp_generate_blank_projections": [_P, _I, _I, _I],
     "fbp_generate_blank_sinograms": [_P, _I, _I, _I],
@@ -258,6 +261,22 @@ def plan_slabs(geometry: "Geometry", detector_cols: int, detector_rows: int, vol
     return [tuple(out[4 * k:4 * k + 4]) for k in range(slabs)]
 
 
+def project_backward_cone_fdk_batch(solvers: list, geometries: list, volume_sizes: list, launcher=None) -> None:
+    """fbp_project_backward_cone_fdk_batch: each solver's FDK backprojection
+    (its pending weights, filter, precision and clip setting), the jobs on the
+    symmetric backprojector in one persistent launch on the launcher's stream.
+    volume_sizes: (h, v) per job. Asynchronous; each solver's later calls are
+    ordered after the batch."""
+    n = len(solvers)
+    ctxs = (C.c_void_p * n)(*[s.ctx.handle for s in solvers])
+    geoms = (Geometry * n)(*geometries)
+    hs = (C.c_int * n)(*[int(h) for h, _ in volume_sizes])
+    vs = (C.c_int * n)(*[int(v) for _, v in volume_sizes])
+    launch = (launcher or solvers[0]).ctx
+    launch._check(launch.lib.fbp_project_backward_cone_fdk_batch(ctxs, geoms, hs, vs, n, launch.handle),
+                  launch.handle)
+
+
 def library() -> C.CDLL:
     """Load libfbp_b200.so; raises if it has not been built."""
     global _lib
@@ -374,6 +393,10 @@ class FBP3D:
         kernels = {Backprojector.SYMMETRIC: "symmetric", Backprojector.GENERIC_Y8: "generic_y8"}
         return {"kernel": kernels.get(v.value, "generic"),
                 "layout": names.get(l.value, str(l.value)), "box": (bu.value, bv.value), "tile_ny": ny.value}
+
+    def set_symmetric_tile(self, voxels_per_thread_y: int) -> None:
+        """Voxels per thread along y of the symmetric backprojector (8, 16; 0 = 16)."""
+        self.ctx.call("fbp_set_symmetric_tile", int(voxels_per_thread_y))
 
     def set_autotune(self, enable: bool) -> None:
         """Time the backprojector variants on the first backprojection of each geometry and keep the fastest."""

@@ -76,6 +76,8 @@ def parse_args():
                         "split into y-slabs, each rank holding its detector row band (strong scaling)")
     p.add_argument("--backprojector", choices=["auto", "generic", "generic_y8", "symmetric", "tuned"], default="auto",
                    help="backprojector variant of both forms (tuned: timed per geometry on first use)")
+    p.add_argument("--tile-ny", type=int, default=0, choices=[0, 8, 16],
+                   help="voxels per thread along y of the symmetric backprojector (0: the library default)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--oracle-voxels", type=int, default=1000000,
                    help="uniformly drawn voxels of the sampled FP64-oracle accuracy check (0: skip the check)")
@@ -569,6 +571,8 @@ def main() -> None:
         s.set_stream(stream if on_stream is None else on_stream)
         s.set_precision(getattr(F.Precision, FORMS[form][0]))
         s.set_clip_after_backprojection(True)
+        if args.tile_ny:
+            s.set_symmetric_tile(args.tile_ny)
         if args.backprojector == "tuned":
             s.set_autotune(True)
         elif args.backprojector != "auto":

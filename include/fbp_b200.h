@@ -127,6 +127,10 @@ int fbp_set_backprojector(fbp_context* ctx, int variant);
  * symmetric kernel when the geometry allows it. No counterpart in the
  * reference, whose backprojection is one fixed shader. */
 int fbp_set_autotune(fbp_context* ctx, int enable);
+/* Voxels per thread along y of the four-fold symmetric backprojector: 16
+ * (one CTA per SM, 64 accumulators a thread) or 8 (two CTAs per SM); 0 (the
+ * default) = 16. No counterpart in the reference. */
+int fbp_set_symmetric_tile(fbp_context* ctx, int voxels_per_thread_y);
 /* Device bytes held by ctx's buffers. */
 int fbp_memory_in_use(const fbp_context* ctx, size_t* bytes);
 /* What the last backprojection ran (no counterpart in the reference, whose
@@ -317,6 +321,23 @@ int fbp_project_backward_parallel_from_projections(fbp_context* ctx, float full_
     int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :460-490 */
 int fbp_project_backward_parallel_from_sinograms(fbp_context* ctx, float full_rotation_count,
     int volume_resolution_horizontal, int volume_resolution_vertical, float rotation_offset_radian);  /* :492-522 */
+/* Several cone-beam FDK backprojections at once (no counterpart in the
+ * reference, one reconstruction per GL context): for each i, what
+ * fbp_project_backward_cone_fdk_from_projections(contexts[i], geometries[i]...,
+ * volume_h[i], volume_v[i]) computes - pending weights / log and the filter,
+ * each job's clip setting and precision form - but the jobs that run the
+ * four-fold symmetric backprojector with the same staged layout share ONE
+ * persistent launch on `launcher`'s stream: OCC CTAs per SM take (job, tile
+ * orbit, y-slab) work items from a device-side queue, so jobs of uneven size
+ * (volume, detector, views) fill the GPU together and small jobs use the SMs
+ * that a large job's last tiles leave idle. Each job's volume is bit-identical
+ * to the same job batched with any others or alone. Other jobs launch on their
+ * own streams. Asynchronous: each context's later work is ordered after the
+ * batch. A device-side wait that expires in the batched launch is reported by
+ * the launcher; geometry checks by the job's context. All contexts on one
+ * device; the launcher may be one of them. */
+int fbp_project_backward_cone_fdk_batch(fbp_context* const* contexts, const fbp_geometry* geometries,
+                                        const int* volume_h, const int* volume_v, int count, fbp_context* launcher);
 /* One call for the whole cone-beam FDK (weight + filter + backprojection +
  * optional clip) on the resident projections, geometry as above. */
 int fbp_reconstruct_fdk(fbp_context* ctx, const fbp_geometry* geometry, int filter_type,

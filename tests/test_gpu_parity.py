@@ -335,6 +335,58 @@ def test_mixed_seed_sweep(fbp, oracle, phantoms, factor, seed):
     assert err < TOL_MIXED_SWEEP
 
 
+def _batch_case(phantoms, oracle, factor, nviews, seed):
+    c = dict(phantoms.scaled_cone(phantoms.config_cone256(), factor), nviews=nviews, seed=seed)
+    return c, oracle.project_ellipsoids_cone(phantoms.ellipsoids_for(c), c)
+
+
+@pytest.mark.parametrize("precision", ["MIXED", "FP32"])
+def test_batched_backprojection_equals_each_job_alone(fbp, oracle, phantoms, precision):
+    """fbp_project_backward_cone_fdk_batch: jobs of uneven size (volume,
+    detector, views) in one persistent launch give each job's volume bit for
+    bit as the same job batched alone, agree with the one-job kernel and with
+    the FP64 oracle; a job off the symmetric path (90 views) runs beside them."""
+    cases = [_batch_case(phantoms, oracle, 4, 96, 21), _batch_case(phantoms, oracle, 2, 180, 22),
+             _batch_case(phantoms, oracle, 8, 48, 23), _batch_case(phantoms, oracle, 4, 90, 24)]
+
+    def solver_for(c, proj):
+        s = fbp.FBP3D(0)
+        s.set_clip_after_backprojection(False)
+        s.set_precision(getattr(fbp.Precision, precision))
+        sod, odd, w, vw, rot = _cone_args(c)
+        s.upload_projections(proj)
+        s.apply_fdk_weights_to_projections(sod, odd, w)
+        s.apply_filter_to_projections(0)
+        return s
+
+    def geom(c):
+        sod, odd, w, vw, rot = _cone_args(c)
+        return fbp.Geometry.cone(sod, odd, w, vw, rot, c["offset"])
+
+    sizes = [(c["nx"], c["ny"]) for c, _ in cases]
+    together = [solver_for(c, p) for c, p in cases]
+    fbp.project_backward_cone_fdk_batch(together, [geom(c) for c, _ in cases], sizes)
+    vols = [s.read_volume() for s in together]
+    for (c, proj), vol, s_t in zip(cases, vols, together):
+        alone = solver_for(c, proj)
+        fbp.project_backward_cone_fdk_batch([alone], [geom(c)], [(c["nx"], c["ny"])])
+        assert np.array_equal(alone.read_volume(), vol), c["nviews"]
+        one_kernel = solver_for(c, proj)
+        sod, odd, w, vw, rot = _cone_args(c)
+        one_kernel.project_backward_cone_fdk_from_projections(sod, odd, w, vw, rot, c["nx"], c["ny"], c["offset"])
+        single = one_kernel.read_volume()
+        ref = oracle.fdk(proj, c, 0)
+        err = relative_rmse(vol, ref)
+        print(f"batch {precision} {c['nx']}^3 / {c['nviews']} views: vs oracle {err:.2e}, "
+              f"vs one-job kernel {relative_rmse(vol, single):.1e} (bit-equal {np.array_equal(vol, single)})")
+        assert relative_rmse(vol, single) < 1e-6
+        assert err < (TOL_MIXED if precision == "MIXED" else TOL_FP32)
+        for x in (alone, one_kernel):
+            x.ctx.close()
+    for s in together:
+        s.ctx.close()
+
+
 @pytest.mark.parametrize("square", [True, False])
 def test_mixed24_cone(fbp, oracle, phantoms, square):
     """MIXED24 through the symmetric kernel (24-bit interleaved quads) and, for a
