@@ -1211,6 +1211,23 @@ int fbp_project_backward_cone_fdk_from_projections(fbp_context* ctx, float sod, 
   return backproject(ctx, ctx->proj, cone_geom(ctx->proj, sod, odd, det_w, vol_w, rot, h, v, offset));
 }
 
+}  // extern "C"
+
+namespace fbp {
+int plan_cone_projections(fbp_context* c, const fbp_geometry& ge, int h, int v, BPLaunchPlan* plan) {
+  DeviceGuard guard(c->device);
+  FBP_TRY(require_stack(c, c->proj, "cone backprojection"));
+  fbp::BPGeom g = cone_geom(c->proj, ge.source_distance, ge.detector_distance, ge.detector_width, ge.volume_width,
+                            ge.full_rotation_count, h, v, ge.rotation_offset_radian);
+  int ylim = 0;
+  bool mixed = false;
+  FBP_TRY(setup_backproject(c, c->proj, g, &ylim, &mixed));
+  return fbp::plan_backproject(c, g, c->proj, c->vol, ylim, mixed, plan);
+}
+}  // namespace fbp
+
+extern "C" {
+
 int fbp_project_backward_cone_fdk_batch(fbp_context* const* contexts, const fbp_geometry* geometries,
                                         const int* volume_h, const int* volume_v, int count, fbp_context* launcher) {
   FBP_CTX(launcher);
@@ -1231,16 +1248,8 @@ int fbp_project_backward_cone_fdk_batch(fbp_context* const* contexts, const fbp_
   // plan every job on its own stream (weights, filter, packing, footprint pass)
   for (int i = 0; i < count; ++i) {
     fbp_context* c = contexts[i];
-    const fbp_geometry& ge = geometries[i];
-    FBP_TRY(require_stack(c, c->proj, "project_backward_cone_fdk_batch"));
-    fbp::BPGeom g = cone_geom(c->proj, ge.source_distance, ge.detector_distance, ge.detector_width, ge.volume_width,
-                              ge.full_rotation_count, volume_h[i], volume_v[i], ge.rotation_offset_radian);
-    int ylim = 0;
-    bool mixed = false;
-    if (int rc = setup_backproject(c, c->proj, g, &ylim, &mixed))
-      return fbp::set_error(launcher, rc, std::string("batch job ") + std::to_string(i) + ": " + c->last_error);
     plans.p.push_back(fbp::new_bp_plan());
-    if (int rc = fbp::plan_backproject(c, g, c->proj, c->vol, ylim, mixed, plans.p.back()))
+    if (int rc = fbp::plan_cone_projections(c, geometries[i], volume_h[i], volume_v[i], plans.p.back()))
       return fbp::set_error(launcher, rc, std::string("batch job ") + std::to_string(i) + ": " + c->last_error);
   }
   auto event = [&](fbp_context* c) -> cudaEvent_t {

@@ -609,13 +609,15 @@ struct alignas(16) QuadCoef {
 static_assert(sizeof(QuadCoef) == 96, "six 16-byte loads per record");
 
 // Multi-job launch (several reconstructions in one persistent launch): one
-// entry per job in global memory; the work items of job j are
-// [item0, item0 + nbh * nbh * nty), ordered y-slab, then z, then x.
+// entry per job in global memory; work item item0 + i of job j is the job's
+// tile t0 + i (tiles ordered y-slab, then z, then x), so a launch can carry
+// a whole job or a range of its tiles.
 struct QuadJob {
   BPArgs a;
-  long long item0;
-  int nbh;  // representative tiles per axis
-  int nty;  // y-slabs
+  long long item0;  // first work item of the job in this launch
+  long long t0;     // its tile
+  int nbh;          // representative tiles per axis
+  int nty;          // y-slabs
 };
 struct QuadQueue {
   const QuadJob* jobs;    // sorted by item0
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
       const int jb = MULTI ? find_job(qq, item) : 0;
       const BPArgs& ja = job_args<MULTI>(a, qq, jb);
       const BoxMaps& jm = job_maps<MULTI>(maps, qq, jb);
-      const long long t_local = MULTI ? item - qq.jobs[jb].item0 : item;
+      const long long t_local = MULTI ? item - qq.jobs[jb].item0 + qq.jobs[jb].t0 : item;
       const ItemTile til = item_tile<QG, NY>(ja, t_local, MULTI ? qq.jobs[jb].nbh : ja.ntx >> 1);
       const int K = ja.nviews, Q = K >> 2;
       for (int kb = 0; kb < K && !*s_abort; kb += 32) {
@@ -956,7 +958,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
         if constexpr (MULTI) {
           jb = find_job(qq, item);
           const BPArgs& ja = qq.jobs[jb].a;
-          const ItemTile til = item_tile<QG, NY>(ja, item - qq.jobs[jb].item0, qq.jobs[jb].nbh);
+          const ItemTile til = item_tile<QG, NY>(ja, item - qq.jobs[jb].item0 + qq.jobs[jb].t0, qq.jobs[jb].nbh);
           grp = til.g0;
         } else {
           grp = item_tile<QG, NY>(a, item, a.ntx >> 1).g0;
@@ -1142,7 +1144,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
         }
     }
     const BPArgs& ja = job_args<MULTI>(a, qq, jb);
-    const ItemTile til = item_tile<QG, NY>(ja, MULTI ? item - qq.jobs[jb].item0 : item,
+    const ItemTile til = item_tile<QG, NY>(ja, MULTI ? item - qq.jobs[jb].item0 + qq.jobs[jb].t0 : item,
                                            MULTI ? qq.jobs[jb].nbh : a.ntx >> 1);
     const int n = ja.nx;
     const int ix = til.ix0 + tx, iz = til.iz0 + tz;
@@ -1728,7 +1730,12 @@ cudaError_t launch_quad_multi_ny(int layout, const QuadQueue& qq, size_t smem, b
 // persistent launch on the launcher's stream: OCC CTAs per SM walk a queue
 // of (job, tile orbit, y-slab) work items, largest jobs first in the order
 // given. The job table goes up through the launcher's pinned staging.
-int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n) {
+long long bp_plan_tiles(const BPLaunchPlan& p) {
+  return (long long)(p.a.ntx >> 1) * (p.a.ntx >> 1) * ((p.a.ny + p.ny_tile - 1) / p.ny_tile);
+}
+
+int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n, const long long* tile_begin,
+                    const long long* tile_end) {
   if (n <= 0) return FBP_OK;
   const BPLaunchPlan& p0 = *plans[0];
   const long long key = bp_plan_batch_key(p0);
@@ -1770,8 +1777,13 @@ int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n) {
     hj[i].item0 = items;
     hj[i].nbh = p.a.ntx >> 1;
     hj[i].nty = (p.a.ny + p.ny_tile - 1) / p.ny_tile;
+    const long long all = bp_plan_tiles(p);
+    const long long t0 = tile_begin ? std::max(0LL, tile_begin[i]) : 0;
+    const long long t1 = tile_end ? std::min(all, tile_end[i]) : all;
+    if (t1 <= t0) return set_error(L, FBP_ERR_INVALID_ARGUMENT, "empty tile range in a batch");
+    hj[i].t0 = t0;
     hm[i] = p.maps;
-    items += (long long)hj[i].nbh * hj[i].nbh * hj[i].nty;
+    items += t1 - t0;
   }
   *reinterpret_cast<unsigned long long*>(h + jobs_bytes + maps_bytes) = 0ull;
   unsigned char* d = static_cast<unsigned char*>(L->d_batch);

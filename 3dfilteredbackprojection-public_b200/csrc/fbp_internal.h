@@ -250,7 +250,15 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
                      BPLaunchPlan* plan);
 int launch_bp_plan(fbp_context* ctx, const BPLaunchPlan& p);
 long long bp_plan_batch_key(const BPLaunchPlan& p);
-int launch_bp_batch(fbp_context* launcher, BPLaunchPlan* const* plans, int n);
+long long bp_plan_tiles(const BPLaunchPlan& p);  // work items (tile orbits x y-slabs) of a batchable plan
+// Plan ctx's cone-beam FDK backprojection of its projections (pending
+// weights / filter, the volume buffer, footprint pass, packing) in the
+// reference API's geometry terms, without launching it (fbp_api.cu).
+int plan_cone_projections(fbp_context* ctx, const fbp_geometry& g, int h, int v, BPLaunchPlan* plan);
+// tile_begin / tile_end: the range of each job's tiles this launch computes
+// (nullptr: all of them)
+int launch_bp_batch(fbp_context* launcher, BPLaunchPlan* const* plans, int n, const long long* tile_begin = nullptr,
+                    const long long* tile_end = nullptr);
 // (fbp_api.cu) size the stack's packed buffer for `layout`, compute the
 // per-view scales and pack the f32 rows into it.
 int prepare_packed(fbp_context* ctx, Stack& s, int layout);

@@ -16,11 +16,27 @@
 // Worker buffers only grow (see alloc_stack), so after warm-up a slot stops
 // allocating; the budget covers the working sets of running jobs, and each
 // slot retains at most its largest job's buffers.
+//
+// Batching (on by default): a cone job's worker uploads, weights and filters
+// on its own (high-priority) stream, then hands the backprojection to the
+// server's engine thread. The engine plans each job (packing, footprint pass)
+// and feeds the tiles of all waiting jobs to the persistent multi-job
+// backprojector (launch_bp_batch): each launch carries about kChunkUpdates
+// voxel-view updates, taken from the jobs in arrival order, so a large job's
+// tiles are spread over several launches and jobs that arrive meanwhile join
+// the next one instead of waiting for the large job to finish. Launches
+// alternate between two launcher streams, so one launch's CTAs take the SMs
+// as the other's finish. A job's stream waits for every launch that computed
+// some of its tiles, then its worker reads the volume back. Each tile is
+// computed whole by one CTA in a fixed order, so a job's volume is the same
+// bits alone and in any mix. Jobs whose geometry does not take the symmetric
+// backprojector launch alone on their own stream.
 
 #include "fbp_internal.h"
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -34,6 +50,21 @@ namespace {
 using Clock = std::chrono::steady_clock;
 constexpr int kLookahead = 8;    // queued jobs looked at past a head that does not fit
 constexpr int kMaxBypass = 16;   // times a head may be passed over before it blocks the queue
+constexpr double kChunkUpdates = 6e10;  // voxel-view updates per batched launch (about 20 ms)
+
+// A cone job's backprojection handed from its worker to the engine.
+struct BatchJob {
+  fbp_context* ctx = nullptr;
+  fbp_geometry geom{};
+  int h = 0, v = 0;
+  fbp::BPLaunchPlan* plan = nullptr;
+  long long key = 0, tiles = 0, next = 0;
+  double per_tile = 0;    // voxel-view updates of one tile
+  bool planned = false;
+  bool launched = false;  // every tile launched; the job's stream waits for them
+  int status = FBP_OK;
+  std::string error;
+};
 
 struct Job {
   fbp_request req;
@@ -92,6 +123,17 @@ int device_buffer(float** p, size_t* cap, size_t bytes) {
 struct fbp_server {
   int device = -1;
   size_t budget = 0;
+  bool batching = true;
+  double chunk_updates = kChunkUpdates;  // voxel-view updates per batched launch
+  // engine: the persistent multi-job backprojector's feeder
+  std::thread engine;
+  fbp_context* launcher[2] = {nullptr, nullptr};
+  cudaEvent_t launched_ev[2] = {nullptr, nullptr};
+  bool launcher_busy[2] = {false, false};
+  std::deque<BatchJob*> incoming;  // handed over, not yet planned (under mu)
+  std::condition_variable engine_cv, batch_cv;
+  bool engine_stop = false;
+  std::vector<cudaStream_t> worker_streams;
   Clock::time_point t0;
   std::vector<Worker> workers;
   std::mutex mu;
@@ -136,7 +178,31 @@ struct fbp_server {
     }
     const fbp_geometry& g = r.geometry;
     int rc = fbp_set_precision(c, r.precision);
-    if (r.kind == FBP_JOB_CONE) {
+    if (r.kind == FBP_JOB_CONE && batching && launcher[0]) {
+      // upload, weights and filter here; the engine backprojects; then readback
+      if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
+      if (!rc) rc = fbp_upload_projections(c, r.input, r.det_cols, r.det_rows, r.views, 0);
+      if (!rc) rc = fbp_apply_fdk_weights_to_projections(c, g.source_distance, g.detector_distance, g.detector_width);
+      if (!rc) rc = fbp_apply_filter_to_projections(c, r.filter_type);
+      if (!rc) {
+        BatchJob bj;
+        bj.ctx = c;
+        bj.geom = g;
+        bj.geom.kind = FBP_GEOMETRY_CONE;
+        bj.h = r.vol_h;
+        bj.v = r.vol_v;
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          incoming.push_back(&bj);
+          engine_cv.notify_all();
+          batch_cv.wait(lk, [&] { return bj.launched || bj.status != FBP_OK; });
+        }
+        rc = bj.status;
+        if (rc) j.error = bj.error;
+        if (bj.plan) fbp::free_bp_plan(bj.plan);
+      }
+      if (!rc) rc = fbp_read_volume(c, r.output, 0);
+    } else if (r.kind == FBP_JOB_CONE) {
       // one call: upload, weights, filter, slab-wise backprojection with the
       // volume readback overlapped (large volumes in 4 slabs)
       fbp_geometry gc = g;
@@ -165,6 +231,118 @@ struct fbp_server {
     }
     if (rc && j.error.empty()) j.error = fbp_last_error(c);
     return rc;
+  }
+
+  // The engine thread: plans handed-over jobs and launches their tiles in
+  // chunks through the persistent multi-job backprojector.
+  void engine_main() {
+    if (device >= 0) cudaSetDevice(device);
+    std::vector<BatchJob*> active;
+    int turn = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        engine_cv.wait(lk, [&] { return !incoming.empty() || !active.empty() || engine_stop; });
+        if (engine_stop && incoming.empty() && active.empty()) break;
+        while (!incoming.empty()) {
+          active.push_back(incoming.front());
+          incoming.pop_front();
+        }
+      }
+      // plan new jobs on their own streams; jobs off the symmetric path launch alone
+      for (BatchJob* b : active) {
+        if (b->planned) continue;
+        b->planned = true;
+        b->plan = fbp::new_bp_plan();
+        int rc = fbp::plan_cone_projections(b->ctx, b->geom, b->h, b->v, b->plan);
+        if (!rc) {
+          b->key = fbp::bp_plan_batch_key(*b->plan);
+          if (b->key == 0) {
+            rc = fbp::launch_bp_plan(b->ctx, *b->plan);
+            b->next = b->tiles = 0;
+          } else {
+            b->tiles = fbp::bp_plan_tiles(*b->plan);
+            const double all = (double)b->h * b->h * b->v * (double)b->ctx->proj.n;
+            b->per_tile = all / (double)std::max(1LL, b->tiles);
+            // the job's preparatory work (on its stream) precedes every launch of its tiles
+            if (!b->ctx->ev_sync) cudaEventCreateWithFlags(&b->ctx->ev_sync, cudaEventDisableTiming);
+            if (cudaEventRecord(b->ctx->ev_sync, b->ctx->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
+          }
+        }
+        if (rc) {
+          b->status = rc;
+          b->error = fbp_last_error(b->ctx);
+        }
+      }
+      finish(active);
+      if (active.empty()) continue;
+      // one launch: tiles of the waiting jobs in arrival order, about
+      // kChunkUpdates updates, all of the first job's batch key
+      fbp_context* L = launcher[turn];
+      if (launcher_busy[turn]) cudaEventSynchronize(launched_ev[turn]);  // at most one launch per launcher in flight
+      const long long key = active.front()->key;
+      std::vector<fbp::BPLaunchPlan*> plans;
+      std::vector<long long> t0, t1;
+      std::vector<BatchJob*> members;
+      double budget;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        budget = chunk_updates;
+      }
+      for (BatchJob* b : active) {
+        if (b->key != key || budget <= 0) continue;
+        const long long want = (long long)std::ceil(budget / std::max(1.0, b->per_tile));
+        const long long take = std::max(1LL, std::min(b->tiles - b->next, want));
+        plans.push_back(b->plan);
+        t0.push_back(b->next);
+        t1.push_back(b->next + take);
+        members.push_back(b);
+        budget -= take * b->per_tile;
+      }
+      int rc = FBP_OK;
+      for (BatchJob* b : members)
+        if (cudaStreamWaitEvent(L->stream, b->ctx->ev_sync, 0) != cudaSuccess) rc = FBP_ERR_CUDA;
+      if (!rc) rc = fbp::launch_bp_batch(L, plans.data(), (int)plans.size(), t0.data(), t1.data());
+      if (!rc && cudaEventRecord(launched_ev[turn], L->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
+      launcher_busy[turn] = true;
+      for (size_t i = 0; i < members.size(); ++i) {
+        BatchJob* b = members[i];
+        if (rc) {
+          b->status = rc;
+          b->error = fbp_last_error(L);
+          continue;
+        }
+        if (cudaStreamWaitEvent(b->ctx->stream, launched_ev[turn], 0) != cudaSuccess) {
+          b->status = FBP_ERR_CUDA;
+          b->error = "stream wait on the batched backprojection failed";
+          continue;
+        }
+        b->next = t1[i];
+        b->ctx->last_bp[0] = FBP_BACKPROJECTOR_SYMMETRIC;
+        b->ctx->minmax_valid = false;
+      }
+      turn ^= 1;
+      finish(active);
+    }
+  }
+
+  // hand back the jobs that failed or have all their tiles launched
+  void finish(std::vector<BatchJob*>& active) {
+    bool any = false;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (auto it = active.begin(); it != active.end();) {
+        BatchJob* b = *it;
+        if (b->status != FBP_OK || (b->planned && b->next >= b->tiles)) {
+          b->launched = b->status == FBP_OK;
+          it = active.erase(it);
+          any = true;
+        } else {
+          ++it;
+        }
+      }
+    }
+    if (any) batch_cv.notify_all();
   }
 
   void worker_main(Worker& w) {
@@ -217,18 +395,53 @@ int fbp_server_create(fbp_server** out, int device, size_t hbm_budget_bytes, int
       cudaSetDevice(prev);
       hbm_budget_bytes = free_b / 10 * 8;  // 80 % of what is free now
     }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);  // hi: the highest priority (numerically least)
+    int rc = FBP_OK;
     for (auto& w : s->workers) {
-      const int rc = fbp_create(&w.ctx, device);
-      if (rc) {
-        for (auto& v : s->workers) fbp_destroy(v.ctx);
-        delete s;
-        return rc;
+      rc = fbp_create(&w.ctx, device);
+      if (rc) break;
+      // workers' uploads, filters and packing go ahead of queued backprojection launches
+      cudaStream_t st = nullptr;
+      if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess) {
+        rc = FBP_ERR_CUDA;
+        break;
       }
+      s->worker_streams.push_back(st);
+      rc = fbp_set_stream(w.ctx, st);
+      if (rc) break;
+    }
+    for (int i = 0; i < 2 && !rc; ++i) {
+      rc = fbp_create(&s->launcher[i], device);
+      if (!rc && cudaEventCreateWithFlags(&s->launched_ev[i], cudaEventDisableTiming) != cudaSuccess) rc = FBP_ERR_CUDA;
+    }
+    cudaSetDevice(prev);
+    if (rc) {
+      for (auto& v : s->workers) fbp_destroy(v.ctx);
+      for (int i = 0; i < 2; ++i) {
+        fbp_destroy(s->launcher[i]);
+        if (s->launched_ev[i]) cudaEventDestroy(s->launched_ev[i]);
+      }
+      for (cudaStream_t st : s->worker_streams) cudaStreamDestroy(st);
+      delete s;
+      return rc;
     }
   }
   s->budget = hbm_budget_bytes;
+  if (device >= 0) s->engine = std::thread([s] { s->engine_main(); });
   for (auto& w : s->workers) w.thread = std::thread([s, &w] { s->worker_main(w); });
   *out = s;
+  return FBP_OK;
+}
+
+int fbp_server_set_batching(fbp_server* s, int enable, double chunk_updates) {
+  if (!s) return FBP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->batching = enable != 0;
+  s->chunk_updates = chunk_updates > 0 ? chunk_updates : kChunkUpdates;
   return FBP_OK;
 }
 
@@ -282,11 +495,22 @@ int fbp_server_destroy(fbp_server* s) {
   s->work_cv.notify_all();
   for (auto& w : s->workers)
     if (w.thread.joinable()) w.thread.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->engine_stop = true;
+  }
+  s->engine_cv.notify_all();
+  if (s->engine.joinable()) s->engine.join();
   for (auto& w : s->workers) {
     cudaFree(w.d_in);
     cudaFree(w.d_out);
     fbp_destroy(w.ctx);
   }
+  for (int i = 0; i < 2; ++i) {
+    fbp_destroy(s->launcher[i]);
+    if (s->launched_ev[i]) cudaEventDestroy(s->launched_ev[i]);
+  }
+  for (cudaStream_t st : s->worker_streams) cudaStreamDestroy(st);
   for (auto& kv : s->jobs) delete kv.second;
   delete s;
   return FBP_OK;

@@ -167,6 +167,7 @@ SIGNATURES = {
     "fbp2d_project_forward": [_P, _P, _I, _I, _P, _I, _I, C.POINTER(Geometry)],
     "fbp_server_create": [C.POINTER(C.c_void_p), _I, C.c_size_t, _I],
     "fbp_server_submit": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
+    "fbp_server_set_batching": [C.c_void_p, _I, C.c_double],
     "fbp_server_wait": [C.c_void_p, C.c_longlong, C.c_void_p],
     "fbp_server_destroy": [C.c_void_p],
     "fbp_set_detector_rows": [_P, _I, _I],
@@ -217,6 +218,13 @@ class Server:
         if rc != 0:
             raise FBPError(rc, self.lib.fbp_last_error(None).decode())
         self._keep = {}
+
+    def set_batching(self, enable: bool, chunk_updates: float = 0.0) -> None:
+        """Cone backprojections through the persistent multi-job backprojector
+        (default on), in launches of about chunk_updates voxel-view updates."""
+        rc = self.lib.fbp_server_set_batching(self.handle, 1 if enable else 0, float(chunk_updates))
+        if rc != 0:
+            raise FBPError(rc, "fbp_server_set_batching failed")
 
     def submit(self, request: Request, keep=None) -> int:
         t = C.c_longlong()

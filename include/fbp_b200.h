@@ -276,6 +276,12 @@ typedef struct fbp_job_result {
 typedef struct fbp_server fbp_server;
 int fbp_server_create(fbp_server** server, int device, size_t hbm_budget_bytes, int slots);
 /* device < 0: no GPU, only FBP_JOB_HOST_WAIT jobs (tests of the scheduler). */
+/* enable 1 (default): cone jobs' backprojections go through the server's
+ * engine into the persistent multi-job backprojector (as in
+ * fbp_project_backward_cone_fdk_batch), their tiles launched in chunks of
+ * about chunk_updates voxel-view updates (<= 0: 6e10, about 20 ms) mixed
+ * with the other waiting jobs' tiles; 0: each job launches its own kernels. */
+int fbp_server_set_batching(fbp_server* server, int enable, double chunk_updates);
 int fbp_server_submit(fbp_server* server, const fbp_request* request, long long* ticket);
 int fbp_server_wait(fbp_server* server, long long ticket, fbp_job_result* result);
 int fbp_server_destroy(fbp_server* server); /* runs the queued jobs, then stops */

@@ -887,6 +887,30 @@ def test_server_results_alone_equal_results_in_the_mix(fbp):
         np.testing.assert_array_equal(a, m)
 
 
+def test_server_batched_chunks_equal_unbatched_jobs(fbp):
+    """The engine's chunked launches (a few tiles per launch, so every cone
+    job's tiles spread over many persistent launches mixed with the other
+    jobs') give the same bits as each job launching its own kernels alone."""
+    rng = np.random.default_rng(62)
+    reqs, keep, alone = _server_jobs(fbp, rng)
+    s = fbp.Server(0, 0, 1)
+    s.set_batching(False)
+    for r in reqs:
+        res = s.wait(s.submit(r))
+        assert res.status == 0, res.error
+    s.close()
+    mix = [np.empty_like(o) for o in alone]
+    for r, o in zip(reqs, mix):
+        r.output = o.ctypes.data
+    s = fbp.Server(0, 0, 4)
+    s.set_batching(True, chunk_updates=3e6)
+    res = [s.wait(t) for t in [s.submit(r) for r in reqs]]
+    s.close()
+    assert all(r.status == 0 for r in res), [r.error for r in res]
+    for a, m in zip(alone, mix):
+        np.testing.assert_array_equal(a, m)
+
+
 def test_server_cone_job_matches_oracle_and_bad_jobs_fail_alone(fbp, oracle, phantoms):
     c, proj = _cone_case(phantoms, oracle, 4)
     sod, odd, w, vw, rot = _cone_args(c)
