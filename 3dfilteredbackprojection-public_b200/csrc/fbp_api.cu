@@ -5,6 +5,9 @@
 
 #include "fbp_internal.h"
 
+#include <cstdio>
+#include <cstdlib>
+
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -340,18 +343,77 @@ fbp::BPGeom cone_geom(const Stack& s, float sod, float odd, float det_w, float v
 }
 
 // Autotuner: the first backprojection of a geometry (with autotuning on) times
-// each applicable kernel - the four-fold symmetric one and the generic one
-// with 16 or with 8 voxels per thread along y - on a central slab of up to 48
-// y-slices (written into the volume, which the real launch then overwrites)
-// and keeps the fastest for that geometry, form and stack layout.
-int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, bool mixed, int* variant) {
-  const double key[21] = {(double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu,
-                          (double)g.nv, (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz, (double)ctx->precision,
-                          (double)(s.filtered ? s.filt_layout : -1), (double)g.row_off, (double)g.nv_total,
-                          (double)g.y_off, (double)g.ny_total, (double)s.sinogram};
+// each applicable shape - the four-fold symmetric kernel with 16 voxels per
+// thread along y (one CTA per SM) or 8 (two CTAs per SM), the generic kernel
+// with 16 or 8 voxels per thread, each with its full view ring or a 4-stage
+// one - on a central slab of up to 48 y-slices (written into the volume,
+// which the real launch then overwrites) and keeps the fastest for that
+// geometry, form, stack layout and GPU. With a cache file set, choices are
+// read from it and new ones appended, so other processes skip the timing.
+using TuneShape = fbp_context::TuneShape;
+
+void tune_key(const fbp_context* ctx, const Stack& s, const fbp::BPGeom& g, double* key) {
+  const double k[fbp_context::kTuneKey] = {
+      (double)g.kind, g.sod, g.sdd, g.du, g.dv, g.vox, g.span, g.offset, (double)g.nu, (double)g.nv,
+      (double)g.nviews, (double)g.nx, (double)g.ny, (double)g.nz, (double)ctx->precision,
+      (double)(s.filtered ? s.filt_layout : -1), (double)g.row_off, (double)g.nv_total, (double)g.y_off,
+      (double)g.ny_total, (double)s.sinogram, (double)ctx->num_sms, (double)ctx->device_cc};
+  std::copy(k, k + fbp_context::kTuneKey, key);
+}
+
+void apply_shape(fbp_context* ctx, const TuneShape& t) {
+  ctx->bp_variant = t.variant;
+  ctx->quad_tile_ny = t.quad_ny;
+  ctx->bp_stages = t.stages;
+}
+
+// "key... | variant quad_ny stages ms" per line
+void load_tune_cache(fbp_context* ctx) {
+  ctx->tune_cache_loaded = true;
+  FILE* f = std::fopen(ctx->tune_cache.c_str(), "r");
+  if (!f) return;
+  char line[2048];
+  while (std::fgets(line, sizeof line, f)) {
+    fbp_context::TuneEntry t;
+    char* p = line;
+    bool ok = true;
+    for (int i = 0; i < fbp_context::kTuneKey && ok; ++i) {
+      char* end = nullptr;
+      t.key[i] = std::strtod(p, &end);
+      ok = end != p;
+      p = end;
+    }
+    if (!ok || std::sscanf(p, " | %d %d %d %f", &t.shape.variant, &t.shape.quad_ny, &t.shape.stages, &t.ms) != 4)
+      continue;
+    ctx->tuned.push_back(t);
+  }
+  std::fclose(f);
+}
+
+void store_tune_cache(const fbp_context* ctx, const fbp_context::TuneEntry& t) {
+  std::string line;
+  char buf[64];
+  for (int i = 0; i < fbp_context::kTuneKey; ++i) {
+    std::snprintf(buf, sizeof buf, "%.17g ", t.key[i]);
+    line += buf;
+  }
+  std::snprintf(buf, sizeof buf, "| %d %d %d %.4f\n", t.shape.variant, t.shape.quad_ny, t.shape.stages, t.ms);
+  line += buf;
+  // one short write in append mode: lines of concurrent processes do not interleave
+  if (FILE* f = std::fopen(ctx->tune_cache.c_str(), "a")) {
+    std::fwrite(line.data(), 1, line.size(), f);
+    std::fclose(f);
+  }
+}
+
+int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, bool mixed, TuneShape* best_shape) {
+  double key[fbp_context::kTuneKey];
+  tune_key(ctx, s, g, key);
+  if (!ctx->tune_cache.empty() && !ctx->tune_cache_loaded) load_tune_cache(ctx);
   for (const auto& t : ctx->tuned)
-    if (std::equal(key, key + 21, t.key)) {
-      *variant = t.variant;
+    if (std::equal(key, key + fbp_context::kTuneKey, t.key)) {
+      *best_shape = t.shape;
+      ++ctx->tune_cached;
       return FBP_OK;
     }
   const int nt = std::min(g.ny, 48), y0 = (g.ny - nt) / 2;
@@ -360,16 +422,18 @@ int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, boo
   gt.y_off = g.y_off + y0;
   gt.ny = nt;
   gt.vol_ystride = g.vol_ystride > 0 ? g.vol_ystride : g.ny;
-  const int cand[3] = {FBP_BACKPROJECTOR_SYMMETRIC, FBP_BACKPROJECTOR_GENERIC, FBP_BACKPROJECTOR_GENERIC_Y8};
+  const TuneShape cand[6] = {{FBP_BACKPROJECTOR_SYMMETRIC, 16, 0}, {FBP_BACKPROJECTOR_SYMMETRIC, 8, 0},
+                             {FBP_BACKPROJECTOR_GENERIC, 0, 0},    {FBP_BACKPROJECTOR_GENERIC, 0, 4},
+                             {FBP_BACKPROJECTOR_GENERIC_Y8, 0, 0}, {FBP_BACKPROJECTOR_GENERIC_Y8, 0, 4}};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   FBP_TRY(fbp::cuda_check(ctx, cudaEventCreate(&e0), "event"));
   FBP_TRY(fbp::cuda_check(ctx, cudaEventCreate(&e1), "event"));
-  const int saved_variant = ctx->bp_variant;
+  const TuneShape saved{ctx->bp_variant, ctx->quad_tile_ny, ctx->bp_stages};
   float best = 1e30f;
   int rc = FBP_OK;
-  *variant = FBP_BACKPROJECTOR_GENERIC;
-  for (const int c : cand) {
-    ctx->bp_variant = c;
+  *best_shape = TuneShape{FBP_BACKPROJECTOR_GENERIC, 0, 0};
+  for (const TuneShape& c : cand) {
+    apply_shape(ctx, c);
     int r = fbp::launch_backproject(ctx, gt, s, ctx->vol + (size_t)y0 * g.nx, 0, mixed);  // plan, pack: untimed
     if (r == FBP_ERR_UNSUPPORTED) continue;  // geometry not symmetric, windows too large, ...
     if (r) {
@@ -388,17 +452,20 @@ int autotune_backprojector(fbp_context* ctx, Stack& s, const fbp::BPGeom& g, boo
     cudaEventElapsedTime(&ms, e0, e1);
     if (ms < best) {
       best = ms;
-      *variant = c;
+      *best_shape = c;
     }
   }
-  ctx->bp_variant = saved_variant;
+  apply_shape(ctx, saved);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
+  ++ctx->tune_timed;
   fbp_context::TuneEntry t;
-  std::copy(key, key + 21, t.key);
-  t.variant = *variant;
+  std::copy(key, key + fbp_context::kTuneKey, t.key);
+  t.shape = *best_shape;
+  t.ms = best;
   ctx->tuned.push_back(t);
+  if (!ctx->tune_cache.empty()) store_tune_cache(ctx, t);
   return FBP_OK;
 }
 
@@ -439,12 +506,13 @@ int backproject(fbp_context* ctx, Stack& s, fbp::BPGeom g) {
   bool mixed = false;
   FBP_TRY(setup_backproject(ctx, s, g, &ylim, &mixed));
   if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && g.ny > 1) {
-    int variant = FBP_BACKPROJECTOR_AUTO;
-    int rc = autotune_backprojector(ctx, s, g, mixed, &variant);
+    TuneShape shape;
+    int rc = autotune_backprojector(ctx, s, g, mixed, &shape);
     if (rc == FBP_OK) {
-      ctx->bp_variant = variant;
+      const TuneShape saved{ctx->bp_variant, ctx->quad_tile_ny, ctx->bp_stages};
+      apply_shape(ctx, shape);
       rc = fbp::launch_backproject(ctx, g, s, ctx->vol, ylim, mixed);
-      ctx->bp_variant = FBP_BACKPROJECTOR_AUTO;
+      apply_shape(ctx, saved);
     }
     s.pack_ready = false;
     // the outer slices can have wider windows than the tuning slab: the
@@ -600,6 +668,7 @@ int fbp_create(fbp_context** out, int device) {
   fbp_context* ctx = new fbp_context();
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
+  ctx->device_cc = prop.major * 10 + prop.minor;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
       cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess ||
@@ -729,6 +798,28 @@ int fbp_last_backprojection(const fbp_context* ctx, int* variant, int* layout, i
 int fbp_set_autotune(fbp_context* ctx, int enable) {
   FBP_CTX(ctx);
   ctx->autotune = enable ? 1 : 0;
+  return FBP_OK;
+}
+
+int fbp_set_autotune_cache(fbp_context* ctx, const char* path) {
+  FBP_CTX(ctx);
+  ctx->tune_cache = path ? path : "";
+  ctx->tune_cache_loaded = false;
+  return FBP_OK;
+}
+
+int fbp_autotune_stats(const fbp_context* ctx, int* timed, int* from_cache) {
+  if (!ctx) return FBP_ERR_INVALID_ARGUMENT;
+  if (timed) *timed = ctx->tune_timed;
+  if (from_cache) *from_cache = ctx->tune_cached;
+  return FBP_OK;
+}
+
+int fbp_set_view_ring(fbp_context* ctx, int stages) {
+  FBP_CTX(ctx);
+  if (stages != 0 && (stages < 2 || stages > 8))
+    return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "view ring stages must be 0 or 2..8");
+  ctx->bp_stages = stages;
   return FBP_OK;
 }
 
@@ -1381,11 +1472,11 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
   const bool mixed = ctx->precision != FBP_PRECISION_FP32;
   std::vector<cudaEvent_t> done(slabs, nullptr);
   int rc = FBP_OK;
-  const int saved_variant = ctx->bp_variant;
+  const TuneShape saved{ctx->bp_variant, ctx->quad_tile_ny, ctx->bp_stages};
   if (ctx->autotune && ctx->bp_variant == FBP_BACKPROJECTOR_AUTO && v > 1) {
-    int variant = FBP_BACKPROJECTOR_AUTO;
-    rc = autotune_backprojector(ctx, s, gg, mixed, &variant);
-    ctx->bp_variant = variant;
+    TuneShape shape;
+    rc = autotune_backprojector(ctx, s, gg, mixed, &shape);
+    if (rc == FBP_OK) apply_shape(ctx, shape);
   }
   // y-slab k is backprojected straight into the whole volume, then copied to
   // the host on the copy stream while slab k + 1 computes
@@ -1398,9 +1489,9 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
     gs.vol_ystride = v;
     const int ylim = ctx->clip_after_bp ? std::max(0, std::min(gs.ny, gs.nz - y0)) : 0;
     rc = fbp::launch_backproject(ctx, gs, s, ctx->vol + (size_t)y0 * h, ylim, mixed);
-    if (rc == FBP_ERR_UNSUPPORTED && ctx->bp_variant != saved_variant) {
+    if (rc == FBP_ERR_UNSUPPORTED && ctx->bp_variant != saved.variant) {
       // a tuned choice that an outer slab's windows do not allow
-      ctx->bp_variant = saved_variant;
+      apply_shape(ctx, saved);
       rc = fbp::launch_backproject(ctx, gs, s, ctx->vol + (size_t)y0 * h, ylim, mixed);
     }
     s.pack_ready = mixed && !s.filtered;  // the first slab packed the views: the others reuse them
@@ -1416,7 +1507,7 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
                          "slab readback");
   }
   s.pack_ready = false;
-  ctx->bp_variant = saved_variant;
+  apply_shape(ctx, saved);
   ctx->minmax_valid = false;
   cudaStreamSynchronize(ctx->copy_stream);
   for (cudaEvent_t e : done)

@@ -1572,7 +1572,8 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
     }
     a.box_bytes = (int)max_box;
     const size_t per_stage = a.box_bytes + sizeof(ViewCoef) + 2 * sizeof(uint64_t);
-    const int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
+    int stages = (int)std::min<size_t>(kMaxStages, (smem_cap - 64) / per_stage);
+    if (ctx->bp_stages > 0) stages = std::min(stages, ctx->bp_stages);
     if (stages < 2)
       return set_error(ctx, FBP_ERR_UNSUPPORTED, "staged detector window does not fit in shared memory");
     a.chunk = stages;

@@ -118,12 +118,24 @@ struct fbp_context {
   int det_row_off = 0, det_rows_total = 0;  // fbp_set_detector_rows (0 rows: the whole detector)
   int slab_y0 = 0, slab_ny = 0;             // fbp_set_volume_slab (0 slices: the whole volume)
   int last_bp[5] = {-1, -1, 0, 0, 0};  // variant, layout, box_u, box_v, tile height of the last backprojection
-  int autotune = 0;                    // time the backprojector variants per geometry on first use
+  int bp_stages = 0;                    // generic backprojector: view ring stages (0: as many as fit, up to 8)
+  int autotune = 0;                    // time the backprojector shapes per geometry on first use
+  int device_cc = 0;                   // compute capability (major * 10 + minor), part of the tuning key
+  static constexpr int kTuneKey = 23;  // geometry, form, layout, slab, GPU
+  struct TuneShape {
+    int variant = FBP_BACKPROJECTOR_AUTO;
+    int quad_ny = 0;  // symmetric: voxels per thread along y
+    int stages = 0;   // generic: view ring stages
+  };
   struct TuneEntry {
-    double key[21];
-    int variant;
+    double key[kTuneKey];
+    TuneShape shape;
+    float ms = 0.f;
   };
   std::vector<TuneEntry> tuned;        // autotuner choices per geometry
+  std::string tune_cache;              // file of tuning choices shared between processes ("" = none)
+  bool tune_cache_loaded = false;
+  int tune_timed = 0, tune_cached = 0; // geometries timed / taken from the choices known
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched by this context
 

@@ -115,6 +115,9 @@ SIGNATURES = {
                                 C.POINTER(C.c_int)],
     "fbp_set_autotune": [_P, _I],
     "fbp_set_symmetric_tile": [_P, _I],
+    "fbp_set_autotune_cache": [_P, C.c_char_p],
+    "fbp_autotune_stats": [_P, C.POINTER(_I), C.POINTER(_I)],
+    "fbp_set_view_ring": [_P, _I],
     "fbp_project_backward_cone_fdk_batch": [C.POINTER(C.c_void_p), C.POINTER(Geometry), C.POINTER(_I),
                                             C.POINTER(_I), _I, _P],
     "fbp_generate_blank_volume": [_P, _I, _I, _I],
@@ -405,6 +408,20 @@ class FBP3D:
     def set_symmetric_tile(self, voxels_per_thread_y: int) -> None:
         """Voxels per thread along y of the symmetric backprojector (8, 16; 0 = 16)."""
         self.ctx.call("fbp_set_symmetric_tile", int(voxels_per_thread_y))
+
+    def set_autotune_cache(self, path) -> None:
+        """File of tuning choices shared between processes (None: none)."""
+        self.ctx.call("fbp_set_autotune_cache", None if path is None else str(path).encode())
+
+    def autotune_stats(self) -> tuple[int, int]:
+        """(geometries timed, geometries taken from known choices)."""
+        a, b = C.c_int(), C.c_int()
+        self.ctx.call("fbp_autotune_stats", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def set_view_ring(self, stages: int) -> None:
+        """View ring stages of the generic backprojector (2..8; 0 = as many as fit)."""
+        self.ctx.call("fbp_set_view_ring", int(stages))
 
     def set_autotune(self, enable: bool) -> None:
         """Time the backprojector variants on the first backprojection of each geometry and keep the fastest."""

@@ -66,6 +66,10 @@ def parse_args():
                    help="cone1440: the headline 1440x1470x1440 case; cone256: 256^3, 360 views (profiling); "
                         "serving: the mixed request stream (reconstructions/s, p50/p99 latency)")
     p.add_argument("--requests", type=int, default=2000, help="serving: requests in the stream")
+    p.add_argument("--poisson-requests", type=int, default=600,
+                   help="serving: requests of the stream timed under Poisson arrivals")
+    p.add_argument("--no-serving", action="store_true",
+                   help="cone workloads: leave the serving block (config 5) out of the line")
     p.add_argument("--slots", type=int, default=5, help="serving: concurrent jobs of the chosen form")
     p.add_argument("--load", type=float, default=0.7,
                    help="serving: Poisson arrival rate as a fraction of the plain one-at-a-time capacity")
@@ -365,14 +369,20 @@ def serving_requests(n: int, seed: int = 1004) -> list[dict]:
     return out
 
 
-def serving_main(args) -> None:
-    """Serving on one GPU: the stream's capacity (reconstructions/s, every
-    request submitted at once) for the plain form run one job at a time (FP32,
-    one slot) and for the chosen form under continuous batching (MIXED,
-    `--slots` slots), then p50/p99 latency of both under seeded Poisson
-    arrivals at `--load` x the plain capacity. Inputs: seeded random
-    ellipsoids projected analytically on the GPU (fan jobs: the central
-    detector row), held in pinned host memory as the requests arrive."""
+def serving_block(args, n_requests: int, n_poisson: int) -> dict:
+    """Serving on one GPU: the chosen form under continuous
+    batching (MIXED, `--slots` worker slots, cone backprojections through the
+    persistent multi-job backprojector) against the plain FP32 form run one
+    job at a time. Capacity = reconstructions/s with the whole stream
+    submitted at once; latency = p50 / p99 of finish - arrival under seeded
+    Poisson arrivals at `--load` x the plain capacity (the first `n_poisson`
+    requests). The plain form runs one job at a time, so its stream time is
+    the sum of its jobs' service times: every distinct job shape is timed
+    alone through the server (one slot, upload + reconstruction + readback,
+    median of 3) and the plain capacity and FIFO latencies follow from those
+    times; an actual plain run of the first 200 requests checks the sum.
+    Inputs: seeded random ellipsoids projected analytically on the GPU (fan
+    jobs: the central detector row), held in pinned host memory."""
     import numpy as np
     import torch
 
@@ -382,7 +392,7 @@ def serving_main(args) -> None:
     import phantoms as P
 
     torch.cuda.set_device(0)
-    reqs = serving_requests(args.requests)
+    reqs = serving_requests(n_requests)
 
     def shape_key(r):
         return (r["kind"], r["n"], r["views"], r.get("det", r.get("bins")))
@@ -428,18 +438,23 @@ def serving_main(args) -> None:
         q.input, q.output = inp.data_ptr(), out.data_ptr()
         return q
 
-    def run(precision, slots, arrivals=None):
+    def server(precision, slots):
         srv = F.Server(0, 0, slots)
+        srv.set_batching(precision != F.Precision.FP32)
         # warm every slot's buffers with the largest jobs (buffers only grow)
         big = max(reqs, key=lambda r: r["n"] ** 3 * r["views"] if r["kind"] == "cone" else 0)
         big2 = max(reqs, key=lambda r: r["n"] ** 2 * r["views"] if r["kind"] == "fan" else 0)
         warm = [srv.submit(request_struct(w, precision, outs[shape_key(w)][0])) for w in [big] * slots + [big2] * slots]
         for t in warm:
             assert srv.wait(t).status == 0
+        return srv
+
+    def run(precision, slots, stream, arrivals=None):
+        srv = server(precision, slots)
         rr = {k: 0 for k in outs}
         tickets = []
         t0 = time.perf_counter()
-        for i, r in enumerate(reqs):
+        for i, r in enumerate(stream):
             if arrivals is not None:
                 delay = arrivals[i] - (time.perf_counter() - t0)
                 if delay > 0:
@@ -454,30 +469,62 @@ def serving_main(args) -> None:
         assert not bad, bad[:3]
         lat = np.array([x.finished_ms - x.queued_ms for x in res])
         span = (max(x.finished_ms for x in res) - min(x.queued_ms for x in res)) * 1e-3
-        return dict(recon_per_s=len(res) / span, p50_ms=float(np.percentile(lat, 50)),
+        return dict(requests=len(res), recon_per_s=len(res) / span, p50_ms=float(np.percentile(lat, 50)),
                     p99_ms=float(np.percentile(lat, 99)), makespan_s=span)
 
-    plain_cap = run(F.Precision.FP32, 1)
-    chosen_cap = run(F.Precision.MIXED, args.slots)
+    # ---- plain one at a time: per-shape service times
+    srv = server(F.Precision.FP32, 1)
+    service = {}
+    for key in sorted({shape_key(r) for r in reqs}):
+        r = next(x for x in reqs if shape_key(x) == key)
+        ts = []
+        for _ in range(3):
+            res = srv.wait(srv.submit(request_struct(r, F.Precision.FP32, outs[key][0])))
+            assert res.status == 0, res.error
+            ts.append((res.finished_ms - res.started_ms) * 1e-3)
+        service[key] = float(np.median(ts))
+    srv.close()
+    t_plain = np.array([service[shape_key(r)] for r in reqs])
+    plain_cap = {"requests": len(reqs), "recon_per_s": len(reqs) / t_plain.sum(), "makespan_s": float(t_plain.sum()),
+                 "from": "sum of per-shape service times measured alone"}
+    check = run(F.Precision.FP32, 1, reqs[:200])
+    plain_cap["measured_first_200"] = {"recon_per_s": check["recon_per_s"],
+                                       "from_service_times": 200 / t_plain[:200].sum()}
     rate = args.load * plain_cap["recon_per_s"]
-    arrivals = np.cumsum(np.random.default_rng(1005).exponential(1.0 / rate, size=len(reqs)))
-    plain_lat = run(F.Precision.FP32, 1, arrivals)
-    chosen_lat = run(F.Precision.MIXED, args.slots, arrivals)
+    npo = min(n_poisson, len(reqs))
+    arrivals = np.cumsum(np.random.default_rng(1005).exponential(1.0 / rate, size=npo))
+    # plain under Poisson arrivals: one FIFO server with those service times
+    fin, lat = 0.0, []
+    for a, t in zip(arrivals, t_plain[:npo]):
+        fin = max(a, fin) + t
+        lat.append((fin - a) * 1e3)
+    plain_lat = {"requests": npo, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                 "from": "FIFO of the measured service times"}
+    chosen_cap = run(F.Precision.MIXED, args.slots, reqs)
+    chosen_lat = run(F.Precision.MIXED, args.slots, reqs[:npo], arrivals)
     mix = {"fan2d": sum(r["kind"] == "fan" for r in reqs), "cone_128_512": sum(r["kind"] == "cone" and r["n"] < 768
                                                                                for r in reqs),
            "cone_768": sum(r["kind"] == "cone" and r["n"] == 768 for r in reqs)}
-    line = {
+    return {
         "metric": "mixed-stream reconstructions/s", "value": chosen_cap["recon_per_s"], "unit": "recon/s",
-        "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 accumulation, f16 filtered views (chosen)", "data": "synthetic: seeded random ellipsoids, "
-        "analytic projections (GPU), pinned host inputs",
         "config": {"workload": "serving_mixed_stream", "requests": len(reqs), "mix": mix, "slots": args.slots,
-                   "arrival_rate_per_s": rate, "load_vs_plain_capacity": args.load},
+                   "poisson_requests": npo, "arrival_rate_per_s": rate, "load_vs_plain_capacity": args.load,
+                   "batching": "cone backprojections through the persistent multi-job backprojector"},
         "chosen": {"capacity": chosen_cap, "poisson": chosen_lat},
         "plain_one_at_a_time_fp32": {"capacity": plain_cap, "poisson": plain_lat},
         "chosen_over_plain_recon_per_s": chosen_cap["recon_per_s"] / plain_cap["recon_per_s"],
-        "p99_ms": chosen_lat["p99_ms"], "p50_ms": chosen_lat["p50_ms"],
+        "p50_ms": chosen_lat["p50_ms"], "p99_ms": chosen_lat["p99_ms"],
     }
+
+
+def serving_main(args) -> None:
+    """--workload serving: the serving block alone, as its own JSON line."""
+    blk = serving_block(args, args.requests, args.poisson_requests)
+    line = {"metric": blk["metric"], "value": blk["value"], "unit": blk["unit"], "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 accumulate / f16 filtered views (chosen)",
+            "data": "synthetic: seeded random ellipsoids, analytic projections (GPU), pinned host inputs"}
+    line.update({k: v for k, v in blk.items() if k not in line})
     print(json.dumps(line), flush=True)
 
 
@@ -814,6 +861,10 @@ def main() -> None:
                        f"({'compiled from its sources' if r['use_ref'] else 'oracle restatement'}), "
                        f"{r['sample_updates']:.3g} updates of the FP32 CPU backprojector restatement, "
                        f"extrapolated to the full job ({r['full_seconds']:.0f} s)")}
+    if rank == 0 and world == 1 and args.workload == "cone1440" and args.scale == 1 and not args.no_serving:
+        del pristine
+        torch.cuda.empty_cache()
+        line["serving"] = serving_block(args, args.requests, args.poisson_requests)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -127,6 +127,19 @@ int fbp_set_backprojector(fbp_context* ctx, int variant);
  * symmetric kernel when the geometry allows it. No counterpart in the
  * reference, whose backprojection is one fixed shader. */
 int fbp_set_autotune(fbp_context* ctx, int enable);
+/* With autotuning on: the shapes the tuner times are the symmetric kernel
+ * with 16 or 8 voxels per thread along y and the generic kernel with 16 or 8
+ * voxels per thread, each with its full view ring or a 4-stage one. A cache
+ * file (path; NULL or "" = none) keeps the choices across processes: they are
+ * read from it on the first tuning and each new choice is appended as one
+ * line (key of geometry, form, layout, slab and GPU; shape; time), so another
+ * process with the same geometry takes the cached shape without timing. */
+int fbp_set_autotune_cache(fbp_context* ctx, const char* path);
+/* Geometries the tuner timed, and geometries whose shape came from the
+ * choices already known (this context's or the cache file's). */
+int fbp_autotune_stats(const fbp_context* ctx, int* timed, int* from_cache);
+/* View ring stages of the generic backprojector (2..8; 0 = as many as fit). */
+int fbp_set_view_ring(fbp_context* ctx, int stages);
 /* Voxels per thread along y of the four-fold symmetric backprojector: 16
  * (one CTA per SM, 64 accumulators a thread) or 8 (two CTAs per SM); 0 (the
  * default) = 16. No counterpart in the reference. */

@@ -625,6 +625,79 @@ def test_autotuned_backprojector(fbp, oracle, precision):
         assert relative_rmse(got, ref) < tol
 
 
+TUNER_SHAPES = [("SYMMETRIC", 16, 0), ("SYMMETRIC", 8, 0), ("GENERIC", 0, 0), ("GENERIC", 0, 4),
+                ("GENERIC_Y8", 0, 0), ("GENERIC_Y8", 0, 4)]
+
+
+@pytest.mark.parametrize("precision", ["FP32", "MIXED"])
+@pytest.mark.parametrize("shape", TUNER_SHAPES, ids=lambda t: f"{t[0]}-{t[1]}-{t[2]}")
+def test_every_tuner_shape_matches_the_oracle(fbp, oracle, shape, precision):
+    """Each shape the autotuner may pick (kernel, voxels per thread along y,
+    view ring stages), set explicitly, against the oracle."""
+    variant, ny, stages = shape
+    c, proj = _sym_case(oracle, nviews=192)
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(getattr(fbp.Precision, precision))
+    s.set_backprojector(getattr(fbp.Backprojector, variant))
+    if ny:
+        s.set_symmetric_tile(ny)
+    s.set_view_ring(stages)
+    got = _gpu_fdk(s, c, proj, 0)
+    info = s.last_backprojection()
+    assert info["kernel"] == variant.lower() and (not ny or info["tile_ny"] == ny)
+    err = relative_rmse(got, oracle.fdk(proj, c, 0))
+    print(f"shape {shape} {precision}: {info} rel RMSE {err:.2e}")
+    assert err < (TOL_FP32 if precision == "FP32" else TOL_MIXED)
+
+
+_TUNE_SCRIPT = """
+import json, sys
+sys.path[:0] = [{pkg!r}, {oracle_dir!r}]
+import numpy as np
+import fbp_b200 as F
+proj = np.load({proj!r})
+s = F.FBP3D(0)
+s.set_clip_after_backprojection(False)
+s.set_autotune(True)
+s.set_autotune_cache({cache!r})
+s.upload_projections(proj)
+s.apply_fdk_weights_to_projections(*{wargs!r})
+s.apply_filter_to_projections(0)
+s.project_backward_cone_fdk_from_projections(*{bargs!r})
+vol = s.read_volume()
+print(json.dumps(dict(stats=s.autotune_stats(), info=s.last_backprojection(), sum=float(vol.astype(np.float64).sum()),
+                      crc=int(np.frombuffer(vol.tobytes(), np.uint32).astype(np.uint64).sum()))))
+"""
+
+
+def test_autotune_cache_is_shared_between_processes(fbp, oracle, tmp_path):
+    """A first process times the shapes and appends its choice to the cache
+    file; a second process with the same geometry takes that shape from the
+    file without timing anything and computes the same volume."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    c, proj = _sym_case(oracle, nviews=96)
+    np.save(tmp_path / "proj.npy", proj)
+    sod, odd, w, vw, rot = _cone_args(c)
+    script = _TUNE_SCRIPT.format(pkg=str(root / "3dfilteredbackprojection-public_b200"), oracle_dir=str(root / "oracle"),
+                                 proj=str(tmp_path / "proj.npy"), cache=str(tmp_path / "tune.txt"),
+                                 wargs=(sod, odd, w), bargs=(sod, odd, w, vw, rot, c["nx"], c["ny"], c["offset"]))
+    runs = []
+    for _ in range(2):
+        r = subprocess.run([sys.executable, "-c", script], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    assert runs[0]["stats"] == [1, 0] and runs[1]["stats"] == [0, 1]
+    assert runs[0]["info"] == runs[1]["info"]
+    assert runs[0]["crc"] == runs[1]["crc"]
+    assert len((tmp_path / "tune.txt").read_text().splitlines()) == 1
+
+
 @pytest.mark.parametrize("factor", [2, 1])
 def test_symmetric_backprojector_mixed(fbp, oracle, phantoms, factor):
     """MIXED form through the four-fold symmetric backprojector on the 256^3
