@@ -113,6 +113,118 @@ struct FilterKArgs {
   const float* hbr;
 };
 
+// Butterfly passes over the P rows of `buf` (n = 2^L complex samples each).
+// Two radix-2 stages are done per pass on four elements in registers (the
+// same operations in the same order as two separate radix-2 stages, with half
+// the shared-memory round trips and barriers).
+struct FftRows {
+  float2* buf;
+  const float2* tw;  // tw[k] = exp(-2 pi i k / n), k < n / 2
+  int n, L, P;
+};
+
+// forward DIF radix-2 stage lh (half-size h = 2^lh)
+__device__ __forceinline__ void fwd_r2(const FftRows& f, int lh) {
+  const int h = 1 << lh, half = f.n >> 1, tsh = f.L - 1 - lh;
+  for (int b = threadIdx.x; b < f.P * half; b += blockDim.x) {
+    const int p = b >> (f.L - 1), q = b & (half - 1);
+    const int j = q & (h - 1), blk = q >> lh;
+    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
+    const float2 x0 = d[0], x1 = d[h];
+    d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
+    d[h] = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), f.tw[j << tsh]);
+  }
+}
+
+// forward DIF stages lh and lh - 1 (lh >= 1) on blocks of 2^(lh + 1)
+__device__ __forceinline__ void fwd_r4(const FftRows& f, int lh) {
+  const int h = 1 << lh, h2 = h >> 1, quarter = f.n >> 2, tsh = f.L - 1 - lh;
+  for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
+    const int p = b / quarter, q = b - p * quarter;
+    const int j = q & (h2 - 1), blk = q >> (lh - 1);
+    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
+    const float2 e0 = d[0], e1 = d[h2], e2 = d[h], e3 = d[h + h2];
+    const float2 t0 = make_float2(e0.x + e2.x, e0.y + e2.y);
+    const float2 t2 = cmul(make_float2(e0.x - e2.x, e0.y - e2.y), f.tw[j << tsh]);
+    const float2 t1 = make_float2(e1.x + e3.x, e1.y + e3.y);
+    const float2 t3 = cmul(make_float2(e1.x - e3.x, e1.y - e3.y), f.tw[(j + h2) << tsh]);
+    const float2 w = f.tw[j << (tsh + 1)];
+    d[0] = make_float2(t0.x + t1.x, t0.y + t1.y);
+    d[h2] = cmul(make_float2(t0.x - t1.x, t0.y - t1.y), w);
+    d[h] = make_float2(t2.x + t3.x, t2.y + t3.y);
+    d[h + h2] = cmul(make_float2(t2.x - t3.x, t2.y - t3.y), w);
+  }
+}
+
+// inverse DIT radix-2 stage lh
+__device__ __forceinline__ void inv_r2(const FftRows& f, int lh) {
+  const int h = 1 << lh, half = f.n >> 1, tsh = f.L - 1 - lh;
+  for (int b = threadIdx.x; b < f.P * half; b += blockDim.x) {
+    const int p = b >> (f.L - 1), q = b & (half - 1);
+    const int j = q & (h - 1), blk = q >> lh;
+    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
+    const float2 x0 = d[0];
+    const float2 x1 = cmulc(d[h], f.tw[j << tsh]);
+    d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
+    d[h] = make_float2(x0.x - x1.x, x0.y - x1.y);
+  }
+}
+
+// inverse DIT stages lh and lh + 1 on blocks of 2^(lh + 2)
+__device__ __forceinline__ void inv_r4(const FftRows& f, int lh) {
+  const int h = 1 << lh, quarter = f.n >> 2, tsh = f.L - 1 - lh;
+  for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
+    const int p = b / quarter, q = b - p * quarter;
+    const int j = q & (h - 1), blk = q >> lh;
+    float2* d = f.buf + p * f.n + (blk << (lh + 2)) + j;
+    const float2 e0 = d[0], e1 = d[h], e2 = d[2 * h], e3 = d[3 * h];
+    const float2 w = f.tw[j << tsh];
+    const float2 x1 = cmulc(e1, w), x3 = cmulc(e3, w);
+    const float2 a0 = make_float2(e0.x + x1.x, e0.y + x1.y), a1 = make_float2(e0.x - x1.x, e0.y - x1.y);
+    const float2 a2 = make_float2(e2.x + x3.x, e2.y + x3.y), a3 = make_float2(e2.x - x3.x, e2.y - x3.y);
+    const float2 y = cmulc(a2, f.tw[j << (tsh - 1)]), z = cmulc(a3, f.tw[(j + h) << (tsh - 1)]);
+    d[0] = make_float2(a0.x + y.x, a0.y + y.y);
+    d[2 * h] = make_float2(a0.x - y.x, a0.y - y.y);
+    d[h] = make_float2(a1.x + z.x, a1.y + z.y);
+    d[3 * h] = make_float2(a1.x - z.x, a1.y - z.y);
+  }
+}
+
+// The last two forward stages (1, 0), the response H (bit-reversed, / n) and
+// the first two inverse stages (0, 1) of each block of four, in registers.
+__device__ __forceinline__ void middle_r4(const FftRows& f, const float* hb) {
+  const int quarter = f.n >> 2;
+  const float2 w1 = f.tw[1 << (f.L - 2)], w0 = f.tw[0];
+  for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
+    const int p = b / quarter, q = b - p * quarter;
+    float2* d = f.buf + p * f.n + 4 * q;
+    const float* hq = hb + 4 * q;
+    const float2 e0 = d[0], e1 = d[1], e2 = d[2], e3 = d[3];
+    // forward stage 1 (pairs 0-2 with w0, 1-3 with w1), stage 0 (pairs 0-1, 2-3 with w0)
+    const float2 t0 = make_float2(e0.x + e2.x, e0.y + e2.y);
+    const float2 t2 = cmul(make_float2(e0.x - e2.x, e0.y - e2.y), w0);
+    const float2 t1 = make_float2(e1.x + e3.x, e1.y + e3.y);
+    const float2 t3 = cmul(make_float2(e1.x - e3.x, e1.y - e3.y), w1);
+    float2 s0 = make_float2(t0.x + t1.x, t0.y + t1.y);
+    float2 s1 = cmul(make_float2(t0.x - t1.x, t0.y - t1.y), w0);
+    float2 s2 = make_float2(t2.x + t3.x, t2.y + t3.y);
+    float2 s3 = cmul(make_float2(t2.x - t3.x, t2.y - t3.y), w0);
+    s0 = make_float2(s0.x * hq[0], s0.y * hq[0]);
+    s1 = make_float2(s1.x * hq[1], s1.y * hq[1]);
+    s2 = make_float2(s2.x * hq[2], s2.y * hq[2]);
+    s3 = make_float2(s3.x * hq[3], s3.y * hq[3]);
+    // inverse stage 0 (pairs 0-1, 2-3 with w0), stage 1 (pairs 0-2 with w0, 1-3 with w1)
+    const float2 x1 = cmulc(s1, w0), x3 = cmulc(s3, w0);
+    const float2 a0 = make_float2(s0.x + x1.x, s0.y + x1.y), a1 = make_float2(s0.x - x1.x, s0.y - x1.y);
+    const float2 a2 = make_float2(s2.x + x3.x, s2.y + x3.y), a3 = make_float2(s2.x - x3.x, s2.y - x3.y);
+    const float2 y = cmulc(a2, w0), z = cmulc(a3, w1);
+    d[0] = make_float2(a0.x + y.x, a0.y + y.y);
+    d[2] = make_float2(a0.x - y.x, a0.y - y.y);
+    d[1] = make_float2(a1.x + z.x, a1.y + z.y);
+    d[3] = make_float2(a1.x - z.x, a1.y - z.y);
+  }
+}
+
 // One CTA filters `pairs_per_cta` row pairs per iteration, grid-stride.
 __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -124,6 +236,7 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) hb[i] = a.hbr[i];
   const RowSet& rs = a.rs;
   const int P = a.pairs_per_cta;
+  const FftRows f{buf, tw, n, a.log2n, P};
   const long long ngroups = (a.npairs + P - 1) / P;
   for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     __syncthreads();
@@ -140,39 +253,37 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
       buf[idx] = make_float2(re, im);
     }
     __syncthreads();
-    // forward DIF
-    for (int lh = a.log2n - 1; lh >= 0; --lh) {
-      const int h = 1 << lh;
-      const int tsh = a.log2n - 1 - lh;  // twiddle stride n/(2h) = 2^tsh
-      for (int b = threadIdx.x; b < P * half; b += blockDim.x) {
-        int p = b >> (a.log2n - 1), q = b & (half - 1);
-        int j = q & (h - 1), blk = q >> lh;
-        float2* d = buf + p * n + (blk << (lh + 1)) + j;
-        float2 x0 = d[0], x1 = d[h];
-        d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
-        d[h] = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), tw[j << tsh]);
-      }
+    // forward DIF (natural order in, bit-reversed out): an odd stage first,
+    // then pairs of stages down to stage 2
+    int lh = f.L - 1;
+    if (f.L & 1) {
+      fwd_r2(f, lh--);
       __syncthreads();
     }
-    for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
-      float hv = hb[idx & (n - 1)];
-      float2 x = buf[idx];
-      buf[idx] = make_float2(x.x * hv, x.y * hv);
+    for (; lh >= 3; lh -= 2) {
+      fwd_r4(f, lh);
+      __syncthreads();
+    }
+    int next;  // first inverse stage still to do
+    if (lh == 1) {
+      middle_r4(f, hb);
+      next = 2;
+    } else {  // n <= 2: the response on its own
+      for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
+        const float hv = hb[idx & (n - 1)];
+        const float2 x = buf[idx];
+        buf[idx] = make_float2(x.x * hv, x.y * hv);
+      }
+      next = 0;
     }
     __syncthreads();
-    // inverse DIT
-    for (int lh = 0; lh < a.log2n; ++lh) {
-      const int h = 1 << lh;
-      const int tsh = a.log2n - 1 - lh;
-      for (int b = threadIdx.x; b < P * half; b += blockDim.x) {
-        int p = b >> (a.log2n - 1), q = b & (half - 1);
-        int j = q & (h - 1), blk = q >> lh;
-        float2* d = buf + p * n + (blk << (lh + 1)) + j;
-        float2 x0 = d[0];
-        float2 x1 = cmulc(d[h], tw[j << tsh]);
-        d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
-        d[h] = make_float2(x0.x - x1.x, x0.y - x1.y);
-      }
+    // inverse DIT (bit-reversed in, natural order out): pairs of stages, then an odd last one
+    for (; next + 1 < f.L; next += 2) {
+      inv_r4(f, next);
+      __syncthreads();
+    }
+    if (next < f.L) {
+      inv_r2(f, next);
       __syncthreads();
     }
     // store
