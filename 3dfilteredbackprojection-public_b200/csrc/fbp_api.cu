@@ -630,7 +630,7 @@ int prepare_packed(fbp_context* ctx, Stack& s, int layout) {
   // the four-term difference of the gradient layout is at most 4 max|value|;
   // the 24-bit layout keeps the FP32 exponent and needs no scale
   if (layout != kLayoutQuadG24)
-    if (int rc = launch_view_scales(ctx, rowset_of(s), quad ? 8192.f : 32768.f, scale, s.inv_scale)) return rc;
+    if (int rc = launch_view_scales(ctx, rowset_of(s), quad ? 8192.f : 16384.f, scale, s.inv_scale)) return rc;
   if (int rc = launch_pack(ctx, s, layout, s.filt, fpitch, scale)) return rc;
   s.filt_layout = layout;
   s.filt_pitch = fpitch;

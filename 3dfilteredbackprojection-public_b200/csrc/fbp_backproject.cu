@@ -349,7 +349,7 @@ constexpr uint32_t kMagicBits = 0x4B400000u;
 // window base, the column and -kMagicBits * RB); no conversion instructions.
 // wa, wb already carry W for the FP32 layouts.
 template <int LAYOUT>
-__device__ __forceinline__ void tap(float v, uint32_t c0, uint32_t RB, float wa, float wb, __half2 fu2, float W,
+__device__ __forceinline__ void tap(float v, uint32_t c0, uint32_t RB, float wa, float wb, float fu, float W,
                                     float& accum) {
   const float t = __fadd_rz(v, kMagic);
   const float fv = v - (t - kMagic);  // in [0, 1)
@@ -366,9 +366,10 @@ __device__ __forceinline__ void tap(float v, uint32_t c0, uint32_t RB, float wa,
     const float r1 = fmaf(wb, Y.y, wa * X.y);
     accum += fmaf(fv, r1 - r0, r0);
   } else {
-    const __half2 X = lds_h2(addr), Y = lds_h2(addr + 4);
-    const float2 R = __half22float2(__hfma2(fu2, __hsub2(Y, X), X));  // (row v, row v + 1) lerped in u
-    accum = fmaf(W, fmaf(fv, R.y - R.x, R.x), accum);
+    // element = (row v, row v + 1 minus row v); the u-lerp of both in FP32
+    const float2 x = __half22float2(lds_h2(addr)), y = __half22float2(lds_h2(addr + 4));
+    const float2 ag = ffma2(make_float2(fu, fu), fsub2(y, x), x);
+    accum = fmaf(W, fmaf(fv, ag.y, ag.x), accum);
   }
 }
 
@@ -507,10 +508,9 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
       const float vmax_ok = (float)(BV - kRowTail) - (float)(kSlack / 2);
       if (iu >= 0 && iu <= BU - 2 && vl >= 0.f && vlast < vmax_ok) {
         const float wa = W - W * fu, wb = W * fu;
-        const __half2 fu2 = __float2half2_rn(fu);
         const uint32_t c0 = smem_u32(smem + (size_t)s * a.box_bytes) + (uint32_t)(iu * ESZ) - kMagicBits * RB;
 #pragma unroll
-        for (int j = 0; j < NY; ++j) tap<LAYOUT>(fmaf((float)j, dvv, vl), c0, RB, wa, wb, fu2, W, KAHAN ? part[j] : acc[j]);
+        for (int j = 0; j < NY; ++j) tap<LAYOUT>(fmaf((float)j, dvv, vl), c0, RB, wa, wb, fu, W, KAHAN ? part[j] : acc[j]);
       } else {
         bad = true;  // cannot happen when the footprint pass is right; recorded below
       }
@@ -1093,7 +1093,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
             const float v = fmaf((float)j, dvv, vl);
 #pragma unroll
             for (int r = 0; r < 4; ++r)
-              tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu2, Wr[r],
+              tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu, Wr[r],
                           KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j]);
           }
         }

@@ -105,6 +105,16 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
+// Shared memory of filter_fft_kernel: twiddles (n / 2 float2), the response
+// (n floats), then the rows' buffer (P x n float2) from a 16-byte boundary
+// (for n = 1 the first two parts end 4 bytes in).
+__host__ __device__ constexpr size_t fft_buf_offset(int n) {
+  return (sizeof(float2) * (n / 2) + sizeof(float) * n + 15) / 16 * 16;
+}
+__host__ __device__ constexpr size_t fft_smem_bytes(int n, int pairs) {
+  return fft_buf_offset(n) + sizeof(float2) * n * pairs;
+}
+
 struct FilterKArgs {
   RowSet rs;
   int n, log2n, pairs_per_cta;
@@ -231,7 +241,7 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
   const int n = a.n, half = n >> 1;
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float* hb = reinterpret_cast<float*>(tw + half);
-  float2* buf = reinterpret_cast<float2*>(hb + n);
+  float2* buf = reinterpret_cast<float2*>(smem_raw + fft_buf_offset(n));
   for (int i = threadIdx.x; i < half; i += blockDim.x) tw[i] = a.tw[i];
   for (int i = threadIdx.x; i < n; i += blockDim.x) hb[i] = a.hbr[i];
   const RowSet& rs = a.rs;
@@ -345,7 +355,7 @@ __global__ void view_scale_kernel(const unsigned* vmax, int nviews, float limit,
   inv[k] = 1.f / s;
 }
 
-// f32 rows -> pair16: element (view, e, c) = (row e - 1, row e) * scale.
+// f32 rows -> pair16: element (view, e, c) = (row e - 1, row e - row e - 1) * scale.
 __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                    const float* scale, __half2* out, long long opitch) {
   const long long total = (long long)n_views * (n_v + 1) * m;
@@ -359,7 +369,11 @@ __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, in
     const float lo = e >= 1 ? src[row(e - 1) * spitch + c] : 0.f;
     const float hi = e < n_v ? src[row(e) * spitch + c] : 0.f;
     const float sc = scale[view];
-    out[er * opitch + c] = __floats2half2_rn(lo * sc, hi * sc);
+    // (row e - 1, row e minus row e - 1 as read back): the second value's
+    // rounding does not add to the first's (error feedback, as the quads)
+    const __half hl = __float2half_rn(lo * sc);
+    const __half hd = __float2half_rn(fmaf(hi, sc, -__half2float(hl)));
+    out[er * opitch + c] = __halves2half2(hl, hd);
   }
 }
 
@@ -616,7 +630,7 @@ int launch_filter_fft(fbp_context* ctx, const RowSet& rs, int n) {
   a.npairs = (rs.rows + 1) / 2;
   a.tw = ctx->ftab.twiddle;
   a.hbr = ctx->ftab.hbr;
-  size_t smem = sizeof(float2) * (n / 2) + sizeof(float) * n + sizeof(float2) * n * a.pairs_per_cta;
+  size_t smem = fft_smem_bytes(n, a.pairs_per_cta);
   // per device and process-wide: set on every launch (same value from every context)
   cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   long long groups = (a.npairs + a.pairs_per_cta - 1) / a.pairs_per_cta;
@@ -811,7 +825,7 @@ extern "C" int fbp2d_filter_sinogram_noalloc(float* sinogram, int bins, int view
   a.npairs = (rs.rows + 1) / 2;
   a.tw = tw;
   a.hbr = hbr;
-  const size_t smem = sizeof(float2) * (n / 2) + sizeof(float) * n + sizeof(float2) * n * a.pairs_per_cta;
+  const size_t smem = fft_smem_bytes(n, a.pairs_per_cta);
   if ((e = cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024)) !=
       cudaSuccess)
     return cuda_check(nullptr, e, "fbp2d_filter_sinogram_noalloc: shared memory attribute");

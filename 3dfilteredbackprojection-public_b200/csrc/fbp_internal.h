@@ -98,7 +98,7 @@ struct FilterTables {
 // for i < m, k < kp (zero for k >= m), as BF16 hi rows then BF16 lo rows.
 struct ToeplitzTables {
   int m = 0, n = 0, filter = -1;
-  void* th = nullptr;  // 2 * m * kp BF16 values, then m FP32 column sums of T
+  void* th = nullptr;  // 2 * m * kp BF16 values, then 9 x m FP32 columns T P_j (row baseline basis)
   size_t cap = 0;      // bytes allocated at th (grow only)
 };
 

@@ -8,11 +8,16 @@
 // BF16 hi + lo parts (hi = bf16(x), lo = bf16(x - hi)), and
 // Y = Xh Th + Xh Tl + Xl Th is accumulated in FP32 in tensor memory (the
 // dropped Xl Tl term and the split residuals are ~2^-17 of |x|). Each row's
-// mean mu is taken out before the split and its filtered contribution
-// mu * s (s = column sums of T, FP64-summed) added in the epilogue: detector
-// rows sit on a large offset (line integrals of ~10 against a high-pass output
-// a hundred times smaller), and the split's error follows |x - mu| instead
-// of |x| (1.6e-4 -> 4.9e-5 relative on noisy 1536-wide rows).
+// smooth baseline b (a degree-8 Legendre fit of the row, 9 coefficients) is
+// taken out before the split and its filtered contribution T b = sum_j c_j
+// (T P_j) (the columns T P_j summed in FP64) added in the epilogue: detector
+// rows sit on large, slowly varying values (line integrals of ~10, plateaus
+// of opaque rays) against a high-pass output ten to a hundred times smaller,
+// and the split's error follows |x - b| instead of |x|. On the noisy 2D fan
+// case (768 bins, Poisson I0 = 1e5) the image error against the FP64 oracle
+// is 3.2e-4 with the row mean alone and 4.1e-5 with the degree-8 baseline
+// (numpy emulation of the same split); any baseline is exact in principle,
+// since the same coefficients are subtracted and added back.
 //
 // Kernel: one CTA per 128 x 256 output tile. Warp 0 streams 64-wide K blocks
 // of Xh, Xl, Th, Tl into a two-stage shared-memory ring with TMA (128-byte
@@ -30,6 +35,8 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cmath>
+#include <utility>
 
 namespace fbp {
 namespace {
@@ -41,6 +48,13 @@ constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
 constexpr int TMEM_COLS = 256;
 constexpr uint32_t kWait = 1u << 22;
 constexpr int kEpiStride = 33;  // floats per staged row (bank-conflict-free)
+constexpr int kBasis = 9;       // Legendre polynomials P_0 .. P_8 of the row baseline
+
+// Inverse Gram matrix of the baseline basis on the row's samples (FP64 on the
+// host, rounded to FP32): coefficients c = Ginv * (moments <x, P_j>).
+struct BasisGram {
+  float ginv[kBasis * kBasis];
+};
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -106,8 +120,8 @@ struct GemmArgs {
   int nrows;        // rows in this chunk
   int m;            // samples per row (N and K extent)
   int ntile_n;      // tiles along N
-  const float* mu;      // per chunk row: the mean taken out before the split
-  const float* colsum;  // per output column i: sum over k < m of T[k][i]
+  const float* coef;    // per chunk row: kBasis coefficients of the baseline taken out before the split
+  const float* tp;      // [j][i]: (T P_j)[i] = sum over k < m of P_j(k) T[k][i]
   int* err;
 };
 
@@ -224,11 +238,20 @@ __global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_cons
       asm volatile("bar.sync 1, 128;" ::: "memory");
       // warp w writes tile rows w, w + 4, ...; lane = column: row-contiguous stores
       const int col = col0 + c * 32 + lane;
+      float tpc[kBasis];
+#pragma unroll
+      for (int j = 0; j < kBasis; ++j) tpc[j] = col < g.m ? g.tp[(size_t)j * g.m + col] : 0.f;
       if (ok && !*s_abort && col < g.m) {
         for (int r = w; r < BM; r += 4) {
           const int lr = rowt + r;
-          if (lr < g.nrows)
-            store_row_sample(g.rs, g.row0 + lr, col, fmaf(g.mu[lr], g.colsum[col], stage[r * kEpiStride + lane]));
+          if (lr < g.nrows) {
+            // the filtered baseline of the row: sum_j c_j (T P_j)[col]
+            const float* cr = g.coef + (size_t)lr * kBasis;
+            float y = stage[r * kEpiStride + lane];
+#pragma unroll
+            for (int j = 0; j < kBasis; ++j) y = fmaf(cr[j], tpc[j], y);
+            store_row_sample(g.rs, g.row0 + lr, col, y);
+          }
         }
       }
       asm volatile("bar.sync 1, 128;" ::: "memory");
@@ -242,30 +265,67 @@ __global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_cons
   }
 }
 
-// X rows (fused log / weight) -> BF16 hi and lo rows of kp samples (zero past
-// m). One warp per row, four samples per lane step: 16-byte loads, 8-byte stores.
+// Legendre polynomials P_0 .. P_8 at t in [-1, 1] by their recurrence
+// (j + 1) P_{j+1} = (2j + 1) t P_j - j P_{j-1}.
+__device__ __forceinline__ void legendre9(float t, float (&p)[kBasis]) {
+  p[0] = 1.f;
+  p[1] = t;
+#pragma unroll
+  for (int j = 1; j + 1 < kBasis; ++j)
+    p[j + 1] = fmaf((float)(2 * j + 1) / (float)(j + 1) * t, p[j], -(float)j / (float)(j + 1) * p[j - 1]);
+}
+
+// X rows (fused log / weight) -> BF16 hi and lo rows of x - b (zero past m),
+// b = the row's degree-8 Legendre fit, whose coefficients go to coef. One
+// warp per row, four samples per lane step: 16-byte loads, 8-byte stores.
 __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long row0, int nrows, int kp,
-                                                         __nv_bfloat16* xh, __nv_bfloat16* xl, float* mu) {
+                                                         __nv_bfloat16* xh, __nv_bfloat16* xl, float* coef,
+                                                         const BasisGram gram) {
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  const float half_span = rs.m > 1 ? 0.5f * (float)(rs.m - 1) : 1.f;
+  const float inv_half = 1.f / half_span;
   for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows; r += warps) {
     const long long gr = row0 + r;
     const float4* src = reinterpret_cast<const float4*>(rs.data + gr * rs.pitch);
     uint2* oh = reinterpret_cast<uint2*>(xh + r * kp);
     uint2* ol = reinterpret_cast<uint2*>(xl + r * kp);
-    // the row's mean (of the weighted / log-normalised values)
-    float sum = 0.f;
+    // moments <x, P_j> of the (weighted / log-normalised) row
+    float mom[kBasis];
+#pragma unroll
+    for (int j = 0; j < kBasis; ++j) mom[j] = 0.f;
     for (int q = lane; 4 * q < rs.m; q += 32) {
       const float4 v = src[q];
       const float raw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
       for (int t = 0; t < 4; ++t)
-        if (4 * q + t < rs.m) sum += pre_op(rs, gr, 4 * q + t, raw[t]);
+        if (4 * q + t < rs.m) {
+          const float x = pre_op(rs, gr, 4 * q + t, raw[t]);
+          float p[kBasis];
+          legendre9(((float)(4 * q + t) - half_span) * inv_half, p);
+#pragma unroll
+          for (int j = 0; j < kBasis; ++j) mom[j] = fmaf(x, p[j], mom[j]);
+        }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    const float mean = sum / (float)rs.m;
-    if (lane == 0) mu[r] = mean;
+    for (int j = 0; j < kBasis; ++j)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mom[j] += __shfl_xor_sync(0xffffffffu, mom[j], o);
+    float c[kBasis];
+#pragma unroll
+    for (int a = 0; a < kBasis; ++a) {
+      float s = 0.f;
+#pragma unroll
+      for (int b = 0; b < kBasis; ++b) s = fmaf(gram.ginv[a * kBasis + b], mom[b], s);
+      c[a] = s;
+    }
+    if (lane < kBasis) {
+      float mine = c[0];
+#pragma unroll
+      for (int a = 1; a < kBasis; ++a)
+        if (lane == a) mine = c[a];
+      coef[r * kBasis + lane] = mine;
+    }
     for (int q = lane; q < (kp >> 2); q += 32) {
       const int i = 4 * q;
       float x[4] = {0.f, 0.f, 0.f, 0.f};
@@ -273,7 +333,16 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
         const float4 v = src[q];
         const float raw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int t = 0; t < 4; ++t) x[t] = i + t < rs.m ? pre_op(rs, gr, i + t, raw[t]) - mean : 0.f;
+        for (int t = 0; t < 4; ++t) {
+          if (i + t < rs.m) {
+            float p[kBasis];
+            legendre9(((float)(i + t) - half_span) * inv_half, p);
+            float b = 0.f;
+#pragma unroll
+            for (int j = 0; j < kBasis; ++j) b = fmaf(c[j], p[j], b);
+            x[t] = pre_op(rs, gr, i + t, raw[t]) - b;
+          }
+        }
       }
       __nv_bfloat16 h[4], l[4];
 #pragma unroll
@@ -287,12 +356,25 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
   }
 }
 
-// s[i] = sum over k < m of T[k][i] = g[(i - k) mod n], summed in FP64.
-__global__ void toeplitz_colsum_kernel(const float* g, int n, int m, float* s) {
+// tp[j][i] = sum over k < m of P_j(t_k) T[k][i] = P_j(t_k) g[(i - k) mod n], in FP64.
+__global__ void toeplitz_basis_kernel(const float* g, int n, int m, float* tp) {
+  const double half = m > 1 ? 0.5 * (m - 1) : 1.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int k = 0; k < m; ++k) acc += (double)g[(((i - k) % n) + n) % n];
-    s[i] = (float)acc;
+    double acc[kBasis];
+    for (int j = 0; j < kBasis; ++j) acc[j] = 0.0;
+    for (int k = 0; k < m; ++k) {
+      const double t = (k - half) / half, gk = (double)g[(((i - k) % n) + n) % n];
+      double pm = 1.0, pj = t;
+      acc[0] += gk;
+      acc[1] += t * gk;
+      for (int j = 1; j + 1 < kBasis; ++j) {
+        const double pn = ((2 * j + 1) * t * pj - j * pm) / (j + 1);
+        acc[j + 1] += pn * gk;
+        pm = pj;
+        pj = pn;
+      }
+    }
+    for (int j = 0; j < kBasis; ++j) tp[(size_t)j * m + i] = (float)acc[j];
   }
 }
 
@@ -315,6 +397,43 @@ __global__ void build_toeplitz_kernel(const float* g, int n, int m, int kp, __nv
 
 bool toeplitz_supported(int m) { return m >= 64 && m <= 8192; }
 
+namespace {
+// Inverse Gram matrix of P_0 .. P_8 at t_k = (k - (m - 1) / 2) / ((m - 1) / 2),
+// k < m, in FP64 (Gauss-Jordan with partial pivoting; the matrix is nearly
+// diagonal), rounded to FP32.
+BasisGram basis_gram(int m) {
+  double G[kBasis][2 * kBasis] = {};
+  const double half = m > 1 ? 0.5 * (m - 1) : 1.0;
+  for (int k = 0; k < m; ++k) {
+    const double t = (k - half) / half;
+    double p[kBasis];
+    p[0] = 1.0;
+    p[1] = t;
+    for (int j = 1; j + 1 < kBasis; ++j) p[j + 1] = ((2 * j + 1) * t * p[j] - j * p[j - 1]) / (j + 1);
+    for (int a = 0; a < kBasis; ++a)
+      for (int b = 0; b < kBasis; ++b) G[a][b] += p[a] * p[b];
+  }
+  for (int a = 0; a < kBasis; ++a) G[a][kBasis + a] = 1.0;
+  for (int col = 0; col < kBasis; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < kBasis; ++r)
+      if (std::fabs(G[r][col]) > std::fabs(G[piv][col])) piv = r;
+    for (int c = 0; c < 2 * kBasis; ++c) std::swap(G[col][c], G[piv][c]);
+    const double d = G[col][col];
+    for (int c = 0; c < 2 * kBasis; ++c) G[col][c] /= d;
+    for (int r = 0; r < kBasis; ++r) {
+      if (r == col) continue;
+      const double f = G[r][col];
+      for (int c = 0; c < 2 * kBasis; ++c) G[r][c] -= f * G[col][c];
+    }
+  }
+  BasisGram out;
+  for (int a = 0; a < kBasis; ++a)
+    for (int b = 0; b < kBasis; ++b) out.ginv[a * kBasis + b] = (float)G[a][kBasis + b];
+  return out;
+}
+}  // namespace
+
 int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter) {
   const int m = rs.m;
   if (!toeplitz_supported(m)) return set_error(ctx, FBP_ERR_UNSUPPORTED, "Toeplitz filter needs 64 <= width <= 8192");
@@ -324,7 +443,7 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   if (!(t.m == m && t.n == n && t.filter == filter)) {
     t.m = 0;
     const size_t bytes = sizeof(__nv_bfloat16) * (size_t)m * kp;
-    const size_t need = 2 * bytes + sizeof(float) * m;
+    const size_t need = 2 * bytes + sizeof(float) * kBasis * m;
     if (need > t.cap) {  // grow only
       cudaFree(t.th);
       t.th = nullptr;
@@ -336,9 +455,9 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
     build_toeplitz_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, kp, (__nv_bfloat16*)t.th,
                                                                      (__nv_bfloat16*)t.th + (size_t)m * kp);
     if (int rc = launched(ctx, "build_toeplitz_kernel")) return rc;
-    toeplitz_colsum_kernel<<<(m + 127) / 128, 128, 0, ctx->stream>>>(
+    toeplitz_basis_kernel<<<(m + 127) / 128, 128, 0, ctx->stream>>>(
         ctx->ftab.kernel, n, m, reinterpret_cast<float*>(static_cast<unsigned char*>(t.th) + 2 * bytes));
-    if (int rc = launched(ctx, "toeplitz_colsum_kernel")) return rc;
+    if (int rc = launched(ctx, "toeplitz_basis_kernel")) return rc;
     t.m = m;
     t.n = n;
     t.filter = filter;
@@ -346,13 +465,15 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   // rows in chunks so that the split operands stay small
   const long long chunk = std::min<long long>(rs.rows, 1LL << 16);
   const size_t sbytes = sizeof(__nv_bfloat16) * (size_t)chunk * kp;
-  unsigned char* sp = static_cast<unsigned char*>(scratch(ctx, 2 * sbytes + sizeof(float) * chunk + 1024));
+  unsigned char* sp =
+      static_cast<unsigned char*>(scratch(ctx, 2 * sbytes + sizeof(float) * kBasis * chunk + 1024));
   if (!sp) return FBP_ERR_OUT_OF_MEMORY;
   __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(sp);
   __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(sp + sbytes);
-  float* mu = reinterpret_cast<float*>(sp + 2 * sbytes);
-  const float* colsum = reinterpret_cast<const float*>(static_cast<const unsigned char*>(t.th) +
-                                                        2 * sizeof(__nv_bfloat16) * (size_t)m * kp);
+  float* coef = reinterpret_cast<float*>(sp + 2 * sbytes);
+  const float* tp = reinterpret_cast<const float*>(static_cast<const unsigned char*>(t.th) +
+                                                    2 * sizeof(__nv_bfloat16) * (size_t)m * kp);
+  const BasisGram gram = basis_gram(m);
   CUtensorMap mah, mal, mbh, mbl;
   if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mah, xh, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
   if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mal, xl, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
@@ -365,7 +486,7 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   const int ntn = (m + BN - 1) / BN;
   for (long long r0 = 0; r0 < rs.rows; r0 += chunk) {
     const int nr = (int)std::min<long long>(chunk, rs.rows - r0);
-    split_rows_kernel<<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl, mu);
+    split_rows_kernel<<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
     if (int rc = launched(ctx, "split_rows_kernel")) return rc;
     GemmArgs ga;
     ga.rs = rs;
@@ -373,8 +494,8 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
     ga.nrows = nr;
     ga.m = m;
     ga.ntile_n = ntn;
-    ga.mu = mu;
-    ga.colsum = colsum;
+    ga.coef = coef;
+    ga.tp = tp;
     ga.err = ctx->d_err;
     const int grid = ((nr + BM - 1) / BM) * ntn;
     toeplitz_gemm_kernel<<<grid, 256, smem, ctx->stream>>>(mah, mal, mbh, mbl, ga);

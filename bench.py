@@ -183,7 +183,13 @@ def sample_error(got, ref, bands=None) -> dict:
     d = np.asarray(got, np.float64) - ref
     out = {"rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref)), "max_abs": float(np.abs(d).max())}
     if bands:
+        # per band: RMSE over the band's own reference RMS (ill-conditioned where
+        # the band holds almost no signal, e.g. slices outside the phantom) and
+        # over the whole sample's reference RMS
+        rms_all = float(np.sqrt(np.mean(ref ** 2)))
         out["bands"] = {k: {"rel_rmse": float(np.linalg.norm(d[a:b]) / np.linalg.norm(ref[a:b])),
+                            "rmse_over_sample_rms": float(np.sqrt(np.mean(d[a:b] ** 2)) / rms_all),
+                            "ref_rms_over_sample_rms": float(np.sqrt(np.mean(ref[a:b] ** 2)) / rms_all),
                             "max_abs": float(np.abs(d[a:b]).max())} for k, (a, b) in bands.items()}
     return out
 

