@@ -129,7 +129,11 @@ struct fbp_server {
   std::thread engine;
   fbp_context* launcher[2] = {nullptr, nullptr};
   cudaEvent_t launched_ev[2] = {nullptr, nullptr};
+  cudaEvent_t start_ev[2] = {nullptr, nullptr};  // timing of each launcher's launch in flight
   bool launcher_busy[2] = {false, false};
+  // statistics (under mu): device time of the batched launches, host time in transfers
+  double stat_batch_ms = 0, stat_upload_ms = 0, stat_readback_ms = 0;
+  long long stat_launches = 0, stat_batched_jobs = 0;
   std::deque<BatchJob*> incoming;  // handed over, not yet planned (under mu)
   std::condition_variable engine_cv, batch_cv;
   bool engine_stop = false;
@@ -181,7 +185,12 @@ struct fbp_server {
     if (r.kind == FBP_JOB_CONE && batching && launcher[0]) {
       // upload, weights and filter here; the engine backprojects; then readback
       if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
+      const double tu = now_ms();
       if (!rc) rc = fbp_upload_projections(c, r.input, r.det_cols, r.det_rows, r.views, 0);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        stat_upload_ms += now_ms() - tu;
+      }
       if (!rc) rc = fbp_apply_fdk_weights_to_projections(c, g.source_distance, g.detector_distance, g.detector_width);
       if (!rc) rc = fbp_apply_filter_to_projections(c, r.filter_type);
       if (!rc) {
@@ -201,7 +210,13 @@ struct fbp_server {
         if (rc) j.error = bj.error;
         if (bj.plan) fbp::free_bp_plan(bj.plan);
       }
+      const double tr = now_ms();
       if (!rc) rc = fbp_read_volume(c, r.output, 0);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        stat_readback_ms += now_ms() - tr;
+        ++stat_batched_jobs;
+      }
     } else if (r.kind == FBP_JOB_CONE) {
       // one call: upload, weights, filter, slab-wise backprojection with the
       // volume readback overlapped (large volumes in 4 slabs)
@@ -279,7 +294,15 @@ struct fbp_server {
       // one launch: tiles of the waiting jobs in arrival order, about
       // kChunkUpdates updates, all of the first job's batch key
       fbp_context* L = launcher[turn];
-      if (launcher_busy[turn]) cudaEventSynchronize(launched_ev[turn]);  // at most one launch per launcher in flight
+      if (launcher_busy[turn]) {  // at most one launch per launcher in flight
+        cudaEventSynchronize(launched_ev[turn]);
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, start_ev[turn], launched_ev[turn]) == cudaSuccess) {
+          std::lock_guard<std::mutex> lk(mu);
+          stat_batch_ms += ms;
+        }
+        launcher_busy[turn] = false;
+      }
       const long long key = active.front()->key;
       std::vector<fbp::BPLaunchPlan*> plans;
       std::vector<long long> t0, t1;
@@ -302,7 +325,12 @@ struct fbp_server {
       int rc = FBP_OK;
       for (BatchJob* b : members)
         if (cudaStreamWaitEvent(L->stream, b->ctx->ev_sync, 0) != cudaSuccess) rc = FBP_ERR_CUDA;
+      if (!rc && cudaEventRecord(start_ev[turn], L->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
       if (!rc) rc = fbp::launch_bp_batch(L, plans.data(), (int)plans.size(), t0.data(), t1.data());
+      if (!rc) {
+        std::lock_guard<std::mutex> lk(mu);
+        ++stat_launches;
+      }
       if (!rc && cudaEventRecord(launched_ev[turn], L->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
       launcher_busy[turn] = true;
       for (size_t i = 0; i < members.size(); ++i) {
@@ -416,7 +444,8 @@ int fbp_server_create(fbp_server** out, int device, size_t hbm_budget_bytes, int
     }
     for (int i = 0; i < 2 && !rc; ++i) {
       rc = fbp_create(&s->launcher[i], device);
-      if (!rc && cudaEventCreateWithFlags(&s->launched_ev[i], cudaEventDisableTiming) != cudaSuccess) rc = FBP_ERR_CUDA;
+      if (!rc && (cudaEventCreate(&s->launched_ev[i]) != cudaSuccess || cudaEventCreate(&s->start_ev[i]) != cudaSuccess))
+        rc = FBP_ERR_CUDA;
     }
     cudaSetDevice(prev);
     if (rc) {
@@ -424,6 +453,7 @@ int fbp_server_create(fbp_server** out, int device, size_t hbm_budget_bytes, int
       for (int i = 0; i < 2; ++i) {
         fbp_destroy(s->launcher[i]);
         if (s->launched_ev[i]) cudaEventDestroy(s->launched_ev[i]);
+        if (s->start_ev[i]) cudaEventDestroy(s->start_ev[i]);
       }
       for (cudaStream_t st : s->worker_streams) cudaStreamDestroy(st);
       delete s;
@@ -442,6 +472,18 @@ int fbp_server_set_batching(fbp_server* s, int enable, double chunk_updates) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->batching = enable != 0;
   s->chunk_updates = chunk_updates > 0 ? chunk_updates : kChunkUpdates;
+  return FBP_OK;
+}
+
+int fbp_server_stats(fbp_server* s, double* batch_gpu_ms, double* upload_ms, double* readback_ms,
+                     long long* batch_launches, long long* batched_jobs) {
+  if (!s) return FBP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (batch_gpu_ms) *batch_gpu_ms = s->stat_batch_ms;
+  if (upload_ms) *upload_ms = s->stat_upload_ms;
+  if (readback_ms) *readback_ms = s->stat_readback_ms;
+  if (batch_launches) *batch_launches = s->stat_launches;
+  if (batched_jobs) *batched_jobs = s->stat_batched_jobs;
   return FBP_OK;
 }
 
@@ -509,6 +551,7 @@ int fbp_server_destroy(fbp_server* s) {
   for (int i = 0; i < 2; ++i) {
     fbp_destroy(s->launcher[i]);
     if (s->launched_ev[i]) cudaEventDestroy(s->launched_ev[i]);
+    if (s->start_ev[i]) cudaEventDestroy(s->start_ev[i]);
   }
   for (cudaStream_t st : s->worker_streams) cudaStreamDestroy(st);
   for (auto& kv : s->jobs) delete kv.second;

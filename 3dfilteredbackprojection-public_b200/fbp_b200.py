@@ -171,6 +171,8 @@ SIGNATURES = {
     "fbp_server_create": [C.POINTER(C.c_void_p), _I, C.c_size_t, _I],
     "fbp_server_submit": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
     "fbp_server_set_batching": [C.c_void_p, _I, C.c_double],
+    "fbp_server_stats": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                         C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "fbp_server_wait": [C.c_void_p, C.c_longlong, C.c_void_p],
     "fbp_server_destroy": [C.c_void_p],
     "fbp_set_detector_rows": [_P, _I, _I],
@@ -228,6 +230,16 @@ class Server:
         rc = self.lib.fbp_server_set_batching(self.handle, 1 if enable else 0, float(chunk_updates))
         if rc != 0:
             raise FBPError(rc, "fbp_server_set_batching failed")
+
+    def stats(self) -> dict:
+        """fbp_server_stats: batched backprojection device time, upload / readback host time."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        d, e = C.c_longlong(), C.c_longlong()
+        rc = self.lib.fbp_server_stats(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e))
+        if rc != 0:
+            raise FBPError(rc, "fbp_server_stats failed")
+        return {"batch_gpu_ms": a.value, "upload_ms": b.value, "readback_ms": c.value,
+                "batch_launches": d.value, "batched_jobs": e.value}
 
     def submit(self, request: Request, keep=None) -> int:
         t = C.c_longlong()

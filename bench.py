@@ -470,13 +470,14 @@ def serving_block(args, n_requests: int, n_poisson: int) -> dict:
             rr[key] += 1
             tickets.append(srv.submit(request_struct(r, precision, out)))
         res = [srv.wait(t) for t in tickets]
+        st = srv.stats()
         srv.close()
         bad = [x.error.decode() for x in res if x.status != 0]
         assert not bad, bad[:3]
         lat = np.array([x.finished_ms - x.queued_ms for x in res])
         span = (max(x.finished_ms for x in res) - min(x.queued_ms for x in res)) * 1e-3
         return dict(requests=len(res), recon_per_s=len(res) / span, p50_ms=float(np.percentile(lat, 50)),
-                    p99_ms=float(np.percentile(lat, 99)), makespan_s=span)
+                    p99_ms=float(np.percentile(lat, 99)), makespan_s=span, server_stats=st)
 
     # ---- plain one at a time: per-shape service times
     srv = server(F.Precision.FP32, 1)

@@ -295,6 +295,13 @@ int fbp_server_create(fbp_server** server, int device, size_t hbm_budget_bytes, 
  * about chunk_updates voxel-view updates (<= 0: 6e10, about 20 ms) mixed
  * with the other waiting jobs' tiles; 0: each job launches its own kernels. */
 int fbp_server_set_batching(fbp_server* server, int enable, double chunk_updates);
+/* Since the server was created: device time of the batched backprojection
+ * launches (each launch timed on its stream, summed), host time the cone
+ * jobs of the batching path spent in their uploads and volume readbacks
+ * (summed over workers), batched launches, and jobs that took that path.
+ * Any output pointer may be NULL. */
+int fbp_server_stats(fbp_server* server, double* batch_gpu_ms, double* upload_ms, double* readback_ms,
+                     long long* batch_launches, long long* batched_jobs);
 int fbp_server_submit(fbp_server* server, const fbp_request* request, long long* ticket);
 int fbp_server_wait(fbp_server* server, long long ticket, fbp_job_result* result);
 int fbp_server_destroy(fbp_server* server); /* runs the queued jobs, then stops */
