@@ -8,7 +8,7 @@
 // BF16 hi + lo parts (hi = bf16(x), lo = bf16(x - hi)), and
 // Y = Xh Th + Xh Tl + Xl Th is accumulated in FP32 in tensor memory (the
 // dropped Xl Tl term and the split residuals are ~2^-17 of |x|). Each row's
-// smooth baseline b (a degree-8 Legendre fit of the row, 9 coefficients) is
+// smooth baseline b (a degree-8 Chebyshev fit of the row, 9 coefficients) is
 // taken out before the split and its filtered contribution T b = sum_j c_j
 // (T P_j) (the columns T P_j summed in FP64) added in the epilogue: detector
 // rows sit on large, slowly varying values (line integrals of ~10, plateaus
@@ -48,7 +48,7 @@ constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 96 KB
 constexpr int TMEM_COLS = 256;
 constexpr uint32_t kWait = 1u << 22;
 constexpr int kEpiStride = 33;  // floats per staged row (bank-conflict-free)
-constexpr int kBasis = 9;       // Legendre polynomials P_0 .. P_8 of the row baseline
+constexpr int kBasis = 9;       // Chebyshev polynomials P_0 .. P_8 of the row baseline
 
 // Inverse Gram matrix of the baseline basis on the row's samples (FP64 on the
 // host, rounded to FP32): coefficients c = Ginv * (moments <x, P_j>).
@@ -265,47 +265,58 @@ __global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_cons
   }
 }
 
-// Legendre polynomials P_0 .. P_8 at t in [-1, 1] by their recurrence
-// (j + 1) P_{j+1} = (2j + 1) t P_j - j P_{j-1}.
-__device__ __forceinline__ void legendre9(float t, float (&p)[kBasis]) {
+// Chebyshev polynomials P_0 .. P_8 at t in [-1, 1]: P_{j+1} = 2 t P_j - P_{j-1}.
+__device__ __forceinline__ void cheb9(float t, float (&p)[kBasis]) {
+  const float t2 = t + t;
   p[0] = 1.f;
   p[1] = t;
 #pragma unroll
-  for (int j = 1; j + 1 < kBasis; ++j)
-    p[j + 1] = fmaf((float)(2 * j + 1) / (float)(j + 1) * t, p[j], -(float)j / (float)(j + 1) * p[j - 1]);
+  for (int j = 1; j + 1 < kBasis; ++j) p[j + 1] = fmaf(t2, p[j], -p[j - 1]);
 }
 
 // X rows (fused log / weight) -> BF16 hi and lo rows of x - b (zero past m),
-// b = the row's degree-8 Legendre fit, whose coefficients go to coef. One
+// b = the row's degree-8 Chebyshev fit, whose coefficients go to coef. One
 // warp per row, four samples per lane step: 16-byte loads, 8-byte stores.
+// STAGE: the row's pre-processed samples wait in shared memory (kp floats per
+// warp) between the fit and the split instead of being read and
+// pre-processed twice.
+template <bool STAGE>
 __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long row0, int nrows, int kp,
                                                          __nv_bfloat16* xh, __nv_bfloat16* xl, float* coef,
                                                          const BasisGram gram) {
-  const int lane = threadIdx.x & 31;
+  extern __shared__ __align__(16) float rowbuf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float4* buf = reinterpret_cast<float4*>(rowbuf + (size_t)wib * kp);
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   const float half_span = rs.m > 1 ? 0.5f * (float)(rs.m - 1) : 1.f;
   const float inv_half = 1.f / half_span;
-  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows; r += warps) {
+  const int nq4 = kp >> 2;  // float4 groups of the padded row
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + wib; r < nrows; r += warps) {
     const long long gr = row0 + r;
     const float4* src = reinterpret_cast<const float4*>(rs.data + gr * rs.pitch);
     uint2* oh = reinterpret_cast<uint2*>(xh + r * kp);
     uint2* ol = reinterpret_cast<uint2*>(xl + r * kp);
-    // moments <x, P_j> of the (weighted / log-normalised) row
+    // moments <x, P_j> of the pre-processed row (zero past m)
     float mom[kBasis];
 #pragma unroll
     for (int j = 0; j < kBasis; ++j) mom[j] = 0.f;
-    for (int q = lane; 4 * q < rs.m; q += 32) {
-      const float4 v = src[q];
-      const float raw[4] = {v.x, v.y, v.z, v.w};
+    for (int q = lane; q < nq4; q += 32) {
+      float x[4] = {0.f, 0.f, 0.f, 0.f};
+      if (4 * q < rs.m) {  // the row pitch is a multiple of 4: the 16-byte load stays in the row
+        const float4 v = src[q];
+        const float raw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-      for (int t = 0; t < 4; ++t)
-        if (4 * q + t < rs.m) {
-          const float x = pre_op(rs, gr, 4 * q + t, raw[t]);
-          float p[kBasis];
-          legendre9(((float)(4 * q + t) - half_span) * inv_half, p);
+        for (int t = 0; t < 4; ++t)
+          if (4 * q + t < rs.m) x[t] = pre_op(rs, gr, 4 * q + t, raw[t]);
+      }
+      if (STAGE) buf[q] = make_float4(x[0], x[1], x[2], x[3]);
 #pragma unroll
-          for (int j = 0; j < kBasis; ++j) mom[j] = fmaf(x, p[j], mom[j]);
-        }
+      for (int t = 0; t < 4; ++t) {
+        float p[kBasis];
+        cheb9(((float)(4 * q + t) - half_span) * inv_half, p);
+#pragma unroll
+        for (int j = 0; j < kBasis; ++j) mom[j] = fmaf(x[t], p[j], mom[j]);
+      }
     }
 #pragma unroll
     for (int j = 0; j < kBasis; ++j)
@@ -314,10 +325,10 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
     float c[kBasis];
 #pragma unroll
     for (int a = 0; a < kBasis; ++a) {
-      float s = 0.f;
+      float sum = 0.f;
 #pragma unroll
-      for (int b = 0; b < kBasis; ++b) s = fmaf(gram.ginv[a * kBasis + b], mom[b], s);
-      c[a] = s;
+      for (int b = 0; b < kBasis; ++b) sum = fmaf(gram.ginv[a * kBasis + b], mom[b], sum);
+      c[a] = sum;
     }
     if (lane < kBasis) {
       float mine = c[0];
@@ -326,23 +337,27 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
         if (lane == a) mine = c[a];
       coef[r * kBasis + lane] = mine;
     }
-    for (int q = lane; q < (kp >> 2); q += 32) {
-      const int i = 4 * q;
+    // x - b, split into BF16 hi and lo (each lane reads back what it wrote)
+    for (int q = lane; q < nq4; q += 32) {
       float x[4] = {0.f, 0.f, 0.f, 0.f};
-      if (i < rs.m) {  // the row pitch is a multiple of 4: the 16-byte load stays in the row
+      if (STAGE) {
+        const float4 v = buf[q];
+        x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+      } else if (4 * q < rs.m) {
         const float4 v = src[q];
         const float raw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          if (i + t < rs.m) {
-            float p[kBasis];
-            legendre9(((float)(i + t) - half_span) * inv_half, p);
-            float b = 0.f;
+        for (int t = 0; t < 4; ++t)
+          if (4 * q + t < rs.m) x[t] = pre_op(rs, gr, 4 * q + t, raw[t]);
+      }
 #pragma unroll
-            for (int j = 0; j < kBasis; ++j) b = fmaf(c[j], p[j], b);
-            x[t] = pre_op(rs, gr, i + t, raw[t]) - b;
-          }
-        }
+      for (int t = 0; t < 4; ++t) {
+        float p[kBasis];
+        cheb9(((float)(4 * q + t) - half_span) * inv_half, p);
+        float b = 0.f;
+#pragma unroll
+        for (int j = 0; j < kBasis; ++j) b = fmaf(c[j], p[j], b);
+        x[t] = 4 * q + t < rs.m ? x[t] - b : 0.f;
       }
       __nv_bfloat16 h[4], l[4];
 #pragma unroll
@@ -368,7 +383,7 @@ __global__ void toeplitz_basis_kernel(const float* g, int n, int m, float* tp) {
       acc[0] += gk;
       acc[1] += t * gk;
       for (int j = 1; j + 1 < kBasis; ++j) {
-        const double pn = ((2 * j + 1) * t * pj - j * pm) / (j + 1);
+        const double pn = 2.0 * t * pj - pm;
         acc[j + 1] += pn * gk;
         pm = pj;
         pj = pn;
@@ -398,7 +413,7 @@ __global__ void build_toeplitz_kernel(const float* g, int n, int m, int kp, __nv
 bool toeplitz_supported(int m) { return m >= 64 && m <= 8192; }
 
 namespace {
-// Inverse Gram matrix of P_0 .. P_8 at t_k = (k - (m - 1) / 2) / ((m - 1) / 2),
+// Inverse Gram matrix of the Chebyshev P_0 .. P_8 at t_k = (k - (m - 1) / 2) / ((m - 1) / 2),
 // k < m, in FP64 (Gauss-Jordan with partial pivoting; the matrix is nearly
 // diagonal), rounded to FP32.
 BasisGram basis_gram(int m) {
@@ -409,7 +424,7 @@ BasisGram basis_gram(int m) {
     double p[kBasis];
     p[0] = 1.0;
     p[1] = t;
-    for (int j = 1; j + 1 < kBasis; ++j) p[j + 1] = ((2 * j + 1) * t * p[j] - j * p[j - 1]) / (j + 1);
+    for (int j = 1; j + 1 < kBasis; ++j) p[j + 1] = 2.0 * t * p[j] - p[j - 1];
     for (int a = 0; a < kBasis; ++a)
       for (int b = 0; b < kBasis; ++b) G[a][b] += p[a] * p[b];
   }
@@ -474,6 +489,12 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   const float* tp = reinterpret_cast<const float*>(static_cast<const unsigned char*>(t.th) +
                                                     2 * sizeof(__nv_bfloat16) * (size_t)m * kp);
   const BasisGram gram = basis_gram(m);
+  const size_t stage_smem = kp <= 2048 ? sizeof(float) * 8 * (size_t)kp : 0;  // 8 warps x one padded row
+  if (stage_smem) {
+    const cudaError_t ea =
+        cudaFuncSetAttribute(split_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem);
+    if (ea != cudaSuccess) return cuda_check(ctx, ea, "split smem attribute");
+  }
   CUtensorMap mah, mal, mbh, mbl;
   if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mah, xh, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
   if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mal, xl, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
@@ -486,7 +507,10 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   const int ntn = (m + BN - 1) / BN;
   for (long long r0 = 0; r0 < rs.rows; r0 += chunk) {
     const int nr = (int)std::min<long long>(chunk, rs.rows - r0);
-    split_rows_kernel<<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
+    if (stage_smem)  // rows of up to 2048 samples wait in shared memory between the two passes
+      split_rows_kernel<true><<<ctx->num_sms * 4, 256, stage_smem, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
+    else
+      split_rows_kernel<false><<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
     if (int rc = launched(ctx, "split_rows_kernel")) return rc;
     GemmArgs ga;
     ga.rs = rs;
