@@ -17,10 +17,10 @@
 // allocating; the budget covers the working sets of running jobs, and each
 // slot retains at most its largest job's buffers.
 //
-// Batching (on by default): a cone job's worker uploads, weights and filters
-// on its own (high-priority) stream, then hands the backprojection to the
-// server's engine thread. The engine plans each job (packing, footprint pass)
-// and feeds the tiles of all waiting jobs to the persistent multi-job
+// Batching (on by default): a cone job's worker uploads, weights, filters and
+// plans the backprojection (packing, footprint pass) on its own
+// (high-priority) stream, then hands it to the server's engine thread, which
+// feeds the tiles of all waiting jobs to the persistent multi-job
 // backprojector (launch_bp_batch): each launch carries about kChunkUpdates
 // voxel-view updates, taken from the jobs in arrival order, so a large job's
 // tiles are spread over several launches and jobs that arrive meanwhile join
@@ -200,7 +200,10 @@ struct fbp_server {
         bj.geom.kind = FBP_GEOMETRY_CONE;
         bj.h = r.vol_h;
         bj.v = r.vol_v;
-        {
+        // plan here, on this worker's stream (packing, footprint pass), so
+        // that the engine thread only launches
+        prepare(bj);
+        if (bj.status == FBP_OK && bj.tiles > 0) {
           std::unique_lock<std::mutex> lk(mu);
           incoming.push_back(&bj);
           engine_cv.notify_all();
@@ -262,31 +265,6 @@ struct fbp_server {
         while (!incoming.empty()) {
           active.push_back(incoming.front());
           incoming.pop_front();
-        }
-      }
-      // plan new jobs on their own streams; jobs off the symmetric path launch alone
-      for (BatchJob* b : active) {
-        if (b->planned) continue;
-        b->planned = true;
-        b->plan = fbp::new_bp_plan();
-        int rc = fbp::plan_cone_projections(b->ctx, b->geom, b->h, b->v, b->plan);
-        if (!rc) {
-          b->key = fbp::bp_plan_batch_key(*b->plan);
-          if (b->key == 0) {
-            rc = fbp::launch_bp_plan(b->ctx, *b->plan);
-            b->next = b->tiles = 0;
-          } else {
-            b->tiles = fbp::bp_plan_tiles(*b->plan);
-            const double all = (double)b->h * b->h * b->v * (double)b->ctx->proj.n;
-            b->per_tile = all / (double)std::max(1LL, b->tiles);
-            // the job's preparatory work (on its stream) precedes every launch of its tiles
-            if (!b->ctx->ev_sync) cudaEventCreateWithFlags(&b->ctx->ev_sync, cudaEventDisableTiming);
-            if (cudaEventRecord(b->ctx->ev_sync, b->ctx->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
-          }
-        }
-        if (rc) {
-          b->status = rc;
-          b->error = fbp_last_error(b->ctx);
         }
       }
       finish(active);
@@ -351,6 +329,32 @@ struct fbp_server {
       }
       turn ^= 1;
       finish(active);
+    }
+  }
+
+  // Plan a handed-over job on its worker's stream; a job off the symmetric
+  // path launches alone there (tiles stays 0).
+  void prepare(BatchJob& b) {
+    b.planned = true;
+    b.plan = fbp::new_bp_plan();
+    int rc = fbp::plan_cone_projections(b.ctx, b.geom, b.h, b.v, b.plan);
+    if (!rc) {
+      b.key = fbp::bp_plan_batch_key(*b.plan);
+      if (b.key == 0) {
+        rc = fbp::launch_bp_plan(b.ctx, *b.plan);
+        b.next = b.tiles = 0;
+      } else {
+        b.tiles = fbp::bp_plan_tiles(*b.plan);
+        const double all = (double)b.h * b.h * b.v * (double)b.ctx->proj.n;
+        b.per_tile = all / (double)std::max(1LL, b.tiles);
+        // the job's preparatory work (on its stream) precedes every launch of its tiles
+        if (!b.ctx->ev_sync) cudaEventCreateWithFlags(&b.ctx->ev_sync, cudaEventDisableTiming);
+        if (cudaEventRecord(b.ctx->ev_sync, b.ctx->stream) != cudaSuccess) rc = FBP_ERR_CUDA;
+      }
+    }
+    if (rc) {
+      b.status = rc;
+      b.error = fbp_last_error(b.ctx);
     }
   }
 
