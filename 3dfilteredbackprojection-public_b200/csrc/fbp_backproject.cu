@@ -950,22 +950,20 @@ __global__ void __launch_bounds__(256 + 32, OCC)
       return;
     }
     const QuadCoef g = coef[e];
-    if (g.flags & (kQExit | kQFirst)) {
-      if (g.flags & kQExit) {  // multi-job launch: no more items (always at a group start)
-        leave = true;
-      } else {
-        item = g.item;
-        if constexpr (MULTI) {
+    if constexpr (MULTI) {  // one job's single item: set up before the loop, the loop counts its quads
+      if (g.flags & (kQExit | kQFirst)) {
+        if (g.flags & kQExit) {  // no more items (always at a group start)
+          leave = true;
+        } else {
+          item = g.item;
           jb = find_job(qq, item);
           const BPArgs& ja = qq.jobs[jb].a;
           const ItemTile til = item_tile<QG, NY>(ja, item - qq.jobs[jb].item0 + qq.jobs[jb].t0, qq.jobs[jb].nbh);
           grp = til.g0;
-        } else {
-          grp = item_tile<QG, NY>(a, item, a.ntx >> 1).g0;
         }
       }
+      last = (g.flags & kQLast) != 0;
     }
-    last = (g.flags & kQLast) != 0;
     if (!(g.flags & kQSkip)) {
       // explicit roundings (no contraction): the same bits in every instantiation
       const float D = fmaf(g.Dx, fx, fmaf(g.Dz, fz, g.D0));
@@ -1173,6 +1171,43 @@ __global__ void __launch_bounds__(256 + 32, OCC)
   };
   static_assert(kKahanQuads == 4 && kFoldQG % 4 == 0, "folds on whole groups of four quads");
   int kq = 0;
+  if constexpr (!MULTI) {
+    // one work item, K quads (as many as views): a loop of known length
+    item = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+    const int K = a.nviews;
+    if constexpr (QG) {
+      grp = item_tile<QG, NY>(a, item, a.ntx >> 1).g0;
+      const int Q = K >> 2;
+      for (int q = 0; q < K; q += 4) {
+        step(std::integral_constant<int, 0>{});
+        if (stop) break;
+        step(std::integral_constant<int, 1>{});
+        if (stop) break;
+        step(std::integral_constant<int, 2>{});
+        if (stop) break;
+        step(std::integral_constant<int, 3>{});
+        if (stop) break;
+        if (KAHAN && (kq += 4) == kFoldQG) {
+          kq = 0;
+          fold();
+        }
+        if (++grp == Q) grp = 0;
+      }
+    } else {
+      for (int q = 0; q < K; ++q) {
+        step(std::integral_constant<int, 0>{});
+        if (stop) break;
+        if (KAHAN && ++kq == kKahanQuads) {
+          kq = 0;
+          fold();
+        }
+      }
+    }
+    if (bad) atomicCAS(a.err, 0, kDevFootprint);
+    if (stop || *s_abort) return;
+    store();
+    return;
+  }
   for (;;) {
     if constexpr (QG) {
       // a group of four quads (an item's quads come in whole groups)

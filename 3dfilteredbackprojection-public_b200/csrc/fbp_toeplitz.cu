@@ -491,8 +491,10 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   const BasisGram gram = basis_gram(m);
   const size_t stage_smem = kp <= 2048 ? sizeof(float) * 8 * (size_t)kp : 0;  // 8 warps x one padded row
   if (stage_smem) {
-    const cudaError_t ea =
-        cudaFuncSetAttribute(split_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem);
+    // the attribute is process-wide and other contexts launch with other row
+    // lengths: always the largest staged size (8 rows of 2048 samples)
+    const cudaError_t ea = cudaFuncSetAttribute(split_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)(sizeof(float) * 8 * 2048));
     if (ea != cudaSuccess) return cuda_check(ctx, ea, "split smem attribute");
   }
   CUtensorMap mah, mal, mbh, mbl;
