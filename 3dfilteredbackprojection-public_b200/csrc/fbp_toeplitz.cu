@@ -8,16 +8,19 @@
 // BF16 hi + lo parts (hi = bf16(x), lo = bf16(x - hi)), and
 // Y = Xh Th + Xh Tl + Xl Th is accumulated in FP32 in tensor memory (the
 // dropped Xl Tl term and the split residuals are ~2^-17 of |x|). Each row's
-// smooth baseline b (a degree-8 Chebyshev fit of the row, 9 coefficients) is
-// taken out before the split and its filtered contribution T b = sum_j c_j
-// (T P_j) (the columns T P_j summed in FP64) added in the epilogue: detector
-// rows sit on large, slowly varying values (line integrals of ~10, plateaus
-// of opaque rays) against a high-pass output ten to a hundred times smaller,
-// and the split's error follows |x - b| instead of |x|. On the noisy 2D fan
-// case (768 bins, Poisson I0 = 1e5) the image error against the FP64 oracle
-// is 3.2e-4 with the row mean alone and 4.1e-5 with the degree-8 baseline
-// (numpy emulation of the same split); any baseline is exact in principle,
-// since the same coefficients are subtracted and added back.
+// smooth baseline b = sum_j c_j P_j (a degree-8 Chebyshev fit of the row, 9
+// coefficients) is taken out before the split and its filtered contribution
+// T b = sum_j c_j (T P_j) added back by the same tensor-core product: the K
+// extent is extended by one 64-wide block whose first 9 columns hold the
+// coefficients c_j (X side, split hi / lo) and the columns T P_j (T side,
+// summed in FP64, split hi / lo). Detector rows sit on large, slowly varying
+// values (line integrals of ~10, plateaus of opaque rays) against a high-pass
+// output ten to a hundred times smaller, and the split's error follows
+// |x - b| instead of |x|. On the noisy 2D fan case (768 bins, Poisson I0 =
+// 1e5) the image error against the FP64 oracle is 3.2e-4 with the row mean
+// alone and 4.1e-5 with the degree-8 baseline (numpy emulation of the same
+// split); any baseline is exact in principle, since the same coefficients are
+// subtracted and added back (to the split's 16 bits).
 //
 // Kernel: one CTA per 128 x 256 output tile. Warp 0 streams 64-wide K blocks
 // of Xh, Xl, Th, Tl into a two-stage shared-memory ring with TMA (128-byte
@@ -120,8 +123,7 @@ struct GemmArgs {
   int nrows;        // rows in this chunk
   int m;            // samples per row (N and K extent)
   int ntile_n;      // tiles along N
-  const float* coef;    // per chunk row: kBasis coefficients of the baseline taken out before the split
-  const float* tp;      // [j][i]: (T P_j)[i] = sum over k < m of P_j(k) T[k][i]
+  int kblocks;          // 64-wide K blocks: the padded row and the baseline block
   int* err;
 };
 
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_cons
   volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_holder + 1);
   const int nt = blockIdx.x % g.ntile_n, mt = blockIdx.x / g.ntile_n;
   const int rowt = mt * BM, col0 = nt * BN;
-  const int KB = (g.m + BK - 1) / BK;
+  const int KB = g.kblocks;
 
   if (tid == 0) {
     *s_abort = 0;
@@ -238,20 +240,10 @@ __global__ void __launch_bounds__(256, 1) toeplitz_gemm_kernel(const __grid_cons
       asm volatile("bar.sync 1, 128;" ::: "memory");
       // warp w writes tile rows w, w + 4, ...; lane = column: row-contiguous stores
       const int col = col0 + c * 32 + lane;
-      float tpc[kBasis];
-#pragma unroll
-      for (int j = 0; j < kBasis; ++j) tpc[j] = col < g.m ? g.tp[(size_t)j * g.m + col] : 0.f;
       if (ok && !*s_abort && col < g.m) {
         for (int r = w; r < BM; r += 4) {
           const int lr = rowt + r;
-          if (lr < g.nrows) {
-            // the filtered baseline of the row: sum_j c_j (T P_j)[col]
-            const float* cr = g.coef + (size_t)lr * kBasis;
-            float y = stage[r * kEpiStride + lane];
-#pragma unroll
-            for (int j = 0; j < kBasis; ++j) y = fmaf(cr[j], tpc[j], y);
-            store_row_sample(g.rs, g.row0 + lr, col, y);
-          }
+          if (lr < g.nrows) store_row_sample(g.rs, g.row0 + lr, col, stage[r * kEpiStride + lane]);
         }
       }
       asm volatile("bar.sync 1, 128;" ::: "memory");
@@ -275,14 +267,15 @@ __device__ __forceinline__ void cheb9(float t, float (&p)[kBasis]) {
 }
 
 // X rows (fused log / weight) -> BF16 hi and lo rows of x - b (zero past m),
-// b = the row's degree-8 Chebyshev fit, whose coefficients go to coef. One
-// warp per row, four samples per lane step: 16-byte loads, 8-byte stores.
+// b = the row's degree-8 Chebyshev fit, whose coefficients (split the same
+// way) fill the first columns of the row's baseline block [kp, kx). One warp
+// per row, four samples per lane step: 16-byte loads, 8-byte stores.
 // STAGE: the row's pre-processed samples wait in shared memory (kp floats per
 // warp) between the fit and the split instead of being read and
 // pre-processed twice.
 template <bool STAGE>
-__global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long row0, int nrows, int kp,
-                                                         __nv_bfloat16* xh, __nv_bfloat16* xl, float* coef,
+__global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long row0, int nrows, int kp, int kx,
+                                                         __nv_bfloat16* xh, __nv_bfloat16* xl,
                                                          const BasisGram gram) {
   extern __shared__ __align__(16) float rowbuf[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -294,8 +287,8 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
   for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + wib; r < nrows; r += warps) {
     const long long gr = row0 + r;
     const float4* src = reinterpret_cast<const float4*>(rs.data + gr * rs.pitch);
-    uint2* oh = reinterpret_cast<uint2*>(xh + r * kp);
-    uint2* ol = reinterpret_cast<uint2*>(xl + r * kp);
+    uint2* oh = reinterpret_cast<uint2*>(xh + r * kx);
+    uint2* ol = reinterpret_cast<uint2*>(xl + r * kx);
     // moments <x, P_j> of the pre-processed row (zero past m)
     float mom[kBasis];
 #pragma unroll
@@ -330,12 +323,24 @@ __global__ void __launch_bounds__(256) split_rows_kernel(RowSet rs, long long ro
       for (int b = 0; b < kBasis; ++b) sum = fmaf(gram.ginv[a * kBasis + b], mom[b], sum);
       c[a] = sum;
     }
-    if (lane < kBasis) {
-      float mine = c[0];
+    // the baseline block of the row (columns kp .. kp + 63): c_0 .. c_8, then zeros
+    if (lane < (kx - kp) / 4) {
+      float v[4];
 #pragma unroll
-      for (int a = 1; a < kBasis; ++a)
-        if (lane == a) mine = c[a];
-      coef[r * kBasis + lane] = mine;
+      for (int t = 0; t < 4; ++t) {
+        v[t] = 0.f;
+#pragma unroll
+        for (int a = 0; a < kBasis; ++a)
+          if (4 * lane + t == a) v[t] = c[a];
+      }
+      __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        h[t] = __float2bfloat16_rn(v[t]);
+        l[t] = __float2bfloat16_rn(v[t] - __bfloat162float(h[t]));
+      }
+      oh[(kp >> 2) + lane] = *reinterpret_cast<const uint2*>(h);
+      ol[(kp >> 2) + lane] = *reinterpret_cast<const uint2*>(l);
     }
     // x - b, split into BF16 hi and lo (each lane reads back what it wrote)
     for (int q = lane; q < nq4; q += 32) {
@@ -393,14 +398,19 @@ __global__ void toeplitz_basis_kernel(const float* g, int n, int m, float* tp) {
   }
 }
 
-// Bt[i][k] = T[k][i] = g[(i - k) mod n], split into BF16 hi and lo (k < kp).
-__global__ void build_toeplitz_kernel(const float* g, int n, int m, int kp, __nv_bfloat16* th, __nv_bfloat16* tl) {
-  const long long total = (long long)m * kp;
+// Bt[i][k] = T[k][i] = g[(i - k) mod n] for k < m, (T P_j)[i] for k = kp + j
+// (the baseline block), zero otherwise; split into BF16 hi and lo (k < kx).
+__global__ void build_toeplitz_kernel(const float* g, int n, int m, int kp, int kx, const float* tp,
+                                      __nv_bfloat16* th, __nv_bfloat16* tl) {
+  const long long total = (long long)m * kx;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e / kp), k = (int)(e - (long long)i * kp);
+    const int i = (int)(e / kx), k = (int)(e - (long long)i * kx);
     float t = 0.f;
-    if (k < m) t = g[(((i - k) % n) + n) % n];
+    if (k < m)
+      t = g[(((i - k) % n) + n) % n];
+    else if (k >= kp && k < kp + kBasis)
+      t = tp[(size_t)(k - kp) * m + i];
     const __nv_bfloat16 h = __float2bfloat16_rn(t);
     th[e] = h;
     tl[e] = __float2bfloat16_rn(t - __bfloat162float(h));
@@ -454,10 +464,11 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   if (!toeplitz_supported(m)) return set_error(ctx, FBP_ERR_UNSUPPORTED, "Toeplitz filter needs 64 <= width <= 8192");
   if (rs.rows == 0) return FBP_OK;
   const int kp = (m + BK - 1) / BK * BK;  // K padded to whole 64-blocks (16-byte pitch too)
+  const int kx = kp + BK;                  // and one block for the row baseline
   ToeplitzTables& t = ctx->ttab;
   if (!(t.m == m && t.n == n && t.filter == filter)) {
     t.m = 0;
-    const size_t bytes = sizeof(__nv_bfloat16) * (size_t)m * kp;
+    const size_t bytes = sizeof(__nv_bfloat16) * (size_t)m * kx;
     const size_t need = 2 * bytes + sizeof(float) * kBasis * m;
     if (need > t.cap) {  // grow only
       cudaFree(t.th);
@@ -467,27 +478,24 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
       t.cap = need;
     }
     if (int rc = ensure_filter_tables(ctx, n, filter)) return rc;
-    build_toeplitz_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, kp, (__nv_bfloat16*)t.th,
-                                                                     (__nv_bfloat16*)t.th + (size_t)m * kp);
-    if (int rc = launched(ctx, "build_toeplitz_kernel")) return rc;
-    toeplitz_basis_kernel<<<(m + 127) / 128, 128, 0, ctx->stream>>>(
-        ctx->ftab.kernel, n, m, reinterpret_cast<float*>(static_cast<unsigned char*>(t.th) + 2 * bytes));
+    float* tp = reinterpret_cast<float*>(static_cast<unsigned char*>(t.th) + 2 * bytes);
+    toeplitz_basis_kernel<<<(m + 127) / 128, 128, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, tp);
     if (int rc = launched(ctx, "toeplitz_basis_kernel")) return rc;
+    build_toeplitz_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->ftab.kernel, n, m, kp, kx, tp,
+                                                                     (__nv_bfloat16*)t.th,
+                                                                     (__nv_bfloat16*)t.th + (size_t)m * kx);
+    if (int rc = launched(ctx, "build_toeplitz_kernel")) return rc;
     t.m = m;
     t.n = n;
     t.filter = filter;
   }
   // rows in chunks so that the split operands stay small
   const long long chunk = std::min<long long>(rs.rows, 1LL << 16);
-  const size_t sbytes = sizeof(__nv_bfloat16) * (size_t)chunk * kp;
-  unsigned char* sp =
-      static_cast<unsigned char*>(scratch(ctx, 2 * sbytes + sizeof(float) * kBasis * chunk + 1024));
+  const size_t sbytes = sizeof(__nv_bfloat16) * (size_t)chunk * kx;
+  unsigned char* sp = static_cast<unsigned char*>(scratch(ctx, 2 * sbytes + 1024));
   if (!sp) return FBP_ERR_OUT_OF_MEMORY;
   __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(sp);
   __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(sp + sbytes);
-  float* coef = reinterpret_cast<float*>(sp + 2 * sbytes);
-  const float* tp = reinterpret_cast<const float*>(static_cast<const unsigned char*>(t.th) +
-                                                    2 * sizeof(__nv_bfloat16) * (size_t)m * kp);
   const BasisGram gram = basis_gram(m);
   const size_t stage_smem = kp <= 2048 ? sizeof(float) * 8 * (size_t)kp : 0;  // 8 warps x one padded row
   if (stage_smem) {
@@ -498,11 +506,11 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
     if (ea != cudaSuccess) return cuda_check(ctx, ea, "split smem attribute");
   }
   CUtensorMap mah, mal, mbh, mbl;
-  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mah, xh, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
-  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mal, xl, kp, chunk, (uint64_t)kp * 2, BK, BM)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mah, xh, kx, chunk, (uint64_t)kx * 2, BK, BM)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mal, xl, kx, chunk, (uint64_t)kx * 2, BK, BM)) return rc;
   __nv_bfloat16* th = (__nv_bfloat16*)t.th;
-  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbh, th, kp, m, (uint64_t)kp * 2, BK, BN)) return rc;
-  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbl, th + (size_t)m * kp, kp, m, (uint64_t)kp * 2, BK, BN)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbh, th, kx, m, (uint64_t)kx * 2, BK, BN)) return rc;
+  if (int rc = make_tensor_map_2d_bf16_sw128(ctx, &mbl, th + (size_t)m * kx, kx, m, (uint64_t)kx * 2, BK, BN)) return rc;
   const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
   cudaError_t e = cudaFuncSetAttribute(toeplitz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_check(ctx, e, "toeplitz smem attribute");
@@ -510,9 +518,9 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
   for (long long r0 = 0; r0 < rs.rows; r0 += chunk) {
     const int nr = (int)std::min<long long>(chunk, rs.rows - r0);
     if (stage_smem)  // rows of up to 2048 samples wait in shared memory between the two passes
-      split_rows_kernel<true><<<ctx->num_sms * 4, 256, stage_smem, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
+      split_rows_kernel<true><<<ctx->num_sms * 4, 256, stage_smem, ctx->stream>>>(rs, r0, nr, kp, kx, xh, xl, gram);
     else
-      split_rows_kernel<false><<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, xh, xl, coef, gram);
+      split_rows_kernel<false><<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(rs, r0, nr, kp, kx, xh, xl, gram);
     if (int rc = launched(ctx, "split_rows_kernel")) return rc;
     GemmArgs ga;
     ga.rs = rs;
@@ -520,8 +528,7 @@ int launch_filter_toeplitz(fbp_context* ctx, const RowSet& rs, int n, int filter
     ga.nrows = nr;
     ga.m = m;
     ga.ntile_n = ntn;
-    ga.coef = coef;
-    ga.tp = tp;
+    ga.kblocks = kx / BK;
     ga.err = ctx->d_err;
     const int grid = ((nr + BM - 1) / BM) * ntn;
     toeplitz_gemm_kernel<<<grid, 256, smem, ctx->stream>>>(mah, mal, mbh, mbl, ga);
