@@ -714,9 +714,11 @@ __global__ void __launch_bounds__(256 + 32, OCC)
   QuadCoef* coef = reinterpret_cast<QuadCoef*>(smem + R);
   uint64_t* full = reinterpret_cast<uint64_t*>(coef + E);
   uint64_t* empty = full + E;
-  int* end_pos = reinterpret_cast<int*>(empty + E);
-  volatile int* s_abort = end_pos + E;
-  float* comp = reinterpret_cast<float*>(smem + R + E * sizeof(QuadCoef) + E * 16 + E * 4 + 64);
+  // end_pos: ring byte position (64-bit: a persistent CTA allocates far more
+  // than 2^31 bytes over its items) where each entry's windows end
+  long long* end_pos = reinterpret_cast<long long*>(empty + E);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(end_pos + E);
+  float* comp = reinterpret_cast<float*>(smem + R + E * sizeof(QuadCoef) + E * 16 + E * 8 + 64);
 
   if (tid == 0) {
     *s_abort = *(volatile int*)err != 0;
@@ -734,7 +736,8 @@ __global__ void __launch_bounds__(256 + 32, OCC)
     // ---------------------------------------------------------------- producer
     // head / tail: ring bytes allocated / freed; oldest: first quad not yet
     // known to be released; seq: quads issued since the launch (all items)
-    int head = 0, tail = 0, oldest = 0, seq = 0;
+    long long head = 0, tail = 0;
+    int oldest = 0, seq = 0;
     bool more = true, first = true;
     while (more && !*s_abort) {
       // the next work item: this CTA's tile, or the queue's next item
@@ -811,8 +814,8 @@ __global__ void __launch_bounds__(256 + 32, OCC)
           const int e = q % E;
           const int qneed = __shfl_sync(0xffffffffu, need, i);
           // allocate qneed contiguous ring bytes: wrap to 0 when the tail end is too short
-          const int pos = head % R;
-          const int start = pos + qneed > R ? head + (R - pos) : head;
+          const int pos = (int)(head % R);
+          const long long start = pos + qneed > R ? head + (R - pos) : head;
           bool ok = true;
           while (oldest < q && (oldest <= q - E || start + qneed - tail > R)) {
             if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, err)) {
@@ -828,7 +831,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
             break;
           }
           if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
-          const int off = start % R;
+          const int off = (int)(start % R);
           if (lane == i) {
             qc.cbase = smem_u32(smem) + (uint32_t)off - kMagicBits * qc.rb;
             coef[e] = qc;
@@ -1580,7 +1583,7 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   bool use_quad = quad;
   if (use_quad) {
     // byte ring for the windows + entry records (+ Kahan compensations)
-    const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(int)) + 64;
+    const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(long long)) + 64;
     // Kahan compensations (interleaved layout: FP32 running sums + BF16 compensations)
     const size_t comp = !kahan ? 0 : layout == kLayoutQuadG16 ? (size_t)4 * NY * 256 * (4 + 2)
                                                               : (size_t)4 * NY * 256 * sizeof(float);

@@ -390,6 +390,31 @@ def test_batched_backprojection_equals_each_job_alone(fbp, oracle, phantoms, pre
         s.ctx.close()
 
 
+def test_batched_backprojection_long_queue(fbp, oracle, phantoms):
+    """A persistent launch whose CTAs each walk hundreds of work items (the
+    same 256^3 / 360-view job queued 60 times): each CTA's window ring
+    allocates several GB over its items, past 32-bit byte positions; the
+    volume must equal the one-job kernel's bit for bit."""
+    c = phantoms.config_cone256()
+    proj = oracle.project_ellipsoids_cone(phantoms.ellipsoids_for(c), c)
+    sod, odd, w, vw, rot = _cone_args(c)
+    g = fbp.Geometry.cone(sod, odd, w, vw, rot, c["offset"])
+    s = fbp.FBP3D(0)
+    s.set_clip_after_backprojection(False)
+    s.set_precision(fbp.Precision.MIXED)
+    s.upload_projections(proj)
+    s.apply_fdk_weights_to_projections(sod, odd, w)
+    s.apply_filter_to_projections(0)
+    s.project_backward_cone_fdk_from_projections(sod, odd, w, vw, rot, c["nx"], c["ny"], c["offset"])
+    single = s.read_volume()
+    s.upload_projections(proj)
+    s.apply_fdk_weights_to_projections(sod, odd, w)
+    s.apply_filter_to_projections(0)
+    fbp.project_backward_cone_fdk_batch([s] * 60, [g] * 60, [(c["nx"], c["ny"])] * 60)
+    assert np.array_equal(s.read_volume(), single)
+    s.ctx.close()
+
+
 @pytest.mark.parametrize("square", [True, False])
 def test_mixed24_cone(fbp, oracle, phantoms, square):
     """MIXED24 through the symmetric kernel (24-bit interleaved quads) and, for a
