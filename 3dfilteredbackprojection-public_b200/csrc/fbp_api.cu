@@ -60,6 +60,14 @@ struct DeviceGuard {
     if (rc_ != FBP_OK) return rc_; \
   } while (0)
 
+// Rows of `width` bytes between pitched buffers: one linear copy when both
+// pitches equal the width (the rows are one contiguous block), else a 2D copy.
+cudaError_t copy_rows(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows,
+                      cudaMemcpyKind kind, cudaStream_t stream) {
+  if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, stream);
+  return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, stream);
+}
+
 cudaMemcpyKind kind_of(bool src_dev, bool dst_dev) {
   if (src_dev && dst_dev) return cudaMemcpyDeviceToDevice;
   if (src_dev) return cudaMemcpyDeviceToHost;
@@ -207,7 +215,7 @@ int upload_stack(fbp_context* ctx, Stack& s, const float* src, int u, int v, int
   s.filtered = false;
   s.log_pending = s.weights_pending = false;
   FBP_TRY(fbp::cuda_check(ctx,
-                          cudaMemcpy2DAsync(s.f32, (size_t)s.pitch * 4, src, (size_t)u * 4, (size_t)u * 4,
+                          copy_rows(s.f32, (size_t)s.pitch * 4, src, (size_t)u * 4, (size_t)u * 4,
                                             s.rows(), kind_of(on_dev, true), ctx->stream),
                           "stack upload"));
   return sync_host(ctx, !on_dev);
@@ -225,12 +233,12 @@ int download_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, float* 
     if (!tmp) return FBP_ERR_OUT_OF_MEMORY;
     FBP_TRY(fbp::launch_unpack_rows(ctx, s, row0, nrows, tmp, s.pitch, (long long)row_step));
     FBP_TRY(fbp::cuda_check(ctx,
-                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, tmp, (size_t)s.pitch * 4, (size_t)s.u * 4, nrows,
+                            copy_rows(dst, (size_t)s.u * 4, tmp, (size_t)s.pitch * 4, (size_t)s.u * 4, nrows,
                                               kind_of(true, on_dev), ctx->stream),
                             "row download"));
   } else {
     FBP_TRY(fbp::cuda_check(ctx,
-                            cudaMemcpy2DAsync(dst, (size_t)s.u * 4, s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step,
+                            copy_rows(dst, (size_t)s.u * 4, s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step,
                                               (size_t)s.u * 4, nrows, kind_of(true, on_dev), ctx->stream),
                             "row download"));
   }
@@ -243,7 +251,7 @@ int upload_rows(fbp_context* ctx, Stack& s, size_t row0, size_t nrows, const flo
   if (!src) return fbp::set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "null source pointer");
   FBP_TRY(materialize_f32(ctx, s));
   FBP_TRY(fbp::cuda_check(ctx,
-                          cudaMemcpy2DAsync(s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step, src,
+                          copy_rows(s.f32 + row0 * s.pitch, (size_t)s.pitch * 4 * row_step, src,
                                             (size_t)s.u * 4, (size_t)s.u * 4, nrows, kind_of(on_dev, true),
                                             ctx->stream),
                           "row upload"));
@@ -1443,7 +1451,7 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
   s.filtered = false;
   s.log_pending = s.weights_pending = false;
   FBP_TRY(fbp::cuda_check(ctx,
-                          cudaMemcpy2DAsync(s.f32, (size_t)s.pitch * 4, projections, (size_t)cols * 4, (size_t)cols * 4,
+                          copy_rows(s.f32, (size_t)s.pitch * 4, projections, (size_t)cols * 4, (size_t)cols * 4,
                                             s.rows(), cudaMemcpyHostToDevice, ctx->stream),
                           "projection upload"));
   const bool cone = g->kind == FBP_GEOMETRY_CONE;
@@ -1501,7 +1509,7 @@ int fbp_reconstruct_fdk_to_host(fbp_context* ctx, const float* projections, int 
         (rc = fbp::cuda_check(ctx, cudaStreamWaitEvent(ctx->copy_stream, done[k], 0), "event wait")))
       break;
     rc = fbp::cuda_check(ctx,
-                         cudaMemcpy2DAsync(volume + (size_t)y0 * h, (size_t)v * h * 4, ctx->vol + (size_t)y0 * h,
+                         copy_rows(volume + (size_t)y0 * h, (size_t)v * h * 4, ctx->vol + (size_t)y0 * h,
                                            (size_t)v * h * 4, (size_t)(y1 - y0) * h * 4, h, cudaMemcpyDeviceToHost,
                                            ctx->copy_stream),
                          "slab readback");
@@ -1554,7 +1562,7 @@ static int stage_2d(fbp_context* ctx, const float* sino, int bins, int views, St
   char* base = reinterpret_cast<char*>(ctx->d_stage2d);
   st.f32 = reinterpret_cast<float*>(base + offset_bytes);
   return fbp::cuda_check(ctx,
-                         cudaMemcpy2DAsync(st.f32, (size_t)st.pitch * 4, sino, (size_t)bins * 4, (size_t)bins * 4,
+                         copy_rows(st.f32, (size_t)st.pitch * 4, sino, (size_t)bins * 4, (size_t)bins * 4,
                                            views, cudaMemcpyDeviceToDevice, ctx->stream),
                          "2D sinogram staging");
 }
@@ -1600,7 +1608,7 @@ int fbp2d_filter_sinogram(fbp_context* ctx, float* sino, int bins, int views, in
   rs.pitch = st.pitch;
   FBP_TRY(fbp::launch_filter_toeplitz(ctx, rs, n, filter_type));
   return fbp::cuda_check(ctx,
-                         cudaMemcpy2DAsync(sino, (size_t)bins * 4, st.f32, (size_t)st.pitch * 4, (size_t)bins * 4,
+                         copy_rows(sino, (size_t)bins * 4, st.f32, (size_t)st.pitch * 4, (size_t)bins * 4,
                                            views, cudaMemcpyDeviceToDevice, ctx->stream),
                          "2D filtered rows copy-back");
 }
