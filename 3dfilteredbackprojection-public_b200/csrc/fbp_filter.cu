@@ -358,13 +358,10 @@ __global__ void view_scale_kernel(const unsigned* vmax, int nviews, float limit,
 // f32 rows -> pair16: element (view, e, c) = (row e - 1, row e - row e - 1) * scale.
 __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                    const float* scale, __half2* out, long long opitch) {
-  const long long total = (long long)n_views * (n_v + 1) * m;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long er = t / m;  // element row in output order
-    const int c = (int)(t - er * m);
-    const int view = sinogram ? (int)(er % n_views) : (int)(er / (n_v + 1));
-    const int e = sinogram ? (int)(er / n_views) : (int)(er % (n_v + 1));
+  // grid: x over columns, y over element rows e, z over views
+  const int e = blockIdx.y, view = blockIdx.z;
+  const long long er = sinogram ? (long long)e * n_views + view : (long long)view * (n_v + 1) + e;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m; c += gridDim.x * blockDim.x) {
     auto row = [&](int iv) -> long long { return sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv; };
     const float lo = e >= 1 ? src[row(e - 1) * spitch + c] : 0.f;
     const float hi = e < n_v ? src[row(e) * spitch + c] : 0.f;
@@ -393,13 +390,11 @@ __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, in
 // (2.4e-4 -> 1.2e-4 relative).
 __global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                     const float* scale, uint4* out) {
+  // grid: x over element columns, y over element rows e, z over view groups g
   const int Q = n_views >> 2, P = m + 1;
-  const long long total = (long long)Q * (n_v + 1) * P;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long ge = t / P;
-    const int sc = (int)(t - ge * P);
-    const int g = (int)(ge / (n_v + 1)), e = (int)(ge - (long long)g * (n_v + 1));
+  const int e = blockIdx.y, g = blockIdx.z;
+  const long long ge = (long long)g * (n_v + 1) + e;
+  for (int sc = blockIdx.x * blockDim.x + threadIdx.x; sc < P; sc += gridDim.x * blockDim.x) {
     const int c = sc - 1;  // element column sc covers columns c, c + 1
     uint32_t w[8];
 #pragma unroll
@@ -458,13 +453,11 @@ __device__ __forceinline__ uint32_t store24(float x) {
 // 16-byte plane entries.
 __global__ void pack_quadg24_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                     uint4* out) {
+  // grid: x over element columns, y over element rows e, z over view groups g
   const int Q = n_views >> 2, P = m + 1;
-  const long long total = (long long)Q * (n_v + 1) * P;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long ge = t / P;
-    const int sc = (int)(t - ge * P);
-    const int g = (int)(ge / (n_v + 1)), e = (int)(ge - (long long)g * (n_v + 1));
+  const int e = blockIdx.y, g = blockIdx.z;
+  const long long ge = (long long)g * (n_v + 1) + e;
+  for (int sc = blockIdx.x * blockDim.x + threadIdx.x; sc < P; sc += gridDim.x * blockDim.x) {
     const int c = sc - 1;
     uint32_t w[12];
 #pragma unroll
@@ -662,23 +655,29 @@ int launch_view_scales(fbp_context* ctx, const RowSet& rs, float limit, float* v
 
 int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long long pitch, const float* view_scale) {
   if (layout == kLayoutPair16) {
-    const long long total = (long long)s.n * (s.v + 1) * s.u;
-    pack_pair16_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(
-        s.f32, s.pitch, s.u, s.n, s.v, s.sinogram, view_scale, static_cast<__half2*>(out), pitch);
+    if (s.v + 1 > 65535 || s.n > 65535)
+      return set_error(ctx, FBP_ERR_UNSUPPORTED, "the pair layout takes up to 65534 rows and 65535 views");
+    const dim3 grid((s.u + 255) / 256, s.v + 1, s.n);
+    pack_pair16_kernel<<<grid, 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram, view_scale,
+                                                      static_cast<__half2*>(out), pitch);
     return launched(ctx, "pack_pair16_kernel");
   }
   if (layout == kLayoutQuadG16) {
     if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
-    const long long total = (long long)(s.n / 4) * (s.v + 1) * (s.u + 1);
-    pack_quadg16_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
-                                                                            view_scale, static_cast<uint4*>(out));
+    if (s.v + 1 > 65535 || s.n / 4 > 65535)
+      return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout takes up to 65534 rows and 262140 views");
+    const dim3 grid((s.u + 1 + 255) / 256, s.v + 1, s.n / 4);
+    pack_quadg16_kernel<<<grid, 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram, view_scale,
+                                                       static_cast<uint4*>(out));
     return launched(ctx, "pack_quadg16_kernel");
   }
   if (layout == kLayoutQuadG24) {
     if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
-    const long long total = (long long)(s.n / 4) * (s.v + 1) * (s.u + 1);
-    pack_quadg24_kernel<<<grid_for(ctx, total, 256), 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
-                                                                            static_cast<uint4*>(out));
+    if (s.v + 1 > 65535 || s.n / 4 > 65535)
+      return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout takes up to 65534 rows and 262140 views");
+    const dim3 grid((s.u + 1 + 255) / 256, s.v + 1, s.n / 4);
+    pack_quadg24_kernel<<<grid, 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
+                                                       static_cast<uint4*>(out));
     return launched(ctx, "pack_quadg24_kernel");
   }
   return set_error(ctx, FBP_ERR_INVALID_ARGUMENT, "unknown packed layout");
