@@ -93,6 +93,7 @@ struct BPArgs {
   const uint4* qg;
   int qg_pitch, qg_rows;  // element columns per plane row, element rows per group
   int resident;           // CTAs resident on the GPU at once (view-group skew of the interleaved walk)
+  int band;               // tile orbits along z in one band of the symmetric kernel's tile order
   int* minmax;            // fold the stored values' min / max into this pair (or nullptr)
   int y_off, ny_total;    // the volume is y-slices [y_off, y_off + ny) of ny_total
   int vol_ystride;        // y-slices between z planes of the output buffer
@@ -656,6 +657,12 @@ __device__ __forceinline__ const BoxMaps& job_maps(const BoxMaps& m, const QuadQ
 // read the same views (their windows share L2) instead of all starting at view
 // 0. The offset depends only on the tile, so results are the same whichever
 // CTA, launch or batch computes it.
+//
+// Tile order within a y-slab: bands of `band` orbit rows along z, walked
+// column by column along x, so the ~`resident` tiles that run at once form a
+// near-square patch of the slab (band ~ sqrt(resident)); their windows of one
+// view group then span about half the detector columns a slab-wide row of
+// tiles would, and DRAM reads of the filtered views fall in proportion.
 struct ItemTile {
   int ix0, iy0, iz0;
   int g0, k0;
@@ -666,7 +673,11 @@ __device__ __forceinline__ ItemTile item_tile(const BPArgs& ja, long long t, int
   const long long per = (long long)nbh * nbh;
   const int by = (int)(t / per);
   const int rem = (int)(t - (long long)by * per);
-  const int bz = rem / nbh, bx = rem - bz * nbh;
+  const int H = min(max(1, ja.band), nbh);
+  const int b = rem / (H * nbh);
+  const int hb = min(H, nbh - b * H);  // orbit rows in this band (the last may be short)
+  const int r2 = rem - b * H * nbh;
+  const int bx = r2 / hb, bz = b * H + (r2 - bx * hb);
   it.ix0 = bx * 16;
   it.iz0 = bz * 16;
   it.iy0 = by * NY;
@@ -734,10 +745,11 @@ __global__ void __launch_bounds__(256 + 32, OCC)
 
   if (warp == NCW) {
     // ---------------------------------------------------------------- producer
-    // head / tail: ring bytes allocated / freed; oldest: first quad not yet
-    // known to be released; seq: quads issued since the launch (all items)
+    // head / tail: ring bytes allocated / freed; hpos = head mod R; oldest:
+    // first quad not yet known to be released; seq: quads issued since the
+    // launch (all items)
     long long head = 0, tail = 0;
-    int oldest = 0, seq = 0;
+    int hpos = 0, oldest = 0, seq = 0;
     bool more = true, first = true;
     while (more && !*s_abort) {
       // the next work item: this CTA's tile, or the queue's next item
@@ -814,8 +826,8 @@ __global__ void __launch_bounds__(256 + 32, OCC)
           const int e = q % E;
           const int qneed = __shfl_sync(0xffffffffu, need, i);
           // allocate qneed contiguous ring bytes: wrap to 0 when the tail end is too short
-          const int pos = (int)(head % R);
-          const long long start = pos + qneed > R ? head + (R - pos) : head;
+          const bool wrap = hpos + qneed > R;
+          const long long start = wrap ? head + (R - hpos) : head;
           bool ok = true;
           while (oldest < q && (oldest <= q - E || start + qneed - tail > R)) {
             if (!mbar_wait(&empty[oldest % E], (oldest / E) & 1, err)) {
@@ -831,13 +843,14 @@ __global__ void __launch_bounds__(256 + 32, OCC)
             break;
           }
           if (oldest == q) tail = start;  // nothing outstanding: the whole ring is free
-          const int off = (int)(start % R);
+          const int off = wrap ? 0 : hpos;  // start mod R
           if (lane == i) {
             qc.cbase = smem_u32(smem) + (uint32_t)off - kMagicBits * qc.rb;
             coef[e] = qc;
           }
           if (lane == 0) end_pos[e] = start + qneed;
           head = start + qneed;
+          hpos = off + qneed == R ? 0 : off + qneed;
           const int sk = __shfl_sync(0xffffffffu, (int)(skip || direct), i);
           const int cu0 = __shfl_sync(0xffffffffu, u0, i), cv0 = __shfl_sync(0xffffffffu, v0, i);
           const int cmi = __shfl_sync(0xffffffffu, mi, i), csub = __shfl_sync(0xffffffffu, sub, i);
@@ -1622,6 +1635,7 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
     if (int rc = prepare_packed(ctx, st, layout)) return rc;
   a.inv_scale = (layout == kLayoutPair16 || layout == kLayoutQuadG16) ? st.inv_scale : nullptr;  // set by the pack
   a.resident = occ * ctx->num_sms;  // CTAs resident at once (view-group skew of the symmetric kernel)
+  a.band = std::max(1, (int)std::lround(std::sqrt((double)a.resident)));
   if (is_quad_layout(layout)) {
     a.qg = static_cast<const uint4*>(st.filt);
     a.qg_pitch = st.filt_pitch;
