@@ -101,8 +101,8 @@ def workload(scale: int, name: str = "cone1440") -> dict:
 def measured_traffic(workload_name: str, form: str):
     """DRAM bytes (read + write) of one backprojector launch for this workload
     and form, read from the ncu summary committed in profiles/ (None if
-    absent). The summary holds a capture of a smaller case of the same
-    workload, scaled to a full launch by the voxel-view updates."""
+    absent). The summary holds a one-pass capture of the backprojector kernel
+    alone at the full workload size (the command is in its header)."""
     try:
         for line in (ROOT / "profiles" / "bp_dram_traffic.txt").read_text().splitlines():
             f = line.split()
