@@ -58,11 +58,12 @@ struct ViewCoef {
   int box;           // staged window: width (elements) | rows << 16
 };
 
-// Per-view window boxes: a grid of tensor maps over the same filtered stack
-// whose boxes are 1/4 .. 4/4 of the largest window in each dimension; the
-// producer stages each (tile, view) window with the smallest box that holds
-// it, so a copy moves about what the view needs.
-constexpr int kNW = 4, kNH = 4;
+// Per-view window boxes: a grid of tensor maps over the same filtered stack,
+// 8 widths x 8 heights chosen per geometry from the histogram of window sizes
+// that the footprint pass collects (the largest of each = the largest
+// window); the producer stages each (tile, view) window with the smallest box
+// that holds it, so a copy moves little more than what the view needs.
+constexpr int kNW = kBoxGrid, kNH = kBoxGrid;
 struct BoxMaps {
   CUtensorMap map[kNW * kNH];  // [width index][height index]
   int w[kNW];                  // box widths in elements of the layout
@@ -1265,9 +1266,15 @@ __global__ void __launch_bounds__(256 + 32, OCC)
 
 // Footprint pre-pass: one warp per tile (lanes over views) finds the
 // largest window any (tile, view) needs; same FP64 code as the
-// backprojector's producer, so the largest box always fits.
+// backprojector's producer, so the largest box always fits. With `hist`, it
+// also counts the windows by (width, height), clamped to kBoxHist - 1, in a
+// shared-memory histogram (kBoxHist^2 counters) added to `hist` at the end.
 template <int TX, int TZ, int NY>
-__global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
+__global__ void footprint_kernel(BPArgs a, int nty, int* spans, unsigned* hist) {
+  extern __shared__ unsigned sh_hist[];
+  if (hist)
+    for (int i = threadIdx.x; i < kBoxHist * kBoxHist; i += blockDim.x) sh_hist[i] = 0u;
+  __syncthreads();
   const long long ntiles = (long long)a.ntx * a.ntz * nty;
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -1287,6 +1294,8 @@ __global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
       tile_window(a, g, u0, v0, nu_, nv_);
       gu = max(gu, nu_);
       gv = max(gv, nv_);
+      if (hist)
+        atomicAdd(&sh_hist[min(max(nu_, 0), kBoxHist - 1) * kBoxHist + min(max(nv_, 0), kBoxHist - 1)], 1u);
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -1297,6 +1306,10 @@ __global__ void footprint_kernel(BPArgs a, int nty, int* spans) {
     atomicMax(spans, gu);
     atomicMax(spans + 1, gv);
   }
+  __syncthreads();
+  if (hist)
+    for (int i = threadIdx.x; i < kBoxHist * kBoxHist; i += blockDim.x)
+      if (sh_hist[i]) atomicAdd(&hist[i], sh_hist[i]);
 }
 
 __global__ void clip_kernel(float* vol, int nx, int ny, int nz, int ylim) {
@@ -1410,6 +1423,104 @@ cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size
 }
 
 }  // namespace
+
+// Thresholds t_0 < ... < t_{n-1} = the last candidate, taken from `cand`
+// (ascending), minimising sum_v weight[v] * (smallest t_i >= v) over the
+// values v = 0 .. weight.size() - 1 (weights of values above the last
+// candidate are ignored): dynamic program over the candidates. Fewer
+// candidates than n repeat the last threshold.
+static void best_thresholds(const std::vector<double>& weight, const std::vector<int>& cand, int n, int* out) {
+  const int C = (int)cand.size();
+  // W[j] = total weight of the values <= cand[j]
+  std::vector<double> W(C, 0.0);
+  for (int j = 0; j < C; ++j) {
+    double acc = 0.0;
+    for (int v = 0; v < (int)weight.size() && v <= cand[j]; ++v) acc += weight[v];
+    W[j] = acc;
+  }
+  const double inf = 1e300;
+  std::vector<double> dp((size_t)(n + 1) * C, inf);
+  std::vector<int> from((size_t)(n + 1) * C, -1);
+  for (int j = 0; j < C; ++j) dp[(size_t)1 * C + j] = cand[j] * W[j];
+  for (int m = 2; m <= n; ++m)
+    for (int j = 0; j < C; ++j)
+      for (int i = 0; i < j; ++i) {
+        const double c = dp[(size_t)(m - 1) * C + i] + cand[j] * (W[j] - W[i]);
+        if (c < dp[(size_t)m * C + j]) {
+          dp[(size_t)m * C + j] = c;
+          from[(size_t)m * C + j] = i;
+        }
+      }
+  // the most thresholds that the candidates allow, ending at the last one
+  int m = std::min(n, C);
+  int j = C - 1;
+  std::vector<int> t;
+  for (; m >= 1 && j >= 0; --m) {
+    t.push_back(cand[j]);
+    j = from[(size_t)m * C + j];
+  }
+  std::sort(t.begin(), t.end());
+  for (int i = 0; i < n; ++i) out[i] = t[std::min(i, (int)t.size() - 1)];
+}
+
+// The backprojector's box grid for one plan: kBoxGrid widths (multiples of
+// align, the largest = mbu) and kBoxGrid heights (the largest = mbv) that
+// minimise the staged window area summed over the footprint histogram, by
+// alternating the width and the height programs (each exact for the other
+// fixed). Windows larger than the largest box are left out (they take the
+// direct path or fail the footprint check). Without a histogram: a linear
+// grid, i/8 of the largest window in each dimension.
+static void choose_boxes(const std::vector<unsigned>& hist, int mbu, int mbv, int align, int pair_rows, int* w,
+                         int* h) {
+  const int n = kBoxGrid, B = kBoxHist;
+  for (int i = 0; i < n; ++i) {
+    const int wi = (mbu * (i + 1) + n - 1) / n;
+    w[i] = std::max(align, (wi + align - 1) / align * align);
+    h[i] = std::max(1, (mbv * (i + 1) + n - 1) / n);
+  }
+  w[n - 1] = mbu;
+  h[n - 1] = mbv;
+  if ((int)hist.size() != B * B) return;
+  // counts over (width rounded up to align, rows staged)
+  const int U = std::max(mbu, 1) + 1, V = std::max(mbv, 1) + 1;
+  std::vector<double> cnt((size_t)U * V, 0.0);
+  double total = 0.0;
+  for (int nu = 0; nu < B; ++nu)
+    for (int nv = 0; nv < B; ++nv) {
+      const unsigned c = hist[(size_t)nu * B + nv];
+      if (!c) continue;
+      const int u = std::max(align, (nu + align - 1) / align * align);
+      const int r = std::max(1, nv - pair_rows);
+      if (u > mbu || r > mbv) continue;
+      cnt[(size_t)u * V + r] += c;
+      total += c;
+    }
+  if (total <= 0.0) return;
+  std::vector<int> cu, cv;
+  for (int u = align; u <= mbu; u += align) cu.push_back(u);
+  if (cu.empty() || cu.back() != mbu) cu.push_back(mbu);
+  for (int r = 1; r <= mbv; ++r) cv.push_back(r);
+  auto pick = [](const int* t, int n, int x) {
+    for (int i = 0; i < n; ++i)
+      if (t[i] >= x) return t[i];
+    return t[n - 1];
+  };
+  for (int it = 0; it < 3; ++it) {
+    std::vector<double> wu(U, 0.0), wv(V, 0.0);
+    for (int u = 0; u < U; ++u)
+      for (int r = 0; r < V; ++r) {
+        const double c = cnt[(size_t)u * V + r];
+        if (c) wu[u] += c * pick(h, n, r);
+      }
+    best_thresholds(wu, cu, n, w);
+    for (int u = 0; u < U; ++u)
+      for (int r = 0; r < V; ++r) {
+        const double c = cnt[(size_t)u * V + r];
+        if (c) wv[r] += c * pick(w, n, u);
+      }
+    best_thresholds(wv, cv, n, h);
+  }
+}
 
 // A planned backprojection: everything a launch needs (arguments, tensor
 // maps, shared memory) after the footprint pass and the packing.
@@ -1551,30 +1662,39 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   if (!hit) {
     ctx->plan_next = (ctx->plan_next + 1) % (int)(sizeof(ctx->plans) / sizeof(ctx->plans[0]));
     plan.valid = false;
-    if (ctx->span_cap < 4) {
+    // 4 span words, then the (width, height) histogram
+    constexpr int kSpanWords = 4 + kBoxHist * kBoxHist;
+    if (ctx->span_cap < kSpanWords) {
       cudaFree(ctx->d_span);
       ctx->d_span = nullptr;
       ctx->span_cap = 0;
-      if (cuda_check(ctx, cudaMalloc(&ctx->d_span, sizeof(int) * 4), "cudaMalloc(footprint spans)"))
+      if (cuda_check(ctx, cudaMalloc(&ctx->d_span, sizeof(int) * kSpanWords), "cudaMalloc(footprint spans)"))
         return FBP_ERR_OUT_OF_MEMORY;
-      ctx->span_cap = 4;
+      ctx->span_cap = kSpanWords;
     }
-    cudaMemsetAsync(ctx->d_span, 0, 4 * sizeof(int), ctx->stream);
+    cudaMemsetAsync(ctx->d_span, 0, kSpanWords * sizeof(int), ctx->stream);
+    unsigned* d_hist = reinterpret_cast<unsigned*>(ctx->d_span + 4);
     const long long ntiles = (long long)a.ntx * a.ntz * nty;
-    const int blocks = (int)std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)ctx->num_sms * 16));
-    if (is2d)
-      footprint_kernel<16, 16, 1><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
-    else if (NY == 8)
-      footprint_kernel<16, 16, 8><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
-    else
-      footprint_kernel<16, 16, 16><<<blocks, 256, 0, ctx->stream>>>(a, nty, ctx->d_span);
+    // few blocks: each adds its whole shared histogram to the global one
+    const int blocks = (int)std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)ctx->num_sms * 2));
+    const size_t hist_smem = sizeof(unsigned) * kBoxHist * kBoxHist;
+    auto fk = is2d ? footprint_kernel<16, 16, 1> : NY == 8 ? footprint_kernel<16, 16, 8> : footprint_kernel<16, 16, 16>;
+    if (cuda_check(ctx, cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem),
+                   "footprint_kernel shared memory"))
+      return FBP_ERR_CUDA;
+    fk<<<blocks, 256, hist_smem, ctx->stream>>>(a, nty, ctx->d_span, d_hist);
     if (int rc = launched(ctx, "footprint_kernel")) return rc;
-    int hs[4] = {0, 0, 0, 0};
-    if (cuda_check(ctx, cudaMemcpyAsync(hs, ctx->d_span, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream), "spans") ||
+    std::vector<int> hs(kSpanWords);
+    if (cuda_check(ctx, cudaMemcpyAsync(hs.data(), ctx->d_span, sizeof(int) * kSpanWords, cudaMemcpyDeviceToHost,
+                                        ctx->stream),
+                   "spans") ||
         cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync"))
       return FBP_ERR_CUDA;
     plan.box_u = std::max(hs[0], 2);
     plan.box_v = std::max(hs[1], 2);
+    plan.hist.assign(reinterpret_cast<const unsigned*>(hs.data() + 4),
+                     reinterpret_cast<const unsigned*>(hs.data() + kSpanWords));
+    plan.sel_layout = -1;
     plan.valid = true;
     for (int i = 0; i < 20; ++i) plan.key[i] = key[i];
   }
@@ -1653,13 +1773,14 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   // box row) and at most the ring; larger windows are gathered directly
   const int mbu = is_quad_layout(layout) ? std::min(bu, 128) : bu;
   const int mbv = is_quad_layout(layout) ? std::min(bv, std::max(1, (int)(a.box_bytes / (esize * mbu)))) : bv;
-  for (int i = 0; i < kNW; ++i) {
-    const int w = (mbu * (i + 1) + kNW - 1) / kNW;
-    maps.w[i] = std::max(a.align, (w + a.align - 1) / a.align * a.align);
+  if (!(plan.sel_layout == layout && plan.sel_u == mbu && plan.sel_v == mbv)) {
+    choose_boxes(plan.hist, mbu, mbv, a.align, a.pair_rows, plan.sel_w, plan.sel_h);
+    plan.sel_layout = layout;
+    plan.sel_u = mbu;
+    plan.sel_v = mbv;
   }
-  for (int j = 0; j < kNH; ++j) maps.h[j] = std::max(1, (mbv * (j + 1) + kNH - 1) / kNH);
-  maps.w[kNW - 1] = mbu;
-  maps.h[kNH - 1] = mbv;
+  for (int i = 0; i < kNW; ++i) maps.w[i] = plan.sel_w[i];
+  for (int j = 0; j < kNH; ++j) maps.h[j] = plan.sel_h[j];
   for (int i = 0; i < kNW; ++i)
     for (int j = 0; j < kNH; ++j) {
       if (is_quad_layout(layout)) {  // [group][element row][plane][element column][2 x 8 bytes]

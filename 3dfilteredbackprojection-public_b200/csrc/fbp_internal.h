@@ -104,6 +104,12 @@ struct ToeplitzTables {
 
 }  // namespace fbp
 
+// Backprojector window boxes: widths and heights per plan (a grid of
+// kBoxGrid x kBoxGrid tensor maps), chosen from a histogram of the window
+// sizes whose bins cover widths and heights below kBoxHist.
+constexpr int kBoxGrid = 8;
+constexpr int kBoxHist = 128;
+
 struct fbp_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -170,6 +176,11 @@ struct fbp_context {
     bool valid = false;
     double key[20] = {0};
     int box_u = 0, box_v = 0;
+    // window (width, height) counts over the (tile, view) pairs, kBoxHist^2,
+    // and the box grid chosen from them for one layout and box limits
+    std::vector<unsigned> hist;
+    int sel_layout = -1, sel_u = 0, sel_v = 0;
+    int sel_w[kBoxGrid] = {0}, sel_h[kBoxGrid] = {0};
   } plans[16];
   int plan_next = 0;
   cudaStream_t copy_stream = nullptr;  // slab readback beside the backprojection (created on first use)
