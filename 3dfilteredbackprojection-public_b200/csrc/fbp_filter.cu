@@ -355,6 +355,8 @@ __global__ void view_scale_kernel(const unsigned* vmax, int nviews, float limit,
   inv[k] = 1.f / s;
 }
 
+constexpr int kPackRows = 8;  // element rows per block of the quad packers
+
 // f32 rows -> pair16: element (view, e, c) = (row e - 1, row e - row e - 1) * scale.
 __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                    const float* scale, __half2* out, long long opitch) {
@@ -390,37 +392,53 @@ __global__ void pack_pair16_kernel(const float* src, long long spitch, int m, in
 // (2.4e-4 -> 1.2e-4 relative).
 __global__ void pack_quadg16_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                     const float* scale, uint4* out) {
-  // grid: x over element columns, y over element rows e, z over view groups g
+  // grid: x over element columns, y over runs of kPackRows element rows (each
+  // row's samples are loaded once and carried to the next row), z over view
+  // groups g
   const int Q = n_views >> 2, P = m + 1;
-  const int e = blockIdx.y, g = blockIdx.z;
-  const long long ge = (long long)g * (n_v + 1) + e;
+  const int g = blockIdx.z, e0 = blockIdx.y * kPackRows, e1 = min(e0 + kPackRows, n_v + 1);
+  float k[4];
+#pragma unroll
+  for (int slot = 0; slot < 4; ++slot) k[slot] = scale[g + slot * Q];
   for (int sc = blockIdx.x * blockDim.x + threadIdx.x; sc < P; sc += gridDim.x * blockDim.x) {
     const int c = sc - 1;  // element column sc covers columns c, c + 1
-    uint32_t w[8];
+    // samples of row iv at columns c, c + 1 for the four slots (zero outside)
+    auto load = [&](int iv, float (&lo)[4], float (&hi)[4]) {
 #pragma unroll
-    for (int slot = 0; slot < 4; ++slot) {
-      const int view = g + slot * Q;
-      auto at = [&](int iv, int iu) -> float {
-        if (iv < 0 || iv >= n_v || iu < 0 || iu >= m) return 0.f;
+      for (int slot = 0; slot < 4; ++slot) {
+        const int view = g + slot * Q;
+        const bool ok = iv >= 0 && iv < n_v;
         const long long r = sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv;
-        return src[r * spitch + iu];
-      };
-      const float k = scale[view];
-      const float pa = at(e - 1, c), pb = at(e, c), pc = at(e - 1, c + 1), pd = at(e, c + 1);
-      const __half ha = __float2half_rn(pa * k);
-      const float ar = __half2float(ha);
-      const __half hc1 = __float2half_rn(fmaf(pc, k, -ar));
-      const __half hg0 = __float2half_rn(fmaf(pb, k, -ar));
-      const float c1 = __half2float(hc1), g0 = __half2float(hg0);
-      const __half hg1 = __float2half_rn(fmaf(pd, k, -((ar + c1) + g0)));
-      const __half2 x1 = __halves2half2(ha, hg0);   // (a_r, g0): the row e - 1 value and the row step
-      const __half2 x2 = __halves2half2(hc1, hg1);  // (c1, g1): their steps along u
-      w[2 * slot] = *reinterpret_cast<const uint32_t*>(&x1);
-      w[2 * slot + 1] = *reinterpret_cast<const uint32_t*>(&x2);
+        lo[slot] = ok && c >= 0 ? src[r * spitch + c] : 0.f;
+        hi[slot] = ok && c + 1 < m ? src[r * spitch + c + 1] : 0.f;
+      }
+    };
+    float pa[4], pc[4], pb[4], pd[4];
+    load(e0 - 1, pa, pc);
+    for (int e = e0; e < e1; ++e) {
+      load(e, pb, pd);
+      uint32_t w[8];
+#pragma unroll
+      for (int slot = 0; slot < 4; ++slot) {
+        const float kk = k[slot];
+        const __half ha = __float2half_rn(pa[slot] * kk);
+        const float ar = __half2float(ha);
+        const __half hc1 = __float2half_rn(fmaf(pc[slot], kk, -ar));
+        const __half hg0 = __float2half_rn(fmaf(pb[slot], kk, -ar));
+        const float c1 = __half2float(hc1), g0 = __half2float(hg0);
+        const __half hg1 = __float2half_rn(fmaf(pd[slot], kk, -((ar + c1) + g0)));
+        const __half2 x1 = __halves2half2(ha, hg0);   // (a_r, g0): the row e - 1 value and the row step
+        const __half2 x2 = __halves2half2(hc1, hg1);  // (c1, g1): their steps along u
+        w[2 * slot] = *reinterpret_cast<const uint32_t*>(&x1);
+        w[2 * slot + 1] = *reinterpret_cast<const uint32_t*>(&x2);
+        pa[slot] = pb[slot];
+        pc[slot] = pd[slot];
+      }
+      // two planes per element row: slots 0, 1 then slots 2, 3, 16 bytes per column each
+      const long long ge = (long long)g * (n_v + 1) + e;
+      out[(2 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
+      out[(2 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
     }
-    // two planes per element row: slots 0, 1 then slots 2, 3, 16 bytes per column each
-    out[(2 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
-    out[(2 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
   }
 }
 
@@ -453,36 +471,48 @@ __device__ __forceinline__ uint32_t store24(float x) {
 // 16-byte plane entries.
 __global__ void pack_quadg24_kernel(const float* src, long long spitch, int m, int n_views, int n_v, bool sinogram,
                                     uint4* out) {
-  // grid: x over element columns, y over element rows e, z over view groups g
+  // grid: x over element columns, y over runs of kPackRows element rows, z
+  // over view groups g (as pack_quadg16_kernel)
   const int Q = n_views >> 2, P = m + 1;
-  const int e = blockIdx.y, g = blockIdx.z;
-  const long long ge = (long long)g * (n_v + 1) + e;
+  const int g = blockIdx.z, e0 = blockIdx.y * kPackRows, e1 = min(e0 + kPackRows, n_v + 1);
   for (int sc = blockIdx.x * blockDim.x + threadIdx.x; sc < P; sc += gridDim.x * blockDim.x) {
     const int c = sc - 1;
-    uint32_t w[12];
+    auto load = [&](int iv, float (&lo)[4], float (&hi)[4]) {
 #pragma unroll
-    for (int i = 0; i < 12; ++i) w[i] = 0u;
-#pragma unroll
-    for (int slot = 0; slot < 4; ++slot) {
-      const int view = g + slot * Q;
-      auto at = [&](int iv, int iu) -> float {
-        if (iv < 0 || iv >= n_v || iu < 0 || iu >= m) return 0.f;
+      for (int slot = 0; slot < 4; ++slot) {
+        const int view = g + slot * Q;
+        const bool ok = iv >= 0 && iv < n_v;
         const long long r = sinogram ? (long long)iv * n_views + view : (long long)view * n_v + iv;
-        return src[r * spitch + iu];
-      };
-      const float pa = at(e - 1, c), pb = at(e, c), pc = at(e - 1, c + 1), pd = at(e, c + 1);
-      const float val[4] = {pa, pb - pa, pc - pa, (pd - pc) - (pb - pa)};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t s24 = store24(val[q]);
-        const int byte = 3 * (4 * slot + q), wi = byte >> 2, sh = 8 * (byte & 3);
-        w[wi] |= s24 << sh;
-        if (sh > 8) w[wi + 1] |= s24 >> (32 - sh);
+        lo[slot] = ok && c >= 0 ? src[r * spitch + c] : 0.f;
+        hi[slot] = ok && c + 1 < m ? src[r * spitch + c + 1] : 0.f;
       }
+    };
+    float pa[4], pc[4], pb[4], pd[4];
+    load(e0 - 1, pa, pc);
+    for (int e = e0; e < e1; ++e) {
+      load(e, pb, pd);
+      uint32_t w[12];
+#pragma unroll
+      for (int i = 0; i < 12; ++i) w[i] = 0u;
+#pragma unroll
+      for (int slot = 0; slot < 4; ++slot) {
+        const float val[4] = {pa[slot], pb[slot] - pa[slot], pc[slot] - pa[slot],
+                              (pd[slot] - pc[slot]) - (pb[slot] - pa[slot])};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t s24 = store24(val[q]);
+          const int byte = 3 * (4 * slot + q), wi = byte >> 2, sh = 8 * (byte & 3);
+          w[wi] |= s24 << sh;
+          if (sh > 8) w[wi + 1] |= s24 >> (32 - sh);
+        }
+        pa[slot] = pb[slot];
+        pc[slot] = pd[slot];
+      }
+      const long long ge = (long long)g * (n_v + 1) + e;
+      out[(3 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
+      out[(3 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
+      out[(3 * ge + 2) * P + sc] = make_uint4(w[8], w[9], w[10], w[11]);
     }
-    out[(3 * ge) * P + sc] = make_uint4(w[0], w[1], w[2], w[3]);
-    out[(3 * ge + 1) * P + sc] = make_uint4(w[4], w[5], w[6], w[7]);
-    out[(3 * ge + 2) * P + sc] = make_uint4(w[8], w[9], w[10], w[11]);
   }
 }
 
@@ -666,7 +696,7 @@ int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long lo
     if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
     if (s.v + 1 > 65535 || s.n / 4 > 65535)
       return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout takes up to 65534 rows and 262140 views");
-    const dim3 grid((s.u + 1 + 255) / 256, s.v + 1, s.n / 4);
+    const dim3 grid((s.u + 1 + 255) / 256, (s.v + 1 + kPackRows - 1) / kPackRows, s.n / 4);
     pack_quadg16_kernel<<<grid, 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram, view_scale,
                                                        static_cast<uint4*>(out));
     return launched(ctx, "pack_quadg16_kernel");
@@ -675,7 +705,7 @@ int launch_pack(fbp_context* ctx, const Stack& s, int layout, void* out, long lo
     if (s.n % 4) return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout needs a multiple of 4 views");
     if (s.v + 1 > 65535 || s.n / 4 > 65535)
       return set_error(ctx, FBP_ERR_UNSUPPORTED, "the interleaved layout takes up to 65534 rows and 262140 views");
-    const dim3 grid((s.u + 1 + 255) / 256, s.v + 1, s.n / 4);
+    const dim3 grid((s.u + 1 + 255) / 256, (s.v + 1 + kPackRows - 1) / kPackRows, s.n / 4);
     pack_quadg24_kernel<<<grid, 256, 0, ctx->stream>>>(s.f32, s.pitch, s.u, s.n, s.v, s.sinogram,
                                                        static_cast<uint4*>(out));
     return launched(ctx, "pack_quadg24_kernel");
