@@ -17,7 +17,9 @@
 // allocating; the budget covers the working sets of running jobs, and each
 // slot retains at most its largest job's buffers.
 //
-// Batching (on by default): a cone job's worker uploads, weights, filters and
+// Batching (on by default, for cone jobs of at most 2.4e11 voxel-view
+// updates; larger ones run their own slab pipeline, whose volume readback
+// overlaps its backprojection): a cone job's worker uploads, weights, filters and
 // plans the backprojection (packing, footprint pass) on its own
 // (high-priority) stream, then hands it to the server's engine thread, which
 // feeds the tiles of all waiting jobs to the persistent multi-job
@@ -51,6 +53,7 @@ using Clock = std::chrono::steady_clock;
 constexpr int kLookahead = 8;    // queued jobs looked at past a head that does not fit
 constexpr int kMaxBypass = 16;   // times a head may be passed over before it blocks the queue
 constexpr double kChunkUpdates = 6e10;  // voxel-view updates per batched launch (about 20 ms)
+constexpr double kBatchMaxUpdates = 2.4e11;  // larger cone jobs are not batched
 
 // A cone job's backprojection handed from its worker to the engine.
 struct BatchJob {
@@ -182,7 +185,11 @@ struct fbp_server {
     }
     const fbp_geometry& g = r.geometry;
     int rc = fbp_set_precision(c, r.precision);
-    if (r.kind == FBP_JOB_CONE && batching && launcher[0]) {
+    // a cone job of more than kBatchMaxUpdates updates runs its own slab
+    // pipeline (readback of one slab under the next slab's backprojection);
+    // batching pays for the jobs that a launch can mix
+    const double updates = (double)r.vol_h * r.vol_h * r.vol_v * (double)r.views;
+    if (r.kind == FBP_JOB_CONE && batching && launcher[0] && updates <= kBatchMaxUpdates) {
       // upload, weights and filter here; the engine backprojects; then readback
       if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
       const double tu = now_ms();
