@@ -105,12 +105,10 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
-// Shared memory of filter_fft_kernel: twiddles (n / 2 float2), the response
-// (n floats), then the rows' buffer (P x n float2) from a 16-byte boundary
-// (for n = 1 the first two parts end 4 bytes in).
-__host__ __device__ constexpr size_t fft_buf_offset(int n) {
-  return (sizeof(float2) * (n / 2) + sizeof(float) * n + 15) / 16 * 16;
-}
+// Shared memory of filter_fft_kernel: per-stage twiddle tables (n - 1
+// float2: 2^lh entries for stage lh at offset 2^lh - 1), then the rows'
+// buffer (P x n float2) from a 16-byte boundary.
+__host__ __device__ constexpr size_t fft_buf_offset(int n) { return (sizeof(float2) * n + 15) / 16 * 16; }
 __host__ __device__ constexpr size_t fft_smem_bytes(int n, int pairs) {
   return fft_buf_offset(n) + sizeof(float2) * n * pairs;
 }
@@ -127,76 +125,94 @@ struct FilterKArgs {
 // Two radix-2 stages are done per pass on four elements in registers (the
 // same operations in the same order as two separate radix-2 stages, with half
 // the shared-memory round trips and barriers).
+//
+// Bank conflicts: sample a of the buffer lives at fsw(a), its low four bits
+// XORed with 5 x bits 4-5 of a. A half-warp of 8-byte accesses is
+// conflict-free when its 16 addresses differ in the low four bits; the
+// butterflies touch blk R s + j + r s (j < s, 16 / s consecutive blocks per
+// half-warp for s < 16): for s >= 16 the 16 addresses are one aligned run
+// (the XOR permutes it), for s = 4 (R = 4) bits 2-3 become r ^ (blk & 3), for
+// s = 1 (R = 4, the middle pass) bits 0-1 become r ^ (blk >> 2 & 3); radix-2
+// passes only run at s >= n / 2. Each stage reads its own contiguous twiddle
+// table (stage lh: T[i] = exp(-2 pi i i / 2^(lh + 1)), i < 2^lh), so lanes
+// with consecutive j read consecutive twiddles.
+__device__ __forceinline__ int fsw(int a) { return a ^ (((a >> 4) & 3) * 5); }
 struct FftRows {
   float2* buf;
-  const float2* tw;  // tw[k] = exp(-2 pi i k / n), k < n / 2
+  const float2* tws;  // per-stage tables, stage lh at offset 2^lh - 1
   int n, L, P;
+  __device__ __forceinline__ const float2* T(int lh) const { return tws + ((1 << lh) - 1); }
+  __device__ __forceinline__ float2& at(int a) const { return buf[fsw(a)]; }
 };
 
 // forward DIF radix-2 stage lh (half-size h = 2^lh)
 __device__ __forceinline__ void fwd_r2(const FftRows& f, int lh) {
-  const int h = 1 << lh, half = f.n >> 1, tsh = f.L - 1 - lh;
+  const int h = 1 << lh, half = f.n >> 1;
+  const float2* T = f.T(lh);
   for (int b = threadIdx.x; b < f.P * half; b += blockDim.x) {
     const int p = b >> (f.L - 1), q = b & (half - 1);
     const int j = q & (h - 1), blk = q >> lh;
-    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
-    const float2 x0 = d[0], x1 = d[h];
-    d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
-    d[h] = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), f.tw[j << tsh]);
+    const int d = p * f.n + (blk << (lh + 1)) + j;
+    const float2 x0 = f.at(d), x1 = f.at(d + h);
+    f.at(d) = make_float2(x0.x + x1.x, x0.y + x1.y);
+    f.at(d + h) = cmul(make_float2(x0.x - x1.x, x0.y - x1.y), T[j]);
   }
 }
 
 // forward DIF stages lh and lh - 1 (lh >= 1) on blocks of 2^(lh + 1)
 __device__ __forceinline__ void fwd_r4(const FftRows& f, int lh) {
-  const int h = 1 << lh, h2 = h >> 1, quarter = f.n >> 2, tsh = f.L - 1 - lh;
+  const int h = 1 << lh, h2 = h >> 1, quarter = f.n >> 2;
+  const float2 *T = f.T(lh), *T1 = f.T(lh - 1);
   for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
     const int p = b / quarter, q = b - p * quarter;
     const int j = q & (h2 - 1), blk = q >> (lh - 1);
-    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
-    const float2 e0 = d[0], e1 = d[h2], e2 = d[h], e3 = d[h + h2];
+    const int d = p * f.n + (blk << (lh + 1)) + j;
+    const float2 e0 = f.at(d), e1 = f.at(d + h2), e2 = f.at(d + h), e3 = f.at(d + h + h2);
     const float2 t0 = make_float2(e0.x + e2.x, e0.y + e2.y);
-    const float2 t2 = cmul(make_float2(e0.x - e2.x, e0.y - e2.y), f.tw[j << tsh]);
+    const float2 t2 = cmul(make_float2(e0.x - e2.x, e0.y - e2.y), T[j]);
     const float2 t1 = make_float2(e1.x + e3.x, e1.y + e3.y);
-    const float2 t3 = cmul(make_float2(e1.x - e3.x, e1.y - e3.y), f.tw[(j + h2) << tsh]);
-    const float2 w = f.tw[j << (tsh + 1)];
-    d[0] = make_float2(t0.x + t1.x, t0.y + t1.y);
-    d[h2] = cmul(make_float2(t0.x - t1.x, t0.y - t1.y), w);
-    d[h] = make_float2(t2.x + t3.x, t2.y + t3.y);
-    d[h + h2] = cmul(make_float2(t2.x - t3.x, t2.y - t3.y), w);
+    const float2 t3 = cmul(make_float2(e1.x - e3.x, e1.y - e3.y), T[j + h2]);
+    const float2 w = T1[j];
+    f.at(d) = make_float2(t0.x + t1.x, t0.y + t1.y);
+    f.at(d + h2) = cmul(make_float2(t0.x - t1.x, t0.y - t1.y), w);
+    f.at(d + h) = make_float2(t2.x + t3.x, t2.y + t3.y);
+    f.at(d + h + h2) = cmul(make_float2(t2.x - t3.x, t2.y - t3.y), w);
   }
 }
 
 // inverse DIT radix-2 stage lh
 __device__ __forceinline__ void inv_r2(const FftRows& f, int lh) {
-  const int h = 1 << lh, half = f.n >> 1, tsh = f.L - 1 - lh;
+  const int h = 1 << lh, half = f.n >> 1;
+  const float2* T = f.T(lh);
   for (int b = threadIdx.x; b < f.P * half; b += blockDim.x) {
     const int p = b >> (f.L - 1), q = b & (half - 1);
     const int j = q & (h - 1), blk = q >> lh;
-    float2* d = f.buf + p * f.n + (blk << (lh + 1)) + j;
-    const float2 x0 = d[0];
-    const float2 x1 = cmulc(d[h], f.tw[j << tsh]);
-    d[0] = make_float2(x0.x + x1.x, x0.y + x1.y);
-    d[h] = make_float2(x0.x - x1.x, x0.y - x1.y);
+    const int d = p * f.n + (blk << (lh + 1)) + j;
+    const float2 x0 = f.at(d);
+    const float2 x1 = cmulc(f.at(d + h), T[j]);
+    f.at(d) = make_float2(x0.x + x1.x, x0.y + x1.y);
+    f.at(d + h) = make_float2(x0.x - x1.x, x0.y - x1.y);
   }
 }
 
 // inverse DIT stages lh and lh + 1 on blocks of 2^(lh + 2)
 __device__ __forceinline__ void inv_r4(const FftRows& f, int lh) {
-  const int h = 1 << lh, quarter = f.n >> 2, tsh = f.L - 1 - lh;
+  const int h = 1 << lh, quarter = f.n >> 2;
+  const float2 *T = f.T(lh), *T1 = f.T(lh + 1);
   for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
     const int p = b / quarter, q = b - p * quarter;
     const int j = q & (h - 1), blk = q >> lh;
-    float2* d = f.buf + p * f.n + (blk << (lh + 2)) + j;
-    const float2 e0 = d[0], e1 = d[h], e2 = d[2 * h], e3 = d[3 * h];
-    const float2 w = f.tw[j << tsh];
+    const int d = p * f.n + (blk << (lh + 2)) + j;
+    const float2 e0 = f.at(d), e1 = f.at(d + h), e2 = f.at(d + 2 * h), e3 = f.at(d + 3 * h);
+    const float2 w = T[j];
     const float2 x1 = cmulc(e1, w), x3 = cmulc(e3, w);
     const float2 a0 = make_float2(e0.x + x1.x, e0.y + x1.y), a1 = make_float2(e0.x - x1.x, e0.y - x1.y);
     const float2 a2 = make_float2(e2.x + x3.x, e2.y + x3.y), a3 = make_float2(e2.x - x3.x, e2.y - x3.y);
-    const float2 y = cmulc(a2, f.tw[j << (tsh - 1)]), z = cmulc(a3, f.tw[(j + h) << (tsh - 1)]);
-    d[0] = make_float2(a0.x + y.x, a0.y + y.y);
-    d[2 * h] = make_float2(a0.x - y.x, a0.y - y.y);
-    d[h] = make_float2(a1.x + z.x, a1.y + z.y);
-    d[3 * h] = make_float2(a1.x - z.x, a1.y - z.y);
+    const float2 y = cmulc(a2, T1[j]), z = cmulc(a3, T1[j + h]);
+    f.at(d) = make_float2(a0.x + y.x, a0.y + y.y);
+    f.at(d + 2 * h) = make_float2(a0.x - y.x, a0.y - y.y);
+    f.at(d + h) = make_float2(a1.x + z.x, a1.y + z.y);
+    f.at(d + 3 * h) = make_float2(a1.x - z.x, a1.y - z.y);
   }
 }
 
@@ -204,12 +220,13 @@ __device__ __forceinline__ void inv_r4(const FftRows& f, int lh) {
 // the first two inverse stages (0, 1) of each block of four, in registers.
 __device__ __forceinline__ void middle_r4(const FftRows& f, const float* hb) {
   const int quarter = f.n >> 2;
-  const float2 w1 = f.tw[1 << (f.L - 2)], w0 = f.tw[0];
+  const float2 w1 = f.T(1)[1], w0 = f.T(0)[0];
   for (int b = threadIdx.x; b < f.P * quarter; b += blockDim.x) {
     const int p = b / quarter, q = b - p * quarter;
-    float2* d = f.buf + p * f.n + 4 * q;
-    const float* hq = hb + 4 * q;
-    const float2 e0 = d[0], e1 = d[1], e2 = d[2], e3 = d[3];
+    const int d = p * f.n + 4 * q;
+    const float4 h4 = __ldg(reinterpret_cast<const float4*>(hb) + q);  // the response from global memory (L1)
+    const float hq[4] = {h4.x, h4.y, h4.z, h4.w};
+    const float2 e0 = f.at(d), e1 = f.at(d + 1), e2 = f.at(d + 2), e3 = f.at(d + 3);
     // forward stage 1 (pairs 0-2 with w0, 1-3 with w1), stage 0 (pairs 0-1, 2-3 with w0)
     const float2 t0 = make_float2(e0.x + e2.x, e0.y + e2.y);
     const float2 t2 = cmul(make_float2(e0.x - e2.x, e0.y - e2.y), w0);
@@ -228,25 +245,28 @@ __device__ __forceinline__ void middle_r4(const FftRows& f, const float* hb) {
     const float2 a0 = make_float2(s0.x + x1.x, s0.y + x1.y), a1 = make_float2(s0.x - x1.x, s0.y - x1.y);
     const float2 a2 = make_float2(s2.x + x3.x, s2.y + x3.y), a3 = make_float2(s2.x - x3.x, s2.y - x3.y);
     const float2 y = cmulc(a2, w0), z = cmulc(a3, w1);
-    d[0] = make_float2(a0.x + y.x, a0.y + y.y);
-    d[2] = make_float2(a0.x - y.x, a0.y - y.y);
-    d[1] = make_float2(a1.x + z.x, a1.y + z.y);
-    d[3] = make_float2(a1.x - z.x, a1.y - z.y);
+    f.at(d) = make_float2(a0.x + y.x, a0.y + y.y);
+    f.at(d + 2) = make_float2(a0.x - y.x, a0.y - y.y);
+    f.at(d + 1) = make_float2(a1.x + z.x, a1.y + z.y);
+    f.at(d + 3) = make_float2(a1.x - z.x, a1.y - z.y);
   }
 }
 
 // One CTA filters `pairs_per_cta` row pairs per iteration, grid-stride.
 __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n = a.n, half = n >> 1;
-  float2* tw = reinterpret_cast<float2*>(smem_raw);
-  float* hb = reinterpret_cast<float*>(tw + half);
+  const int n = a.n;
+  float2* tws = reinterpret_cast<float2*>(smem_raw);
   float2* buf = reinterpret_cast<float2*>(smem_raw + fft_buf_offset(n));
-  for (int i = threadIdx.x; i < half; i += blockDim.x) tw[i] = a.tw[i];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) hb[i] = a.hbr[i];
+  // stage lh's table from the n / 2 twiddles exp(-2 pi i k / n)
+  for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
+    const int lh = 31 - __clz(i + 1), k = i + 1 - (1 << lh);
+    tws[i] = a.tw[k << (a.log2n - 1 - lh)];
+  }
+  const float* hb = a.hbr;
   const RowSet& rs = a.rs;
   const int P = a.pairs_per_cta;
-  const FftRows f{buf, tw, n, a.log2n, P};
+  const FftRows f{buf, tws, n, a.log2n, P};
   const long long ngroups = (a.npairs + P - 1) / P;
   for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     __syncthreads();
@@ -260,7 +280,7 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
         re = load_pre(rs, r0, i);
         if (r0 + 1 < rs.rows) im = load_pre(rs, r0 + 1, i);
       }
-      buf[idx] = make_float2(re, im);
+      f.at(idx) = make_float2(re, im);
     }
     __syncthreads();
     // forward DIF (natural order in, bit-reversed out): an odd stage first,
@@ -281,8 +301,8 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
     } else {  // n <= 2: the response on its own
       for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
         const float hv = hb[idx & (n - 1)];
-        const float2 x = buf[idx];
-        buf[idx] = make_float2(x.x * hv, x.y * hv);
+        const float2 x = f.at(idx);
+        f.at(idx) = make_float2(x.x * hv, x.y * hv);
       }
       next = 0;
     }
@@ -301,7 +321,7 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterKArgs a) {
       int p = idx / n, i = idx - p * n;
       long long pr = grp * P + p;
       if (pr >= a.npairs || i >= rs.m) continue;
-      float2 y = buf[idx];
+      float2 y = f.at(idx);
       long long r0 = 2 * pr;
       store_row_sample(rs, r0, i, y.x);
       if (r0 + 1 < rs.rows) store_row_sample(rs, r0 + 1, i, y.y);
