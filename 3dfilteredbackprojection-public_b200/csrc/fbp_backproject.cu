@@ -1424,6 +1424,13 @@ cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size
 
 }  // namespace
 
+// A box width whose shared-memory row stride (planes x width sixteen-byte
+// units) is 3, 4 or 5 mod 8.
+static bool bank_friendly(int planes, int w) {
+  const int r = (planes * w) % 8;
+  return r >= 3 && r <= 5;
+}
+
 // Thresholds t_0 < ... < t_{n-1} = the last candidate, taken from `cand`
 // (ascending), minimising sum_v weight[v] * (smallest t_i >= v) over the
 // values v = 0 .. weight.size() - 1 (weights of values above the last
@@ -1471,8 +1478,8 @@ static void best_thresholds(const std::vector<double>& weight, const std::vector
 // direct path or fail the footprint check). Without a histogram: a linear
 // grid, each of the quarters 1/4 .. 4/4 of the largest window in each
 // dimension taken twice.
-static void choose_boxes(const std::vector<unsigned>& hist, int mbu, int mbv, int align, int pair_rows, int* w,
-                         int* h) {
+static void choose_boxes(const std::vector<unsigned>& hist, int mbu, int mbv, int align, int pair_rows, int planes,
+                         int* w, int* h) {
   const int n = kBoxGrid, B = kBoxHist;
   for (int i = 0; i < n; ++i) {
     const int quarter = i / 2 + 1;
@@ -1498,8 +1505,15 @@ static void choose_boxes(const std::vector<unsigned>& hist, int mbu, int mbv, in
       total += c;
     }
   if (total <= 0.0) return;
+  // widths: multiples of align; with planes > 0 (interleaved layouts, 16-byte
+  // planes) only those whose row stride is 3 to 5 mod 8 sixteen-byte units,
+  // so that the quarter-warp's two voxel rows (same detector column, next
+  // element row) fall in different bank groups (a simulation of the C4
+  // access pattern: 1.22 wavefronts per 16-byte load phase at 4 mod 8, 1.23
+  // at 3 or 5, against 1.31 at 2 or 6 and 1.44 at 0)
   std::vector<int> cu, cv;
-  for (int u = align; u <= mbu; u += align) cu.push_back(u);
+  for (int u = align; u <= mbu; u += align)
+    if (planes <= 0 || bank_friendly(planes, u)) cu.push_back(u);
   if (cu.empty() || cu.back() != mbu) cu.push_back(mbu);
   for (int r = 1; r <= mbv; ++r) cv.push_back(r);
   auto pick = [](const int* t, int n, int x) {
@@ -1773,7 +1787,16 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   BoxMaps maps;
   // interleaved layout: boxes of at most 128 x 256 elements (TMA: 256 words per
   // box row) and at most the ring; larger windows are gathered directly
-  const int mbu = is_quad_layout(layout) ? std::min(bu, 128) : bu;
+  // (the widest box of the interleaved layouts is widened, within 128, to a
+  // bank-friendly row stride, as choose_boxes picks the narrower ones)
+  const int planes = is_quad_layout(layout) ? (int)(esize / 16) : 0;
+  int mbu = is_quad_layout(layout) ? std::min(bu, 128) : bu;
+  if (planes > 0)
+    for (int wider = mbu; wider <= 128 && wider < mbu + 8; ++wider)
+      if (bank_friendly(planes, wider)) {
+        mbu = wider;
+        break;
+      }
   const int mbv = is_quad_layout(layout) ? std::min(bv, std::max(1, (int)(a.box_bytes / (esize * mbu)))) : bv;
   if (!(plan.sel_layout == layout && plan.sel_u == mbu && plan.sel_v == mbv)) {
     // the interleaved layouts take the boxes fitted to the histogram (C4: the
@@ -1782,7 +1805,7 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
     // ms at C4: their shared-memory row stride, 8 bytes x the box width, meets
     // bank conflicts at some fitted widths)
     static const std::vector<unsigned> no_hist;
-    choose_boxes(is_quad_layout(layout) ? plan.hist : no_hist, mbu, mbv, a.align, a.pair_rows, plan.sel_w,
+    choose_boxes(is_quad_layout(layout) ? plan.hist : no_hist, mbu, mbv, a.align, a.pair_rows, planes, plan.sel_w,
                  plan.sel_h);
     plan.sel_layout = layout;
     plan.sel_u = mbu;
