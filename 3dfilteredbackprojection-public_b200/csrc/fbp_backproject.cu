@@ -375,11 +375,10 @@ __device__ __forceinline__ void tap(float v, uint32_t c0, uint32_t RB, float wa,
   }
 }
 
-template <int LAYOUT, int TX, int TZ, int NY, bool KAHAN>
+template <int LAYOUT, int TX, int TZ, int NY>
 __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constant__ BoxMaps maps, const BPArgs a) {
   static_assert(TX % 8 == 0 && TZ % 4 == 0, "warp tile is 8 x 4 columns");
   constexpr int NCW = TX * TZ / 32;  // consumer warps
-  constexpr int KC = 8;              // views per Kahan fold
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -477,13 +476,12 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
   // last for the raw layout (it also reads row v + 1)
   constexpr int kRowTail = LAYOUT == kLayoutRaw32 ? 1 : 0;
 
-  float acc[NY], part[NY], comp[NY];
+  float acc[NY];
 #pragma unroll
-  for (int j = 0; j < NY; ++j) acc[j] = part[j] = comp[j] = 0.f;
+  for (int j = 0; j < NY; ++j) acc[j] = 0.f;
 
   int s = 0;
   uint32_t ph = 0;
-  int kc = 0;
   bool bad = false;
   for (int k = 0; k < a.nviews; ++k) {
     if (!mbar_wait(&full[s], ph, a.err)) {
@@ -512,7 +510,7 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
         const float wa = W - W * fu, wb = W * fu;
         const uint32_t c0 = smem_u32(smem + (size_t)s * a.box_bytes) + (uint32_t)(iu * ESZ) - kMagicBits * RB;
 #pragma unroll
-        for (int j = 0; j < NY; ++j) tap<LAYOUT>(fmaf((float)j, dvv, vl), c0, RB, wa, wb, fu, W, KAHAN ? part[j] : acc[j]);
+        for (int j = 0; j < NY; ++j) tap<LAYOUT>(fmaf((float)j, dvv, vl), c0, RB, wa, wb, fu, W, acc[j]);
       } else {
         bad = true;  // cannot happen when the footprint pass is right; recorded below
       }
@@ -523,26 +521,8 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
       s = 0;
       ph ^= 1;
     }
-    if (KAHAN && ++kc == KC) {
-      kc = 0;
-#pragma unroll
-      for (int j = 0; j < NY; ++j) {
-        const float y = part[j] - comp[j];
-        const float t = acc[j] + y;
-        comp[j] = (t - acc[j]) - y;
-        acc[j] = t;
-        part[j] = 0.f;
-      }
-    }
   }
   if (bad) atomicCAS(a.err, 0, kDevFootprint);
-  if (KAHAN) {
-#pragma unroll
-    for (int j = 0; j < NY; ++j) {
-      const float y = part[j] - comp[j];
-      acc[j] += y;
-    }
-  }
   if (*s_abort) return;
 
   const int ix = ix0 + tx, iz = iz0 + tz;
@@ -582,8 +562,6 @@ __global__ void __launch_bounds__(TX* TZ + 32, 2) bp_kernel(const __grid_constan
 // several quads in flight while the largest still fits.
 
 constexpr int kQuadEntries = 8;  // outstanding view-quads per CTA
-constexpr int kKahanQuads = 4;   // quads (16 views) per Kahan fold
-constexpr int kFoldQG = 64;      // quads per Kahan fold when the running sums live in shared memory
 
 // Quad record flags.
 constexpr int kQSkip = 1;    // the tile footprint misses the detector (or failed a check): no taps
@@ -703,7 +681,7 @@ __device__ __forceinline__ ItemTile item_tile(const BPArgs& ja, long long t, int
 // first quad and store its voxels after its last. An item's arithmetic and
 // view order do not depend on the launch, so a job's volume is the same bits
 // alone or batched with others.
-template <int LAYOUT, int NY, bool KAHAN, int OCC, bool MULTI>
+template <int LAYOUT, int NY, int OCC, bool MULTI>
 __global__ void __launch_bounds__(256 + 32, OCC)
     bp_quad_kernel(const __grid_constant__ BoxMaps maps, const __grid_constant__ BPArgs a,
                    const __grid_constant__ QuadQueue qq) {
@@ -730,7 +708,6 @@ __global__ void __launch_bounds__(256 + 32, OCC)
   // than 2^31 bytes over its items) where each entry's windows end
   long long* end_pos = reinterpret_cast<long long*>(empty + E);
   volatile int* s_abort = reinterpret_cast<volatile int*>(end_pos + E);
-  float* comp = reinterpret_cast<float*>(smem + R + E * sizeof(QuadCoef) + E * 16 + E * 8 + 64);
 
   if (tid == 0) {
     *s_abort = *(volatile int*)err != 0;
@@ -923,33 +900,16 @@ __global__ void __launch_bounds__(256 + 32, OCC)
   const int tx = QG ? (warp & 1) * 8 + ((lane >> 3) & 1) * 4 + (lane & 3) : (warp & 1) * 8 + (lane & 7);
   const int tz = QG ? (warp >> 1) * 4 + (lane >> 4) * 2 + ((lane >> 2) & 1) : (warp >> 1) * 4 + (lane >> 3);
   const float fx = (float)tx, fz = (float)tz;
-  // SMACC (interleaved layout with Kahan sums): the running sums live in
-  // shared memory beside their compensations and only the 4 x NY partial
-  // sums stay in registers, folded every kFoldQG quads.
-  constexpr bool SMACC = QG && KAHAN;
-  float* accs = comp;  // SMACC: FP32 running sums, then BF16 compensations
-  __nv_bfloat16* compb = reinterpret_cast<__nv_bfloat16*>(comp + 4 * NY * 256);
-  float acc[4][NY], part[KAHAN ? 4 : 1][KAHAN ? NY : 1];
+  // plain FP32 sums: four rotations x NY voxels in registers (a
+  // compensated sum was measured to change no digit of the MIXED form's
+  // error, which the FP16 views set, and cost 5% at C4)
+  float acc[4][NY];
   // a new work item: zero every sum of this thread
   auto reset = [&]() {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int j = 0; j < NY; ++j) acc[r][j] = 0.f;
-    if (KAHAN) {
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int j = 0; j < NY; ++j) {
-          part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
-          if (SMACC) {
-            accs[(r * NY + j) * 256 + tid] = 0.f;
-            compb[(r * NY + j) * 256 + tid] = __float2bfloat16_rn(0.f);
-          } else {
-            comp[(r * NY + j) * 256 + tid] = 0.f;
-          }
-        }
-    }
   };
   reset();
   int e = 0;
@@ -1036,8 +996,8 @@ __global__ void __launch_bounds__(256 + 32, OCC)
           auto rot_pairs = [&](const float (&A)[4], const float (&G)[4], float fv, int j) {
 #pragma unroll
             for (int pr = 0; pr < 2; ++pr) {
-              float& d0 = KAHAN ? part[KAHAN ? 2 * pr : 0][KAHAN ? j : 0] : acc[2 * pr][j];
-              float& d1 = KAHAN ? part[KAHAN ? 2 * pr + 1 : 0][KAHAN ? j : 0] : acc[2 * pr + 1][j];
+              float& d0 = acc[2 * pr][j];
+              float& d1 = acc[2 * pr + 1][j];
               const float2 t = ffma2(make_float2(fv, fv), make_float2(G[2 * pr], G[2 * pr + 1]),
                                      make_float2(A[2 * pr], A[2 * pr + 1]));
               const float2 d = ffma2(make_float2(Wr[2 * pr], Wr[2 * pr + 1]), t, make_float2(d0, d1));
@@ -1109,7 +1069,7 @@ __global__ void __launch_bounds__(256 + 32, OCC)
 #pragma unroll
             for (int r = 0; r < 4; ++r)
               tap<LAYOUT>(v, c0 + r * sub, RB, wa[r], wb[r], fu, Wr[r],
-                          KAHAN ? part[KAHAN ? r : 0][KAHAN ? j : 0] : acc[r][j]);
+                          acc[r][j]);
           }
         }
       } else {
@@ -1123,41 +1083,9 @@ __global__ void __launch_bounds__(256 + 32, OCC)
       ph ^= 1;
     }
   };
-  // fold the partial sums into the running sums (Kahan)
-  auto fold = [&]() {
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int j = 0; j < NY; ++j) {
-        const int i = (r * NY + j) * 256 + tid;
-        const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
-        const float sum = SMACC ? accs[i] : acc[r][j];
-        const float y = part[KAHAN ? r : 0][KAHAN ? j : 0] - c;
-        const float t = sum + y;
-        if (SMACC) {
-          compb[i] = __float2bfloat16_rn((t - sum) - y);  // an error term: 8 bits suffice
-          accs[i] = t;
-        } else {
-          comp[i] = (t - sum) - y;
-          acc[r][j] = t;
-        }
-        part[KAHAN ? r : 0][KAHAN ? j : 0] = 0.f;
-      }
-  };
   // the item's sums into its voxels: four rotated columns,
   // (x, z) -> (n-1-z, x) -> (n-1-x, n-1-z) -> (z, n-1-x)
   auto store = [&]() {
-    if (KAHAN) {
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int j = 0; j < NY; ++j) {
-          const int i = (r * NY + j) * 256 + tid;
-          const float sum = SMACC ? accs[i] : acc[r][j];
-          const float c = SMACC ? __bfloat162float(compb[i]) : comp[i];
-          acc[r][j] = sum + (part[KAHAN ? r : 0][KAHAN ? j : 0] - c);
-        }
-    }
     const BPArgs& ja = job_args<MULTI>(a, qq, jb);
     const ItemTile til = item_tile<QG, NY>(ja, MULTI ? item - qq.jobs[jb].item0 + qq.jobs[jb].t0 : item,
                                            MULTI ? qq.jobs[jb].nbh : a.ntx >> 1);
@@ -1186,8 +1114,6 @@ __global__ void __launch_bounds__(256 + 32, OCC)
     }
     if (ja.minmax) fold_minmax(ja.minmax, lo, hi);
   };
-  static_assert(kKahanQuads == 4 && kFoldQG % 4 == 0, "folds on whole groups of four quads");
-  int kq = 0;
   if constexpr (!MULTI) {
     // one work item, K quads (as many as views): a loop of known length
     item = (long long)blockIdx.y * gridDim.x + blockIdx.x;
@@ -1204,20 +1130,12 @@ __global__ void __launch_bounds__(256 + 32, OCC)
         if (stop) break;
         step(std::integral_constant<int, 3>{});
         if (stop) break;
-        if (KAHAN && (kq += 4) == kFoldQG) {
-          kq = 0;
-          fold();
-        }
         if (++grp == Q) grp = 0;
       }
     } else {
       for (int q = 0; q < K; ++q) {
         step(std::integral_constant<int, 0>{});
         if (stop) break;
-        if (KAHAN && ++kq == kKahanQuads) {
-          kq = 0;
-          fold();
-        }
       }
     }
     if (bad) atomicCAS(a.err, 0, kDevFootprint);
@@ -1236,19 +1154,11 @@ __global__ void __launch_bounds__(256 + 32, OCC)
       if (stop) break;
       step(std::integral_constant<int, 3>{});
       if (stop) break;
-      if (KAHAN && (kq += 4) == kFoldQG) {
-        kq = 0;
-        fold();
-      }
       const int Qj = job_args<MULTI>(a, qq, jb).nviews >> 2;
       if (++grp == Qj) grp = 0;
     } else {
       step(std::integral_constant<int, 0>{});
       if (stop || leave) break;
-      if (KAHAN && ++kq == kKahanQuads) {
-        kq = 0;
-        fold();
-      }
     }
     if (last) {
       if (bad) atomicCAS(job_args<MULTI>(a, qq, jb).err, 0, kDevFootprint);
@@ -1257,7 +1167,6 @@ __global__ void __launch_bounds__(256 + 32, OCC)
       store();
       if (!MULTI) break;
       reset();
-      kq = 0;
       last = false;
     }
   }
@@ -1356,8 +1265,8 @@ __global__ void rebin_fan_kernel(const float* fan, int bins, int views, double s
 }
 
 template <int LAYOUT, int TX, int TZ, int NY>
-cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
-  auto kern = kahan ? bp_kernel<LAYOUT, TX, TZ, NY, true> : bp_kernel<LAYOUT, TX, TZ, NY, false>;
+cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, cudaStream_t stream) {
+  auto kern = bp_kernel<LAYOUT, TX, TZ, NY>;
   // The attribute is process-wide: contexts on other threads launch this kernel
   // with other sizes, so it is always raised to the device maximum (a launch
   // still uses only its own dynamic size).
@@ -1372,10 +1281,8 @@ cudaError_t launch_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool k
 }
 
 template <int LAYOUT, int NY, int OCC>
-cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan, cudaStream_t stream) {
-  auto kern = bp_quad_kernel<LAYOUT, NY, false, OCC, false>;
-  if constexpr (LAYOUT != kLayoutQuadG24)  // the 24-bit layout runs without compensation
-    if (kahan) kern = bp_quad_kernel<LAYOUT, NY, true, OCC, false>;
+cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, cudaStream_t stream) {
+  auto kern = bp_quad_kernel<LAYOUT, NY, OCC, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   // all of L1 as shared memory, so that two CTAs of up to 113 KB share an SM
@@ -1387,38 +1294,36 @@ cudaError_t launch_quad_cfg(const BoxMaps& maps, const BPArgs& a, size_t smem, b
 }
 
 template <int NY, int OCC>
-cudaError_t launch_quad_ny(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
-                           cudaStream_t stream) {
+cudaError_t launch_quad_ny(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, cudaStream_t stream) {
   switch (layout) {
     case kLayoutPair32:
-      return launch_quad_cfg<kLayoutPair32, NY, OCC>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutPair32, NY, OCC>(maps, a, smem, stream);
     case kLayoutPair16:
-      return launch_quad_cfg<kLayoutPair16, NY, OCC>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutPair16, NY, OCC>(maps, a, smem, stream);
     case kLayoutQuadG16:
-      return launch_quad_cfg<kLayoutQuadG16, NY, OCC>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutQuadG16, NY, OCC>(maps, a, smem, stream);
     case kLayoutQuadG24:
-      return launch_quad_cfg<kLayoutQuadG24, NY, OCC>(maps, a, smem, false, stream);
+      return launch_quad_cfg<kLayoutQuadG24, NY, OCC>(maps, a, smem, stream);
     default:
-      return launch_quad_cfg<kLayoutRaw32, NY, OCC>(maps, a, smem, kahan, stream);
+      return launch_quad_cfg<kLayoutRaw32, NY, OCC>(maps, a, smem, stream);
   }
 }
 
-cudaError_t launch_quad(int layout, int ny_tile, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
+cudaError_t launch_quad(int layout, int ny_tile, const BoxMaps& maps, const BPArgs& a, size_t smem,
                         cudaStream_t stream) {
-  return ny_tile == 16 ? launch_quad_ny<16, 1>(layout, maps, a, smem, kahan, stream)
-                       : launch_quad_ny<8, 2>(layout, maps, a, smem, kahan, stream);
+  return ny_tile == 16 ? launch_quad_ny<16, 1>(layout, maps, a, smem, stream)
+                       : launch_quad_ny<8, 2>(layout, maps, a, smem, stream);
 }
 
 template <int TX, int TZ, int NY>
-cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, bool kahan,
-                          cudaStream_t stream) {
+cudaError_t launch_layout(int layout, const BoxMaps& maps, const BPArgs& a, size_t smem, cudaStream_t stream) {
   switch (layout) {
     case kLayoutPair32:
-      return launch_cfg<kLayoutPair32, TX, TZ, NY>(maps, a, smem, kahan, stream);
+      return launch_cfg<kLayoutPair32, TX, TZ, NY>(maps, a, smem, stream);
     case kLayoutPair16:
-      return launch_cfg<kLayoutPair16, TX, TZ, NY>(maps, a, smem, kahan, stream);
+      return launch_cfg<kLayoutPair16, TX, TZ, NY>(maps, a, smem, stream);
     default:
-      return launch_cfg<kLayoutRaw32, TX, TZ, NY>(maps, a, smem, kahan, stream);
+      return launch_cfg<kLayoutRaw32, TX, TZ, NY>(maps, a, smem, stream);
   }
 }
 
@@ -1545,7 +1450,7 @@ struct BPLaunchPlan {
   BoxMaps maps;
   size_t smem = 0;
   int layout = 0, ny_tile = 0, occ = 2;
-  bool use_quad = false, kahan = false, is2d = false;
+  bool use_quad = false, is2d = false;
 };
 
 BPLaunchPlan* new_bp_plan() { return new BPLaunchPlan(); }
@@ -1554,10 +1459,8 @@ void free_bp_plan(BPLaunchPlan* p) { delete p; }
 int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed,
                      BPLaunchPlan* plan_out) {
   const double pi = 3.14159265358979323846;
-  // MIXED24: 24-bit views for the symmetric kernel (FP32 rows otherwise), no
-  // compensation (FP32 sums of FP32-precise taps, as the FP32 form)
+  // MIXED24: 24-bit views for the symmetric kernel (FP32 rows otherwise)
   const bool c24 = mixed && ctx->precision == FBP_PRECISION_MIXED24;
-  const bool kahan = mixed && !c24;
   // Four-fold symmetric path: square volume, views over one turn (or
   // 4m + 1 turns) with K % 4 == 0, an even number of 16-wide tiles per axis.
   const bool is2d = g.ny == 1;
@@ -1731,12 +1634,9 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   size_t smem = 0;
   bool use_quad = quad;
   if (use_quad) {
-    // byte ring for the windows + entry records (+ Kahan compensations)
+    // byte ring for the windows + entry records
     const size_t fixed = kQuadEntries * (sizeof(QuadCoef) + 2 * sizeof(uint64_t) + sizeof(long long)) + 64;
-    // Kahan compensations (interleaved layout: FP32 running sums + BF16 compensations)
-    const size_t comp = !kahan ? 0 : layout == kLayoutQuadG16 ? (size_t)4 * NY * 256 * (4 + 2)
-                                                              : (size_t)4 * NY * 256 * sizeof(float);
-    const size_t ring = (smem_cap - fixed - comp) / 128 * 128;
+    const size_t ring = (smem_cap - fixed) / 128 * 128;
     // the interleaved layout gathers windows that do not fit from global memory
     const size_t entry = is_quad_layout(layout) ? 0 : 4 * max_box;
     if (entry > ring) {
@@ -1745,7 +1645,7 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
         return set_error(ctx, FBP_ERR_UNSUPPORTED, "detector windows too large for the symmetric backprojector");
     } else {
       a.box_bytes = (int)ring;
-      smem = ring + fixed + comp;
+      smem = ring + fixed;
     }
   }
   if (!use_quad) {
@@ -1864,7 +1764,6 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   p.ny_tile = NY;
   p.occ = occ;
   p.use_quad = use_quad;
-  p.kahan = kahan;
   p.is2d = is2d;
   return FBP_OK;
 }
@@ -1878,10 +1777,10 @@ int launch_bp_plan(fbp_context* ctx, const BPLaunchPlan& p) {
   ctx->last_bp[2] = p.a.box_u;
   ctx->last_bp[3] = p.a.box_v;
   ctx->last_bp[4] = NY;
-  cudaError_t e = p.use_quad ? launch_quad(p.layout, NY, p.maps, p.a, p.smem, p.kahan, ctx->stream)
-                  : p.is2d   ? launch_layout<16, 16, 1>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream)
-                  : NY == 8  ? launch_layout<16, 16, 8>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream)
-                             : launch_layout<16, 16, 16>(p.layout, p.maps, p.a, p.smem, p.kahan, ctx->stream);
+  cudaError_t e = p.use_quad ? launch_quad(p.layout, NY, p.maps, p.a, p.smem, ctx->stream)
+                  : p.is2d   ? launch_layout<16, 16, 1>(p.layout, p.maps, p.a, p.smem, ctx->stream)
+                  : NY == 8  ? launch_layout<16, 16, 8>(p.layout, p.maps, p.a, p.smem, ctx->stream)
+                             : launch_layout<16, 16, 16>(p.layout, p.maps, p.a, p.smem, ctx->stream);
   if (e == cudaSuccess) ctx->launches++;
   ctx->minmax_valid = e == cudaSuccess && p.a.minmax != nullptr;
   return cuda_check(ctx, e, "bp_kernel");
@@ -1895,16 +1794,14 @@ int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol,
 
 long long bp_plan_batch_key(const BPLaunchPlan& p) {
   if (!p.use_quad) return 0;  // the persistent launch runs the four-fold symmetric kernel
-  return 1 + p.layout + 16LL * p.ny_tile + 1024LL * (p.kahan ? 1 : 0) + 4096LL * p.occ + 65536LL * p.a.box_bytes;
+  return 1 + p.layout + 16LL * p.ny_tile + 4096LL * p.occ + 65536LL * p.a.box_bytes;
 }
 
 namespace {
 
 template <int LAYOUT, int NY, int OCC>
-cudaError_t launch_quad_multi_cfg(const QuadQueue& qq, size_t smem, bool kahan, int grid, cudaStream_t stream) {
-  auto kern = bp_quad_kernel<LAYOUT, NY, false, OCC, true>;
-  if constexpr (LAYOUT != kLayoutQuadG24)
-    if (kahan) kern = bp_quad_kernel<LAYOUT, NY, true, OCC, true>;
+cudaError_t launch_quad_multi_cfg(const QuadQueue& qq, size_t smem, int grid, cudaStream_t stream) {
+  auto kern = bp_quad_kernel<LAYOUT, NY, OCC, true>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
@@ -1916,15 +1813,14 @@ cudaError_t launch_quad_multi_cfg(const QuadQueue& qq, size_t smem, bool kahan, 
 }
 
 template <int NY, int OCC>
-cudaError_t launch_quad_multi_ny(int layout, const QuadQueue& qq, size_t smem, bool kahan, int grid,
-                                 cudaStream_t stream) {
+cudaError_t launch_quad_multi_ny(int layout, const QuadQueue& qq, size_t smem, int grid, cudaStream_t stream) {
   switch (layout) {
     case kLayoutPair32:
-      return launch_quad_multi_cfg<kLayoutPair32, NY, OCC>(qq, smem, kahan, grid, stream);
+      return launch_quad_multi_cfg<kLayoutPair32, NY, OCC>(qq, smem, grid, stream);
     case kLayoutQuadG16:
-      return launch_quad_multi_cfg<kLayoutQuadG16, NY, OCC>(qq, smem, kahan, grid, stream);
+      return launch_quad_multi_cfg<kLayoutQuadG16, NY, OCC>(qq, smem, grid, stream);
     case kLayoutQuadG24:
-      return launch_quad_multi_cfg<kLayoutQuadG24, NY, OCC>(qq, smem, false, grid, stream);
+      return launch_quad_multi_cfg<kLayoutQuadG24, NY, OCC>(qq, smem, grid, stream);
     default:
       return cudaErrorInvalidValue;  // other layouts run one launch per job
   }
@@ -2008,8 +1904,8 @@ int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n, const lon
   qq.err = L->d_err;
   qq.ring = p0.a.box_bytes;
   const int grid = (int)std::min<long long>(items, (long long)p0.occ * L->num_sms);
-  cudaError_t e = p0.ny_tile == 16 ? launch_quad_multi_ny<16, 1>(p0.layout, qq, p0.smem, p0.kahan, grid, L->stream)
-                                   : launch_quad_multi_ny<8, 2>(p0.layout, qq, p0.smem, p0.kahan, grid, L->stream);
+  cudaError_t e = p0.ny_tile == 16 ? launch_quad_multi_ny<16, 1>(p0.layout, qq, p0.smem, grid, L->stream)
+                                   : launch_quad_multi_ny<8, 2>(p0.layout, qq, p0.smem, grid, L->stream);
   if (e == cudaSuccess) L->launches++;
   return cuda_check(L, e, "bp_quad_kernel (batch)");
 }

@@ -261,7 +261,7 @@ struct BPGeom {
 };
 // Backproject the stack's content (filt when filtered, else f32 rows). In
 // the MIXED form (`mixed`) f32 content is first packed into the FP16 layout
-// the selected kernel reads (prepare_packed), with Kahan-compensated sums.
+// the selected kernel reads (prepare_packed); sums are FP32 in every form.
 int launch_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, int clip_ylimit, bool mixed);
 // The same in two steps: plan (footprint pass, packing, tensor maps; work on
 // ctx's stream) and launch. Plans with the same non-zero batch key can also run

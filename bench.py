@@ -10,7 +10,7 @@ A step is one reconstruction: restore the raw projections (device-to-device,
 the filter works in place), FDK weights, row filter, backprojection with the
 fused clip epilogue. `value` (Gvox*view/s = 1440*1470*1440*1440 / step time)
 is the chosen form (split-precision: FP16 filtered views with per-view scale,
-Kahan-compensated FP32 accumulation) with inputs resident in HBM; the plain
+FP32 accumulation) with inputs resident in HBM; the plain
 FP32 form is reported beside it. `e2e` repeats the chosen form through the C
 ABI with pinned host buffers: the projection upload and the volume readback
 are inside the timed region. The K reconstructions run from two host threads

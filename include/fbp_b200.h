@@ -48,8 +48,8 @@ extern "C" {
 /* ---- precision forms ------------------------------------------------------ */
 /* FP32: FP32 FFT filter, FP32 filtered views, FP32 accumulation.           */
 /* MIXED: split-BF16 tensor-core Toeplitz filter (FP32 accumulate), FP16    */
-/*        filtered views with a per-view power-of-two scale, Kahan-          */
-/*        compensated FP32 accumulation over view chunks.                    */
+/*        filtered views with a per-view power-of-two scale, FP32            */
+/*        accumulation.                                                      */
 /* MIXED24: split-BF16 Toeplitz filter, 24-bit filtered views (FP32 with   */
 /*        the low byte dropped: 16 significant bits, FP32 exponent) for the  */
 /*        four-fold symmetric backprojector (FP32 views otherwise), FP32     */

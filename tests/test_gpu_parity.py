@@ -2,7 +2,7 @@
 
 Tolerances (relative RMSE = ||x - oracle|| / ||oracle||):
   FP32 form:   1e-5 for whole reconstructions, 1e-6 for filtered rows
-  MIXED form:  1e-4 (FP16 filtered views with per-view scale, Kahan sums)
+  MIXED form:  1e-4 (FP16 filtered views with per-view scale, FP32 sums)
   MIXED24:     2e-5 (24-bit filtered views, FP32 sums)
   MIXED over five phantom seeds: 8e-5 (20% under the 1e-4 target)
 """
