@@ -199,13 +199,16 @@ __device__ void tile_geo(const BPArgs& a, int k, int ix0, int iy0, int iz0, int 
       const double x = cx ? ex : 0, z = cz ? ez : 0;
       const double D = t.Dx * x + t.Dz * z + t.D0;
       t.dmin = fmin(t.dmin, D);
-      const double u = (t.Ux * x + t.Uz * z + t.U0) / D + a.cu;
+      // one FP64 reciprocal per corner column instead of three divisions (the
+      // producer computes this for every quad, skipped ones included)
+      const double rD = 1.0 / D;
+      const double u = (t.Ux * x + t.Uz * z + t.U0) * rD + a.cu;
       t.umin = fmin(t.umin, u);
       t.umax = fmax(t.umax, u);
 #pragma unroll
       for (int cy = 0; cy < 2; ++cy) {
         const double y = cy ? ey : 0;
-        const double v = t.G * (t.Yc + a.vox * y) / D + a.cv;
+        const double v = t.G * (t.Yc + a.vox * y) * rD + a.cv;
         t.vmin = fmin(t.vmin, v);
         t.vmax = fmax(t.vmax, v);
       }
