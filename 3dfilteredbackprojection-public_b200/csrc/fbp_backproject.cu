@@ -1579,10 +1579,13 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
       break;
     }
   }
-  const bool hit = found != nullptr;
-  fbp_context::BPPlan& plan = hit ? *found : ctx->plans[ctx->plan_next];
+  // a plan made without the histogram (not a symmetric candidate then) is
+  // redone in place when the symmetric kernel may now run
+  const bool redo = found && quad && found->hist.empty();
+  const bool hit = found != nullptr && !redo;
+  fbp_context::BPPlan& plan = found ? *found : ctx->plans[ctx->plan_next];
   if (!hit) {
-    ctx->plan_next = (ctx->plan_next + 1) % (int)(sizeof(ctx->plans) / sizeof(ctx->plans[0]));
+    if (!found) ctx->plan_next = (ctx->plan_next + 1) % (int)(sizeof(ctx->plans) / sizeof(ctx->plans[0]));
     plan.valid = false;
     // 4 span words, then the (width, height) histogram
     constexpr int kSpanWords = 4 + kBoxHist * kBoxHist;
@@ -1594,8 +1597,10 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
         return FBP_ERR_OUT_OF_MEMORY;
       ctx->span_cap = kSpanWords;
     }
-    cudaMemsetAsync(ctx->d_span, 0, kSpanWords * sizeof(int), ctx->stream);
-    unsigned* d_hist = reinterpret_cast<unsigned*>(ctx->d_span + 4);
+    // the window histogram only for the symmetric kernel (its interleaved
+    // layouts fit their boxes to it); the other plans take quarter steps
+    unsigned* d_hist = quad ? reinterpret_cast<unsigned*>(ctx->d_span + 4) : nullptr;
+    cudaMemsetAsync(ctx->d_span, 0, (d_hist ? kSpanWords : 4) * sizeof(int), ctx->stream);
     const long long ntiles = (long long)a.ntx * a.ntz * nty;
     // few blocks: each adds its whole shared histogram to the global one
     const int blocks = (int)std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)ctx->num_sms * 2));
@@ -1606,16 +1611,20 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
       return FBP_ERR_CUDA;
     fk<<<blocks, 256, hist_smem, ctx->stream>>>(a, nty, ctx->d_span, d_hist);
     if (int rc = launched(ctx, "footprint_kernel")) return rc;
-    std::vector<int> hs(kSpanWords);
-    if (cuda_check(ctx, cudaMemcpyAsync(hs.data(), ctx->d_span, sizeof(int) * kSpanWords, cudaMemcpyDeviceToHost,
+    const int words = d_hist ? kSpanWords : 4;
+    std::vector<int> hs(words);
+    if (cuda_check(ctx, cudaMemcpyAsync(hs.data(), ctx->d_span, sizeof(int) * words, cudaMemcpyDeviceToHost,
                                         ctx->stream),
                    "spans") ||
         cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "footprint sync"))
       return FBP_ERR_CUDA;
     plan.box_u = std::max(hs[0], 2);
     plan.box_v = std::max(hs[1], 2);
-    plan.hist.assign(reinterpret_cast<const unsigned*>(hs.data() + 4),
-                     reinterpret_cast<const unsigned*>(hs.data() + kSpanWords));
+    if (d_hist)
+      plan.hist.assign(reinterpret_cast<const unsigned*>(hs.data() + 4),
+                       reinterpret_cast<const unsigned*>(hs.data() + kSpanWords));
+    else
+      plan.hist.clear();
     plan.sel_layout = -1;
     plan.valid = true;
     for (int i = 0; i < 20; ++i) plan.key[i] = key[i];

@@ -181,7 +181,7 @@ struct fbp_context {
     std::vector<unsigned> hist;
     int sel_layout = -1, sel_u = 0, sel_v = 0;
     int sel_w[kBoxGrid] = {0}, sel_h[kBoxGrid] = {0};
-  } plans[16];
+  } plans[64];  // geometries seen by this context (a serving worker meets dozens)
   int plan_next = 0;
   cudaStream_t copy_stream = nullptr;  // slab readback beside the backprojection (created on first use)
   // batched backprojection launched from this context (grow only)
