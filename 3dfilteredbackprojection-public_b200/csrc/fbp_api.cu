@@ -1637,6 +1637,10 @@ int fbp2d_project_backward(fbp_context* ctx, const float* sino, int bins, int vi
   g.nx = nx;
   g.ny = 1;
   g.nz = nz;
+  // the 2D kernel reads the rows where they are; a geometry whose tile windows
+  // could be very wide (source near the image) takes the general path
+  const int rc = fbp::launch_bp2d(ctx, g, sino, bins, image);
+  if (rc != FBP_ERR_UNSUPPORTED) return rc;
   Stack st;
   FBP_TRY(stage_2d(ctx, sino, bins, views, st, 0));
   return fbp::launch_backproject(ctx, g, st, image, 0, false);

@@ -1339,6 +1339,37 @@ static bool bank_friendly(int planes, int w) {
   return r >= 3 && r <= 5;
 }
 
+// Per-view (cos, sin) of theta_k = offset + span k / K in FP64, computed on
+// the device (no host staging, so a new view set needs no stream sync) and
+// kept while the view set stays the same.
+__global__ void trig_kernel(double2* trig, int n, double offset, double span) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double sn, cs;
+  sincos(offset + span * k / n, &sn, &cs);
+  trig[k] = make_double2(cs, sn);
+}
+
+int ensure_trig(fbp_context* ctx, const BPGeom& g) {
+  if (ctx->trig_cap < g.nviews) {
+    cudaFree(ctx->d_trig);
+    ctx->d_trig = nullptr;
+    ctx->trig_cap = 0;
+    ctx->trig_key[0] = -1;
+    if (cuda_check(ctx, cudaMalloc(&ctx->d_trig, sizeof(double2) * g.nviews), "cudaMalloc(trig)"))
+      return FBP_ERR_OUT_OF_MEMORY;
+    ctx->trig_cap = g.nviews;
+  }
+  if (ctx->trig_key[0] == g.nviews && ctx->trig_key[1] == g.span && ctx->trig_key[2] == g.offset) return FBP_OK;
+  trig_kernel<<<(g.nviews + 127) / 128, 128, 0, ctx->stream>>>(ctx->d_trig, g.nviews,
+                                                                g.offset, g.span);
+  if (int rc = launched(ctx, "trig_kernel")) return rc;
+  ctx->trig_key[0] = g.nviews;
+  ctx->trig_key[1] = g.span;
+  ctx->trig_key[2] = g.offset;
+  return FBP_OK;
+}
+
 // Thresholds t_0 < ... < t_{n-1} = the last candidate, taken from `cand`
 // (ascending), minimising sum_v weight[v] * (smallest t_i >= v) over the
 // values v = 0 .. weight.size() - 1 (weights of values above the last
@@ -1520,39 +1551,7 @@ int plan_backproject(fbp_context* ctx, const BPGeom& g, Stack& st, float* vol, i
   a.err = ctx->d_err;
 
   // per-view trig in FP64 (cached per view set)
-  if (ctx->trig_cap < g.nviews) {
-    cudaFree(ctx->d_trig);
-    ctx->d_trig = nullptr;
-    ctx->trig_cap = 0;
-    ctx->trig_key[0] = -1;
-    if (cuda_check(ctx, cudaMalloc(&ctx->d_trig, sizeof(double2) * g.nviews), "cudaMalloc(trig)"))
-      return FBP_ERR_OUT_OF_MEMORY;
-    ctx->trig_cap = g.nviews;
-  }
-  const bool trig_same = ctx->trig_key[0] == g.nviews && ctx->trig_key[1] == g.span && ctx->trig_key[2] == g.offset;
-  if (!trig_same) {
-    size_t need = sizeof(double2) * g.nviews;
-    if (ctx->h_pinned_bytes < need) {
-      cudaFreeHost(ctx->h_pinned);
-      ctx->h_pinned = nullptr;
-      ctx->h_pinned_bytes = 0;
-      if (cuda_check(ctx, cudaMallocHost(&ctx->h_pinned, need), "cudaMallocHost")) return FBP_ERR_OUT_OF_MEMORY;
-      ctx->h_pinned_bytes = need;
-    }
-    // the pinned buffer may still be read by an earlier copy on this stream
-    if (int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync before trig upload")) return rc;
-    double2* h = static_cast<double2*>(ctx->h_pinned);
-    for (int k = 0; k < g.nviews; ++k) {
-      double th = g.offset + g.span * k / g.nviews;
-      h[k] = make_double2(cos(th), sin(th));
-    }
-    if (int rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_trig, h, need, cudaMemcpyHostToDevice, ctx->stream),
-                            "trig upload"))
-      return rc;
-    ctx->trig_key[0] = g.nviews;
-    ctx->trig_key[1] = g.span;
-    ctx->trig_key[2] = g.offset;
-  }
+  if (int rc = ensure_trig(ctx, g)) return rc;
   a.trig = ctx->d_trig;
 
   // tile configuration: 16 x 16 columns, NY voxels along y (1 for 2D)
@@ -1920,6 +1919,184 @@ int launch_bp_batch(fbp_context* L, BPLaunchPlan* const* plans, int n, const lon
                                    : launch_quad_multi_ny<8, 2>(p0.layout, qq, p0.smem, grid, L->stream);
   if (e == cudaSuccess) L->launches++;
   return cuda_check(L, e, "bp_quad_kernel (batch)");
+}
+
+// ---------------------------------------------------------------------------
+// 2D backprojection (parallel beam and flat-detector fan beam, FBP2D.cpp:96-122
+// and FBP2D.cpp:31-52 with FBP3D's FDK weight restricted to v = 0).
+//
+// The whole filtered sinogram of a 2D job (at most a few MB) sits in L2, so the
+// 3D kernels' TMA window ring, footprint pass and per-view producer would cost
+// more than the taps. A CTA owns a 32 x 32 pixel tile; per chunk of kChunk2D
+// views one warp computes each view's tile-local projective coefficients in
+// FP64 (one view per lane, re-based to the tile origin so FP32 stays
+// accurate) and the detector window the tile needs; all threads then stage the
+// chunk's windows (zero outside the detector) in shared memory and each thread
+// accumulates four pixels of one column: per view one reciprocal of the
+// distance ratio (fan beam), one bilinear tap from shared memory, one FMA.
+constexpr int kTile2D = 32;    // pixels per tile side
+constexpr int kChunk2D = 64;   // views per staged chunk
+constexpr int kPix2D = 4;      // pixels per thread along z
+constexpr int kWin2DMax = 512; // widest staged window (samples): 64 x 512 floats = 128 KB
+
+struct BP2DArgs {
+  const float* sino;  // [views][pitch] filtered rows
+  long long pitch;
+  float* image;       // [nz][nx]
+  const double2* trig;
+  double sod, sdd, du, vox, cu;
+  int nu, nviews, nx, nz;
+  int wmax;           // staged window width (floats) of one view
+  float scale;
+  int* err;
+};
+
+template <bool CONE>
+__global__ void __launch_bounds__(256) bp2d_kernel(const BP2DArgs a) {
+  extern __shared__ __align__(16) unsigned char smem2d[];
+  float* win = reinterpret_cast<float*>(smem2d);                       // kChunk2D x wmax
+  float4* cof = reinterpret_cast<float4*>(win + kChunk2D * a.wmax);    // (Nx, Nz, N0, bu2) per view
+  float4* dco = cof + kChunk2D;                                        // (Dx, Dz, D0, u0 bits) per view
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ix0 = blockIdx.x * kTile2D, iz0 = blockIdx.y * kTile2D;
+  const int tx = lane, tz = warp * kPix2D;
+  float acc[kPix2D];
+#pragma unroll
+  for (int j = 0; j < kPix2D; ++j) acc[j] = 0.f;
+  bool bad = false;
+  const double Xc = (ix0 + 0.5 - 0.5 * a.nx) * a.vox, Zc = (iz0 + 0.5 - 0.5 * a.nz) * a.vox;
+  for (int k0 = 0; k0 < a.nviews; k0 += kChunk2D) {
+    const int nk = min(kChunk2D, a.nviews - k0);
+    __syncthreads();  // the previous chunk's windows are no longer read
+    if (warp == 0) {
+      for (int v = lane; v < nk; v += 32) {
+        const double c = a.trig[k0 + v].x, s = a.trig[k0 + v].y;
+        double Dx = 0.0, Dz = 0.0, D0 = 1.0, Ux, Uz, U0;
+        if (CONE) {
+          const double K = a.sdd / (a.sod * a.du);
+          Dx = a.vox * c / a.sod;
+          Dz = a.vox * s / a.sod;
+          D0 = (a.sod + Xc * c + Zc * s) / a.sod;
+          Ux = -a.vox * s * K;
+          Uz = a.vox * c * K;
+          U0 = (-Xc * s + Zc * c) * K;
+        } else {
+          Ux = -a.vox * s / a.du;
+          Uz = a.vox * c / a.du;
+          U0 = (-Xc * s + Zc * c) / a.du;
+        }
+        // detector window over the tile's four corners (u is monotonic along
+        // each edge, so the corners bound it)
+        double umin = 1e300, umax = -1e300, dmin = 1e300;
+        for (int cc = 0; cc < 4; ++cc) {
+          const double x = (cc & 1) ? kTile2D - 1 : 0, z = (cc & 2) ? kTile2D - 1 : 0;
+          const double D = Dx * x + Dz * z + D0;
+          dmin = fmin(dmin, D);
+          const double u = (Ux * x + Uz * z + U0) / D + a.cu;
+          umin = fmin(umin, u);
+          umax = fmax(umax, u);
+        }
+        // one sample of margin on each side for the FP32 rounding of u
+        const int u0 = (int)floor(umin) - 1;
+        const int need = (int)floor(umax) + 3 - u0;
+        if (dmin <= 1e-6 || need > a.wmax) atomicCAS(a.err, 0, kDevFootprint);
+        const double du0 = a.cu - u0;  // u - u0 = (N . (x, z, 1)) / D with N re-based
+        cof[v] = make_float4((float)(Ux + du0 * Dx), (float)(Uz + du0 * Dz), (float)(U0 + du0 * D0),
+                             __int_as_float(min(need, a.wmax) - 2));
+        dco[v] = make_float4((float)Dx, (float)Dz, (float)D0, __int_as_float(u0));
+      }
+    }
+    __syncthreads();
+    // stage the chunk's windows: row k0 + v, the samples u0 .. u0 + need - 1
+    // that its taps can read (zero outside the detector)
+    for (int i = tid; i < nk * a.wmax; i += blockDim.x) {
+      const int v = i / a.wmax, e = i - v * a.wmax;
+      if (e > __float_as_int(cof[v].w) + 1) continue;
+      const int u = __float_as_int(dco[v].w) + e;
+      win[i] = (u >= 0 && u < a.nu) ? __ldg(a.sino + (long long)(k0 + v) * a.pitch + u) : 0.f;
+    }
+    __syncthreads();
+    const float fx = (float)tx;
+    for (int v = 0; v < nk; ++v) {
+      const float4 N = cof[v], D = dco[v];
+      const int bu2 = __float_as_int(N.w);
+      const float* w = win + v * a.wmax;
+#pragma unroll
+      for (int j = 0; j < kPix2D; ++j) {
+        const float fz = (float)(tz + j);
+        const float num = fmaf(N.x, fx, fmaf(N.y, fz, N.z));
+        float u, W;
+        if (CONE) {
+          const float rD = __frcp_rn(fmaf(D.x, fx, fmaf(D.y, fz, D.z)));
+          u = num * rD;
+          W = rD * rD;
+        } else {
+          u = num;
+          W = 1.f;
+        }
+        const float fu = floorf(u);
+        const int iu = (int)fu;
+        if (iu >= 0 && iu <= bu2) {
+          const float t = u - fu, a0 = w[iu], a1 = w[iu + 1];
+          acc[j] = fmaf(W, fmaf(t, a1 - a0, a0), acc[j]);
+        } else {
+          bad = true;
+        }
+      }
+    }
+  }
+  if (bad) atomicCAS(a.err, 0, kDevFootprint);
+  const int ix = ix0 + tx;
+  if (ix < a.nx)
+#pragma unroll
+    for (int j = 0; j < kPix2D; ++j) {
+      const int iz = iz0 + tz + j;
+      if (iz < a.nz) a.image[(size_t)iz * a.nx + ix] = acc[j] * a.scale;
+    }
+}
+
+int launch_bp2d(fbp_context* ctx, const BPGeom& g, const float* sino, long long pitch, float* image) {
+  const double pi = 3.14159265358979323846;
+  const bool cone = g.kind == FBP_GEOMETRY_CONE;
+  // widest window of a tile over all views: the tile diagonal magnified at the
+  // image point nearest the source
+  const double diag = (kTile2D - 1) * std::sqrt(2.0) * g.vox;
+  double width = diag / g.du;
+  if (cone) {
+    const double r = 0.5 * std::sqrt((double)g.nx * g.nx + (double)g.nz * g.nz) * g.vox + diag;
+    const double dmin = (g.sod - r) / g.sod;
+    if (dmin < 0.05) return FBP_ERR_UNSUPPORTED;  // the source inside or near the image: general path
+    width *= g.sdd / (g.sod * dmin);
+  }
+  const int wmax = ((int)std::ceil(width) + 4 + 3) / 4 * 4;
+  if (wmax > kWin2DMax) return FBP_ERR_UNSUPPORTED;
+  if (int rc = ensure_trig(ctx, g)) return rc;
+  BP2DArgs a;
+  a.sino = sino;
+  a.pitch = pitch;
+  a.image = image;
+  a.trig = ctx->d_trig;
+  a.sod = g.sod;
+  a.sdd = g.sdd;
+  a.du = g.du;
+  a.vox = g.vox;
+  a.cu = 0.5 * g.nu - 0.5;
+  a.nu = g.nu;
+  a.nviews = g.nviews;
+  a.nx = g.nx;
+  a.nz = g.nz;
+  a.wmax = wmax;
+  a.scale = cone ? (float)(pi / g.nviews * g.sdd / (g.sod * g.du)) : (float)(pi / g.nviews / g.du);
+  a.err = ctx->d_err;
+  const size_t smem = sizeof(float) * kChunk2D * wmax + 2 * sizeof(float4) * kChunk2D;
+  auto kern = cone ? bp2d_kernel<true> : bp2d_kernel<false>;
+  if (int rc = cuda_check(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)(sizeof(float) * kChunk2D * kWin2DMax + 2 * sizeof(float4) * kChunk2D)),
+                          "bp2d_kernel shared memory"))
+    return rc;
+  const dim3 grid((g.nx + kTile2D - 1) / kTile2D, (g.nz + kTile2D - 1) / kTile2D);
+  kern<<<grid, 256, smem, ctx->stream>>>(a);
+  return launched(ctx, "bp2d_kernel");
 }
 
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit) {

@@ -286,6 +286,12 @@ int launch_bp_batch(fbp_context* launcher, BPLaunchPlan* const* plans, int n, co
 // per-view scales and pack the f32 rows into it.
 int prepare_packed(fbp_context* ctx, Stack& s, int layout);
 int launch_clip(fbp_context* ctx, float* vol, int nx, int ny, int nz, int y_limit);
+// 2D backprojection (g.ny == 1) of filtered rows [views][pitch] into image
+// [nz][nx]; FBP_ERR_UNSUPPORTED (nothing launched) when a tile's detector
+// window could exceed 512 samples (the caller takes the general path).
+int launch_bp2d(fbp_context* ctx, const BPGeom& g, const float* sino, long long pitch, float* image);
+// Per-view FP64 (cos, sin) table of g's view set in ctx->d_trig.
+int ensure_trig(fbp_context* ctx, const BPGeom& g);
 int launch_rebin_fan(fbp_context* ctx, const float* fan, int bins, int views, const BPGeom& g,
                      float* par, int out_bins, double du_out);
 
