@@ -172,25 +172,63 @@ def oracle_sample(c: dict, raw_views, nvox: int, slice_vox: int = 100_000, chunk
         del q
     clip = ijk[:, 1] < nz  # the reference's clip extent (y-slices below z_size)
     ref[clip] = np.maximum(ref[clip], 0.0)
-    return {"ijk": ijk, "ref": ref, "bands": bands, "seconds": time.perf_counter() - t0,
-            "threads": O.num_threads()}
+    return {"ijk": ijk, "ref": ref, "bands": bands, "in_fov": in_field_of_view(c, ijk),
+            "seconds": time.perf_counter() - t0, "threads": O.num_threads()}
 
 
-def sample_error(got, ref, bands=None) -> dict:
+def in_field_of_view(c: dict, ijk):
+    """True for voxels whose projection lands inside the detector's sample
+    grid in every view of a full circular orbit (so a relative error over
+    them compares reconstructed signal, not the zero fill outside the
+    detector). Closed form for a voxel at radius r from the rotation axis and
+    height Y: its detector u over the orbit peaks at SDD r / sqrt(SOD^2 - r^2)
+    (the tangent ray) and its |v| at SDD |Y| / (SOD - r) (the view with the
+    voxel nearest the source)."""
+    import numpy as np
+    ix, iy, iz = (ijk[:, i].astype(np.float64) for i in range(3))
+    X = (ix + 0.5 - c["nx"] / 2.0) * c["vox"]
+    Y = (iy + 0.5 - c["ny"] / 2.0) * c["vox"]
+    Z = (iz + 0.5 - c["nz"] / 2.0) * c["vox"]
+    r = np.hypot(X, Z)
+    sod, sdd = c["sod"], c["sdd"]
+    u_half = (c["nu"] - 1) / 2.0 * c["du"]  # outermost sample centres: no zero-fill in the bilinear tap
+    v_half = (c["nv"] - 1) / 2.0 * c["dv"]
+    ok = r < sod
+    rs = np.where(ok, r, 0.0)
+    u_max = sdd * rs / np.sqrt(np.maximum(sod * sod - rs * rs, 1e-300))
+    v_max = sdd * np.abs(Y) / np.maximum(sod - rs, 1e-300)
+    return ok & (u_max <= u_half) & (v_max <= v_half)
+
+
+def sample_error(got, ref, bands=None, in_fov=None) -> dict:
     """Relative RMSE and max abs error of `got` against the FP64 `ref`,
-    overall and (bands: name -> index range) per band."""
+    overall and (bands: name -> index range) per band. With `in_fov` (a mask
+    of the voxels the detector sees in every view) each band also reports
+    the share of its voxels in the field of view and the relative RMSE over
+    those voxels alone (None when the band has none)."""
     import numpy as np
     d = np.asarray(got, np.float64) - ref
     out = {"rel_rmse": float(np.linalg.norm(d) / np.linalg.norm(ref)), "max_abs": float(np.abs(d).max())}
+    if in_fov is not None and in_fov.any():
+        out["rel_rmse_in_fov"] = float(np.linalg.norm(d[in_fov]) / np.linalg.norm(ref[in_fov]))
     if bands:
         # per band: RMSE over the band's own reference RMS (ill-conditioned where
-        # the band holds almost no signal, e.g. slices outside the phantom) and
-        # over the whole sample's reference RMS
+        # the band holds almost no signal, e.g. slices outside the phantom or
+        # outside the detector's field of view) and over the whole sample's
+        # reference RMS
         rms_all = float(np.sqrt(np.mean(ref ** 2)))
-        out["bands"] = {k: {"rel_rmse": float(np.linalg.norm(d[a:b]) / np.linalg.norm(ref[a:b])),
-                            "rmse_over_sample_rms": float(np.sqrt(np.mean(d[a:b] ** 2)) / rms_all),
-                            "ref_rms_over_sample_rms": float(np.sqrt(np.mean(ref[a:b] ** 2)) / rms_all),
-                            "max_abs": float(np.abs(d[a:b]).max())} for k, (a, b) in bands.items()}
+        out["bands"] = {}
+        for k, (a, b) in bands.items():
+            band = {"rel_rmse": float(np.linalg.norm(d[a:b]) / np.linalg.norm(ref[a:b])),
+                    "rmse_over_sample_rms": float(np.sqrt(np.mean(d[a:b] ** 2)) / rms_all),
+                    "ref_rms_over_sample_rms": float(np.sqrt(np.mean(ref[a:b] ** 2)) / rms_all),
+                    "max_abs": float(np.abs(d[a:b]).max())}
+            if in_fov is not None:
+                m = in_fov[a:b]
+                band["in_fov_share"] = float(m.mean())
+                band["rel_rmse_in_fov"] = (float(np.linalg.norm(d[a:b][m]) / np.linalg.norm(ref[a:b][m]))
+                                           if m.any() and np.linalg.norm(ref[a:b][m]) > 0 else None)
+            out["bands"][k] = band
     return out
 
 
@@ -762,11 +800,14 @@ def main() -> None:
         ix, iy, iz = (torch.as_tensor(chk["ijk"][:, i], device=dev, dtype=torch.long) for i in range(3))
         for form, vol in vols.items():
             accuracy[f"{form}_vs_fp64_oracle"] = sample_error(vol[iz, iy, ix].double().cpu().numpy(), chk["ref"],
-                                                              chk["bands"])
+                                                              chk["bands"], chk["in_fov"])
         accuracy["oracle_sample"] = (f"{args.oracle_slice_voxels} seeded voxels in each y-slice band and "
                                      f"{args.oracle_voxels} seeded voxels uniform over the volume, each "
                                      f"backprojected in FP64 from the whole detector weighted and filtered "
-                                     f"in FP64 ({chk['seconds']:.0f} s on {chk['threads']} host threads)")
+                                     f"in FP64 ({chk['seconds']:.0f} s on {chk['threads']} host threads); "
+                                     f"rel_rmse_in_fov: over the sampled voxels that project inside the "
+                                     f"detector in every view ({float(chk['in_fov'].mean()):.2f} of the "
+                                     f"sample; none in the outermost slices, which the cone never sees whole)")
     for form in [f for f in vols if f != "plain" and "plain" in vols]:
         a, b = vols[form].double(), vols["plain"].double()
         accuracy[f"{form}_vs_plain_rel_rmse"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))

@@ -33,3 +33,39 @@ def test_oracle_sample_equals_whole_volume_fdk(oracle, phantoms):
     spans = sorted(chk["bands"].values())
     assert spans[0][0] == 0 and spans[-1][1] == len(ijk)
     assert all(spans[i][1] == spans[i + 1][0] for i in range(len(spans) - 1))
+
+
+def test_field_of_view_mask_against_every_view(phantoms):
+    """The closed-form field-of-view mask of the bench's accuracy bands: a
+    voxel it keeps projects inside the detector's sample grid in every view
+    (checked view by view), and the voxels it drops that do stay inside in
+    every listed view lie at the boundary (the closed form takes the
+    continuous orbit's extreme, which the discrete views may just miss)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    c = phantoms.scaled_cone(phantoms.config_cone1440(), 8)  # 180 x 183 x 180, 180 views, 192^2 detector
+    rng = np.random.default_rng(11)
+    n = 20000
+    ijk = np.stack([rng.integers(0, c["nx"], n), rng.integers(0, c["ny"], n), rng.integers(0, c["nz"], n)], 1)
+    mask = bench.in_field_of_view(c, ijk)
+    X = (ijk[:, 0] + 0.5 - c["nx"] / 2.0) * c["vox"]
+    Y = (ijk[:, 1] + 0.5 - c["ny"] / 2.0) * c["vox"]
+    Z = (ijk[:, 2] + 0.5 - c["nz"] / 2.0) * c["vox"]
+    th = c["offset"] + c["span"] * np.arange(c["nviews"]) / c["nviews"]
+    t = X[:, None] * np.cos(th) + Z[:, None] * np.sin(th)
+    s = -X[:, None] * np.sin(th) + Z[:, None] * np.cos(th)
+    L = c["sod"] + t
+    ui = c["sdd"] * s / L / c["du"] + c["nu"] / 2.0 - 0.5
+    vi = c["sdd"] * Y[:, None] / L / c["dv"] + c["nv"] / 2.0 - 0.5
+    inside = ((L > 0) & (ui >= 0) & (ui <= c["nu"] - 1) & (vi >= 0) & (vi <= c["nv"] - 1)).all(axis=1)
+    assert 0.05 < mask.mean() < 0.95
+    assert not (mask & ~inside).any()
+    # dropped although every discrete view is inside: within 2% of the limits
+    near = inside & ~mask
+    r = np.hypot(X, Z)[near]
+    u_max = c["sdd"] * r / np.sqrt(c["sod"] ** 2 - r ** 2)
+    v_max = c["sdd"] * np.abs(Y[near]) / (c["sod"] - r)
+    lim_u, lim_v = (c["nu"] - 1) / 2.0 * c["du"], (c["nv"] - 1) / 2.0 * c["dv"]
+    assert np.all((u_max <= 1.02 * lim_u) & (v_max <= 1.02 * lim_v))
+    assert near.mean() < 0.02
