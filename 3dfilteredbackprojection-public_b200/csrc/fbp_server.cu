@@ -17,9 +17,9 @@
 // allocating; the budget covers the working sets of running jobs, and each
 // slot retains at most its largest job's buffers.
 //
-// Batching (on by default, for cone jobs of at most 2.4e11 voxel-view
-// updates; larger ones run their own slab pipeline, whose volume readback
-// overlaps its backprojection): a cone job's worker uploads, weights, filters and
+// Batching (on by default, for cone jobs of at most 1e10 voxel-view updates,
+// fbp_server_set_batch_limit; larger ones run their own slab pipeline, whose
+// volume readback overlaps its backprojection): a cone job's worker uploads, weights, filters and
 // plans the backprojection (packing, footprint pass) on its own
 // (high-priority) stream, then hands it to the server's engine thread, which
 // feeds the tiles of all waiting jobs to the persistent multi-job
@@ -53,7 +53,15 @@ using Clock = std::chrono::steady_clock;
 constexpr int kLookahead = 8;    // queued jobs looked at past a head that does not fit
 constexpr int kMaxBypass = 16;   // times a head may be passed over before it blocks the queue
 constexpr double kChunkUpdates = 6e10;  // voxel-view updates per batched launch (about 20 ms)
-constexpr double kBatchMaxUpdates = 2.4e11;  // larger cone jobs are not batched
+// Larger cone jobs are not batched. A job of more than ~1e10 updates fills
+// the GPU with its own grid, and jobs on the slots' own streams already share
+// the SMs as their CTAs retire; through the engine, such jobs lost more to
+// its chunked launches (at most two in flight) than they gained. On the
+// serving mix (2000 jobs, 5 slots, one B200) the jobs other than the 768^3
+// ones took 16.1 s with a 2.4e11 limit, 13.1 s with 1e10 and 12.8 s with no
+// batching; the whole stream 106.0, 104.5 and 103.7 s (bound by the 768^3
+// jobs' backprojections).
+constexpr double kBatchMaxUpdates = 1e10;
 
 // A cone job's backprojection handed from its worker to the engine.
 struct BatchJob {
@@ -128,6 +136,7 @@ struct fbp_server {
   size_t budget = 0;
   bool batching = true;
   double chunk_updates = kChunkUpdates;  // voxel-view updates per batched launch
+  double batch_max = kBatchMaxUpdates;    // larger cone jobs run their own slab pipelines
   // engine: the persistent multi-job backprojector's feeder
   std::thread engine;
   fbp_context* launcher[2] = {nullptr, nullptr};
@@ -185,11 +194,16 @@ struct fbp_server {
     }
     const fbp_geometry& g = r.geometry;
     int rc = fbp_set_precision(c, r.precision);
-    // a cone job of more than kBatchMaxUpdates updates runs its own slab
+    // a cone job of more than batch_max updates runs its own slab
     // pipeline (readback of one slab under the next slab's backprojection);
     // batching pays for the jobs that a launch can mix
     const double updates = (double)r.vol_h * r.vol_h * r.vol_v * (double)r.views;
-    if (r.kind == FBP_JOB_CONE && batching && launcher[0] && updates <= kBatchMaxUpdates) {
+    bool batch;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      batch = batching && updates <= batch_max;
+    }
+    if (r.kind == FBP_JOB_CONE && batch && launcher[0]) {
       // upload, weights and filter here; the engine backprojects; then readback
       if (!rc) rc = fbp_set_clip_after_backprojection(c, r.clip);
       const double tu = now_ms();
@@ -483,6 +497,13 @@ int fbp_server_set_batching(fbp_server* s, int enable, double chunk_updates) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->batching = enable != 0;
   s->chunk_updates = chunk_updates > 0 ? chunk_updates : kChunkUpdates;
+  return FBP_OK;
+}
+
+int fbp_server_set_batch_limit(fbp_server* s, double max_updates) {
+  if (!s) return FBP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->batch_max = max_updates > 0 ? max_updates : kBatchMaxUpdates;
   return FBP_OK;
 }
 

@@ -171,6 +171,7 @@ SIGNATURES = {
     "fbp_server_create": [C.POINTER(C.c_void_p), _I, C.c_size_t, _I],
     "fbp_server_submit": [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)],
     "fbp_server_set_batching": [C.c_void_p, _I, C.c_double],
+    "fbp_server_set_batch_limit": [C.c_void_p, C.c_double],
     "fbp_server_stats": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                          C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "fbp_server_wait": [C.c_void_p, C.c_longlong, C.c_void_p],
@@ -230,6 +231,13 @@ class Server:
         rc = self.lib.fbp_server_set_batching(self.handle, 1 if enable else 0, float(chunk_updates))
         if rc != 0:
             raise FBPError(rc, "fbp_server_set_batching failed")
+
+    def set_batch_limit(self, max_updates: float) -> None:
+        """Cone jobs of at most max_updates voxel-view updates are batched
+        (<= 0: 1e10); larger ones run their own slab pipelines."""
+        rc = self.lib.fbp_server_set_batch_limit(self.handle, float(max_updates))
+        if rc != 0:
+            raise FBPError(rc, "fbp_server_set_batch_limit failed")
 
     def stats(self) -> dict:
         """fbp_server_stats: batched backprojection device time, upload / readback host time."""

@@ -554,7 +554,7 @@ def serving_block(args, n_requests: int, n_poisson: int) -> dict:
         "metric": "mixed-stream reconstructions/s", "value": chosen_cap["recon_per_s"], "unit": "recon/s",
         "config": {"workload": "serving_mixed_stream", "requests": len(reqs), "mix": mix, "slots": args.slots,
                    "poisson_requests": npo, "arrival_rate_per_s": rate, "load_vs_plain_capacity": args.load,
-                   "batching": "cone jobs of up to 2.4e11 voxel-view updates through the persistent multi-job "
+                   "batching": "cone jobs of up to 1e10 voxel-view updates through the persistent multi-job "
                                "backprojector, larger ones (768^3) through their own slab pipelines"},
         "chosen": {"capacity": chosen_cap, "poisson": chosen_lat},
         "plain_one_at_a_time_fp32": {"capacity": plain_cap, "poisson": plain_lat},

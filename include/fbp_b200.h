@@ -293,10 +293,17 @@ int fbp_server_create(fbp_server** server, int device, size_t hbm_budget_bytes, 
  * engine into the persistent multi-job backprojector (as in
  * fbp_project_backward_cone_fdk_batch), their tiles launched in chunks of
  * about chunk_updates voxel-view updates (<= 0: 6e10, about 20 ms) mixed
- * with the other waiting jobs' tiles; a cone job of more than 2.4e11
+ * with the other waiting jobs' tiles; a cone job of more than 1e10
  * updates runs its own slab pipeline instead (volume readback under the
  * backprojection); 0: each job launches its own kernels. */
 int fbp_server_set_batching(fbp_server* server, int enable, double chunk_updates);
+/* With batching on, the cone jobs of at most max_updates voxel-view updates
+ * go through the engine (<= 0: 1e10); larger ones run their own slab
+ * pipelines. Independent jobs on their own streams already share the SMs
+ * when their grids are small; the engine pays for jobs too small to fill
+ * the GPU alone. No counterpart in the reference (one reconstruction per
+ * GL context). */
+int fbp_server_set_batch_limit(fbp_server* server, double max_updates);
 /* Since the server was created: device time of the batched backprojection
  * launches (each launch timed on its stream, summed), host time the cone
  * jobs of the batching path spent in their uploads and volume readbacks

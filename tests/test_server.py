@@ -82,3 +82,15 @@ def test_close_runs_queued_jobs(fbp):
     for _ in range(5):
         s.submit(_job(fbp, 10, 2000))
     s.close()  # returns after the queued jobs ran
+
+
+def test_batching_settings_on_a_host_only_server(fbp):
+    """The batching switches are accepted on a server without a device (they
+    only steer cone jobs) and host-only jobs still run."""
+    s = _server(fbp, 1000, 2)
+    s.set_batching(True, 3e10)
+    s.set_batch_limit(1e10)
+    s.set_batch_limit(0.0)  # back to the default limit
+    r = s.wait(s.submit(_job(fbp, 10, 1000)))
+    s.close()
+    assert r.status == 0
