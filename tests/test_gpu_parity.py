@@ -1006,7 +1006,9 @@ def test_server_batched_chunks_equal_unbatched_jobs(fbp):
     s = fbp.Server(0, 0, 4)
     s.set_batching(True, chunk_updates=3e6)
     res = [s.wait(t) for t in [s.submit(r) for r in reqs]]
+    st = s.stats()
     s.close()
+    assert st["batched_jobs"] > 0 and st["batch_launches"] > st["batched_jobs"]  # cone jobs went through the engine
     assert all(r.status == 0 for r in res), [r.error for r in res]
     for a, m in zip(alone, mix):
         np.testing.assert_array_equal(a, m)
