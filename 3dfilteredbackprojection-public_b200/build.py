@@ -4,11 +4,14 @@
 
 Every .cu file under csrc/ is compiled with nvcc for sm_100a only and linked
 into libfbp_b200.so next to this file. Rebuilds only when a source or header
-is newer than the library (or with --force).
+is newer than the library (or with --force). Concurrent callers (one per
+rank under torchrun) serialise on a lock file: the first rebuilds, the others
+find the library current once they hold the lock.
 """
 from __future__ import annotations
 
 import concurrent.futures as cf
+import fcntl
 import os
 import subprocess
 import sys
@@ -55,6 +58,17 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
     BUILD.mkdir(exist_ok=True)
+    with open(BUILD / ".lock", "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            if not force and not _stale():  # another process rebuilt it meanwhile
+                return LIB
+            return _build_locked(verbose)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
+
+
+def _build_locked(verbose: bool) -> Path:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources()))
     tmp = LIB.with_suffix(".so.tmp")
