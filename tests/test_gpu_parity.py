@@ -1014,6 +1014,32 @@ def test_server_batched_chunks_equal_unbatched_jobs(fbp):
         np.testing.assert_array_equal(a, m)
 
 
+def test_server_batch_limit_routes_jobs_and_keeps_their_bits(fbp):
+    """With a batch limit below every cone job's update count no job goes
+    through the engine (each runs its own pipeline on its slot's stream); with
+    the default limit the small test jobs are batched. Outputs are the same
+    bits either way."""
+    rng = np.random.default_rng(63)
+    reqs, keep, first = _server_jobs(fbp, rng)
+    outs = {}
+    for name, limit in [("none batched", 1.0), ("default", 0.0)]:
+        outs[name] = [np.empty_like(o) for o in first]
+        for r, o in zip(reqs, outs[name]):
+            r.output = o.ctypes.data
+        s = fbp.Server(0, 0, 3)
+        s.set_batch_limit(limit)
+        res = [s.wait(t) for t in [s.submit(r) for r in reqs]]
+        st = s.stats()
+        s.close()
+        assert all(r.status == 0 for r in res), [r.error for r in res]
+        if name == "none batched":
+            assert st["batched_jobs"] == 0 and st["batch_launches"] == 0
+        else:
+            assert st["batched_jobs"] > 0
+    for a, b in zip(outs["none batched"], outs["default"]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_server_cone_job_matches_oracle_and_bad_jobs_fail_alone(fbp, oracle, phantoms):
     c, proj = _cone_case(phantoms, oracle, 4)
     sod, odd, w, vw, rot = _cone_args(c)
