@@ -73,6 +73,11 @@ struct BatchJob {
   double per_tile = 0;    // voxel-view updates of one tile
   bool planned = false;
   bool launched = false;  // every tile launched; the job's stream waits for them
+  // set under the server's mutex when the engine hands the job back (all tiles
+  // launched, or failed): the worker waits on this flag alone, so the engine's
+  // earlier writes of status and error are visible to it and the engine no
+  // longer touches the job (it lives on the worker's stack)
+  bool returned = false;
   int status = FBP_OK;
   std::string error;
 };
@@ -84,6 +89,7 @@ struct Job {
   int bypassed = 0;  // later jobs started while this one headed the queue
   int status = FBP_OK;
   bool done = false;
+  bool claimed = false;  // a caller waits on this ticket (it is consumed by the wait)
   double queued = 0, started = 0, finished = 0;  // ms since the server started
   std::string error;
 };
@@ -228,7 +234,7 @@ struct fbp_server {
           std::unique_lock<std::mutex> lk(mu);
           incoming.push_back(&bj);
           engine_cv.notify_all();
-          batch_cv.wait(lk, [&] { return bj.launched || bj.status != FBP_OK; });
+          batch_cv.wait(lk, [&] { return bj.returned; });
         }
         rc = bj.status;
         if (rc) j.error = bj.error;
@@ -388,6 +394,7 @@ struct fbp_server {
         BatchJob* b = *it;
         if (b->status != FBP_OK || (b->planned && b->next >= b->tiles)) {
           b->launched = b->status == FBP_OK;
+          b->returned = true;
           it = active.erase(it);
           any = true;
         } else {
@@ -546,6 +553,8 @@ int fbp_server_wait(fbp_server* s, long long ticket, fbp_job_result* result) {
   auto it = s->jobs.find(ticket);
   if (it == s->jobs.end()) return FBP_ERR_INVALID_ARGUMENT;
   Job* j = it->second;
+  if (j->claimed) return FBP_ERR_STATE;  // another caller is waiting on this ticket
+  j->claimed = true;
   s->done_cv.wait(lk, [&] { return j->done; });
   if (result) {
     result->status = j->status;

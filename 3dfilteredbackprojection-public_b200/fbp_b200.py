@@ -260,6 +260,8 @@ class Server:
     def wait(self, ticket: int) -> JobResult:
         r = JobResult()
         rc = self.lib.fbp_server_wait(self.handle, int(ticket), C.byref(r))
+        if rc == -2:  # FBP_ERR_STATE: the job still runs for the caller already waiting on it
+            raise FBPError(rc, "fbp_server_wait: another caller is waiting on this ticket")
         self._keep.pop(ticket, None)
         if rc != 0:
             raise FBPError(rc, "fbp_server_wait: unknown ticket")

@@ -312,6 +312,9 @@ int fbp_server_set_batch_limit(fbp_server* server, double max_updates);
 int fbp_server_stats(fbp_server* server, double* batch_gpu_ms, double* upload_ms, double* readback_ms,
                      long long* batch_launches, long long* batched_jobs);
 int fbp_server_submit(fbp_server* server, const fbp_request* request, long long* ticket);
+/* Blocks until the job ends; the ticket is consumed. A second caller waiting
+ * on a ticket that another caller already waits on gets FBP_ERR_STATE; an
+ * unknown (or consumed) ticket gives FBP_ERR_INVALID_ARGUMENT. */
 int fbp_server_wait(fbp_server* server, long long ticket, fbp_job_result* result);
 int fbp_server_destroy(fbp_server* server); /* runs the queued jobs, then stops */
 

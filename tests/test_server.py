@@ -94,3 +94,27 @@ def test_batching_settings_on_a_host_only_server(fbp):
     r = s.wait(s.submit(_job(fbp, 10, 1000)))
     s.close()
     assert r.status == 0
+
+
+def test_a_ticket_has_one_waiter(fbp):
+    """A ticket is consumed by its wait: a second caller waiting on a ticket
+    that another caller already waits on gets a state error (the job keeps
+    running for the first), and a consumed ticket is unknown afterwards."""
+    import threading
+    import time
+
+    s = _server(fbp, 1000, 1)
+    t = s.submit(_job(fbp, 10, 400000))  # holds the slot for 0.4 s
+    got = {}
+    first = threading.Thread(target=lambda: got.setdefault("r", s.wait(t)))
+    first.start()
+    time.sleep(0.1)
+    with pytest.raises(fbp.FBPError) as e:
+        s.wait(t)
+    assert e.value.status == -2
+    first.join()
+    assert got["r"].status == 0
+    with pytest.raises(fbp.FBPError) as e:
+        s.wait(t)
+    assert e.value.status == -1
+    s.close()
