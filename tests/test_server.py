@@ -104,11 +104,11 @@ def test_a_ticket_has_one_waiter(fbp):
     import time
 
     s = _server(fbp, 1000, 1)
-    t = s.submit(_job(fbp, 10, 400000))  # holds the slot for 0.4 s
+    t = s.submit(_job(fbp, 10, 3000000))  # holds the slot for 3 s
     got = {}
     first = threading.Thread(target=lambda: got.setdefault("r", s.wait(t)))
     first.start()
-    time.sleep(0.1)
+    time.sleep(0.5)  # the first caller is waiting well before the job ends
     with pytest.raises(fbp.FBPError) as e:
         s.wait(t)
     assert e.value.status == -2
