@@ -69,3 +69,27 @@ def test_field_of_view_mask_against_every_view(phantoms):
     lim_u, lim_v = (c["nu"] - 1) / 2.0 * c["du"], (c["nv"] - 1) / 2.0 * c["dv"]
     assert np.all((u_max <= 1.02 * lim_u) & (v_max <= 1.02 * lim_v))
     assert near.mean() < 0.02
+
+
+def test_sample_error_reports_bands_over_the_field_of_view():
+    """Per band: the relative RMSE over the band, over its voxels inside the
+    field of view (None when it has none), and the share of such voxels."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    rng = np.random.default_rng(5)
+    ref = rng.uniform(1.0, 2.0, 300)
+    got = ref + rng.normal(0.0, 1e-3, 300)
+    got[200:] = ref[200:] + 0.5  # a band with large errors, all outside the field of view
+    in_fov = np.zeros(300, bool)
+    in_fov[:150] = True
+    out = bench.sample_error(got, ref, {"a": (0, 100), "b": (100, 200), "c": (200, 300)}, in_fov)
+    a, b, c = out["bands"]["a"], out["bands"]["b"], out["bands"]["c"]
+    assert a["in_fov_share"] == 1.0 and b["in_fov_share"] == 0.5 and c["in_fov_share"] == 0.0
+    assert c["rel_rmse_in_fov"] is None
+    d = got - ref
+    assert np.isclose(b["rel_rmse_in_fov"], np.linalg.norm(d[100:150]) / np.linalg.norm(ref[100:150]))
+    assert np.isclose(out["rel_rmse_in_fov"], np.linalg.norm(d[:150]) / np.linalg.norm(ref[:150]))
+    assert out["rel_rmse_in_fov"] < 1e-2 < out["rel_rmse"]
+    # without a mask the bands carry no field-of-view keys
+    assert "in_fov_share" not in bench.sample_error(got, ref, {"a": (0, 100)})["bands"]["a"]
